@@ -1,0 +1,236 @@
+/*
+ * topo.h -- C ABI of the B200 (sm_100a) SIMP design-iteration library.
+ *
+ * One `topo_ctx` is one topology-optimisation job: a device-resident mesh
+ * with its SolveFem, PDEFilter and MMA state.  Every entry point replaces one
+ * member function of the reference program
+ * (gkdas2/Unstructured-FEA-based-Topology-Optimization-in-PETSc-and-Eigen);
+ * the replaced interface is cited as file:line beside each declaration.
+ *
+ * Conventions
+ *  - Pointers named *_d are DEVICE pointers (cudaMalloc'd, or from
+ *    topo_device_alloc); everything else is host memory.  Ownership never
+ *    transfers.  Device vectors over elements have n_elems entries; over
+ *    DOFs 3*n_nodes entries, DOF 3n+c = component c of node n
+ *    (SolveFem.cpp:38-57).  m constraint vectors are stored back to back.
+ *  - Every call returns an int status: TOPO_OK (0); > 0 a usable result with
+ *    a warning (TOPO_NOT_CONVERGED: an iterative solve hit its iteration
+ *    cap); < 0 an error (nothing to use).  topo_last_error() gives the text.
+ *    No C++ exception crosses the ABI.
+ *  - All work of one context runs in stream order on the context's stream
+ *    (given at creation; NULL = the library creates one).  Calls that
+ *    return host scalars synchronise that stream.  One context is not
+ *    thread-safe; distinct contexts may be driven from distinct threads.
+ */
+#ifndef TOPO_H
+#define TOPO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TOPO_OK 0
+#define TOPO_NOT_CONVERGED 1
+#define TOPO_ERR_ARG (-1)
+#define TOPO_ERR_CUDA (-2)
+#define TOPO_ERR_OOM (-3)
+#define TOPO_ERR_MESH (-4)
+#define TOPO_ERR_NAN (-5)
+#define TOPO_ERR_UNSUPPORTED (-6)
+#define TOPO_ERR_TIMEOUT (-7)
+#define TOPO_ERR_IO (-8)
+
+#define TOPO_PREC_FP64 0  /* FP64 everywhere (the drop-in form) */
+#define TOPO_PREC_MIXED 1 /* FP32 AMG V-cycle inside FP64 FGMRES */
+
+typedef struct topo_ctx topo_ctx;
+
+/* Options.  Defaults (topo_params_default) are the reference's:
+ * OptPara.cpp:66-78 (Emin 1e-9, Emax 1e6, volfrac 0.12, penal 3, rmin 0.01,
+ * Xmin 0.01, Xmax 1, movlim 0.2, x0 0.5, beta0 1, betamax 8, proj off,
+ * maxItr 200), SolveFem.cpp:11 (nu 0.3), SolveFem.cpp:126-134 (FGMRES,
+ * rtol 1e-5), PDEFilter.cpp:117-120 (CG rtol 1e-5, atol 1e-50, dtol 1e5,
+ * maxit 10000), OptPara.cpp:160-177 (MMA a=0, c=1000, d=0, m=1). */
+typedef struct topo_params {
+    double Emin, Emax, nu, penal, volfrac, rmin, Xmin, Xmax, movlim, x0, beta0, betamax;
+    int proj, maxItr, m;
+    double ch_tol;         /* main.cpp:70 stop rule `ch > 0.01`; <= 0 disables */
+    /* displacement solve: FGMRES + smoothed-aggregation AMG */
+    double fem_rtol;
+    int fem_restart, fem_maxit;
+    int precision;         /* TOPO_PREC_FP64 or TOPO_PREC_MIXED */
+    int amg_max_levels;    /* hierarchy depth cap (PCGAMGSetNlevels(pc,4)) */
+    int amg_coarse_max;    /* coarsen until a level has <= this many DOFs */
+    int amg_smooth_p;      /* 1: smoothed aggregation, 0: plain aggregation */
+    int cheb_degree;       /* Chebyshev-Jacobi smoothing steps per sweep */
+    int fine_smoother_matfree; /* 1: fine-level smoother uses the element operator */
+    /* Helmholtz filter CG (Jacobi) */
+    double filter_rtol, filter_atol, filter_dtol;
+    int filter_maxit;
+    int verbose;           /* 1: print the reference's per-solve lines */
+} topo_params;
+
+typedef struct topo_solve_info {
+    int fem_its;           /* FGMRES iterations of the last displacement solve */
+    double fem_relres;     /* ||F - K U|| / ||F|| after it (SolveFem.cpp:142-152) */
+    int fem_status;        /* 0 converged, 1 iteration cap */
+    int filter_its[4];     /* CG iterations of the last filter solves */
+    int amg_levels;
+    int amg_dofs[8];       /* DOFs per AMG level */
+    int mma_inner_its;     /* dual interior-point steps of the last update */
+    double last_fx, last_gx0, last_ch;
+    double t_fem_ms, t_filter_ms, t_mma_ms, t_setup_ms; /* stage times (CUDA events) */
+} topo_solve_info;
+
+/* ---------------------------------------------------------------- basics */
+const char* topo_last_error(void);
+const char* topo_version(void);
+void topo_params_default(topo_params* p);
+
+/* Device memory for callers without the CUDA runtime. */
+int topo_device_alloc(size_t bytes, void** ptr_d);
+int topo_device_free(void* ptr_d);
+int topo_memcpy_h2d(void* dst_d, const void* src, size_t bytes, topo_ctx* ctx);
+int topo_memcpy_d2h(void* dst, const void* src_d, size_t bytes, topo_ctx* ctx);
+int topo_sync(topo_ctx* ctx);
+
+/* ---------------------------------------------------------------- mesh + context */
+/* Replaces InputMeshData::GetNodeAndElementData + GetBcs
+ * (InputMeshData.cpp:33-285) and the SolveFem / PDEFilter / MMA constructors
+ * (SolveFem.cpp:6-15, PDEFilter.cpp:7-10,36-140, OptPara.cpp:158-177).
+ *   nen          8 (hex8, diagonal numbering) or 4 (tet4)
+ *   vertex       n_nodes*3 doubles (vertex.txt rows)
+ *   element      n_elems*nen 0-based node ids (element.txt rows)
+ *   fixed_dofs   n_fixed DOF ids (fixeddofs.txt)
+ *   n_cases      load cases (NUM_LD); case c owns entries
+ *                case_ptr[c]..case_ptr[c+1]-1 of load_dofs/load_vals
+ *                (loaddof_c.txt / load_c.txt).  n_cases > 1 runs the
+ *                block (multi-load) solver; compliance sums over cases.
+ *   stream       cudaStream_t for all work of this context, or NULL.
+ * Builds the element matrices, volumes (TV), filter operators and the AMG
+ * graph hierarchy on the device. */
+int topo_create(const topo_params* p, int nen, int n_nodes, const double* vertex, int n_elems,
+                const int32_t* element, int n_fixed, const int32_t* fixed_dofs, int n_cases,
+                const int32_t* case_ptr, const int32_t* load_dofs, const double* load_vals,
+                void* stream, topo_ctx** out);
+int topo_destroy(topo_ctx* ctx);
+int topo_get_params(topo_ctx* ctx, topo_params* p);
+int topo_set_params(topo_ctx* ctx, const topo_params* p);  /* scalar options only */
+int topo_sizes(topo_ctx* ctx, int* nen, int* n_nodes, int* n_elems, int* n_cases);
+void* topo_stream(topo_ctx* ctx);
+
+/* ---------------------------------------------------------------- SolveFem */
+/* Element volumes Vol and their sum TV (SolveFem::ComputeTotalVol,
+ * SolveFem.cpp:59-89; 5-tet hex volume SolveFem.cpp:423-467). */
+int topo_fem_volumes(topo_ctx* ctx, double* vol_d, double* total_volume);
+/* Element stiffness (E = 1) of element e, full ndof_e x ndof_e row-major,
+ * DOF order [x0..,y0..,z0..] (SolveFem::Hex8Isoparametric
+ * SolveFem.cpp:339-408; tet4/Tet4Isoparametric.cpp:1-41). Host output. */
+int topo_fem_element_matrix(topo_ctx* ctx, int e, double* ke);
+/* y = K(xphys) u with Dirichlet rows/columns as identity
+ * (AssembleFem + MatZeroRowsColumns + MatMult, SolveFem.cpp:267-337). */
+int topo_fem_apply(topo_ctx* ctx, const double* xphys_d, const double* u_d, double* y_d);
+/* SolveFem::ComputeObjectiveAndSensitivities (SolveFem.h:39-40,
+ * SolveFem.cpp:159-265): solves K U = F, then fx = sum E_e u_e'Ke u_e,
+ * dfdx, gx[0] = sum x vol / TV - volfrac, dgdx[0] = vol / TV.
+ * fx, gx: host; xphys_d, dfdx_d, dgdx_d (m * n_elems): device. */
+int topo_fem_obj_sens(topo_ctx* ctx, const double* xphys_d, double* fx, double* gx, double* dfdx_d,
+                      double* dgdx_d);
+/* The solve alone (SolveFem::ComputeFem, SolveFem.cpp:91-157); U zeroed
+ * first, like AssembleFem's VecZeroEntries(U). */
+int topo_fem_solve(topo_ctx* ctx, const double* xphys_d, double* u_d);
+/* public member U (SolveFem.h:42): last displacement, 3*n_nodes*n_cases */
+int topo_fem_displacement(topo_ctx* ctx, double* u_d);
+/* von Mises stress per element (stress/ComputeStress.cpp:53-104): centroid
+ * stress Emax*D*B*u relaxed by sqrt(x); uses the last displacement. */
+int topo_fem_von_mises(topo_ctx* ctx, const double* xphys_d, double* vms_d);
+
+/* ---------------------------------------------------------------- PDEFilter */
+/* PDEFilter::Filter (PDEFilter.cpp:142-165): xf = clamp(TFX' KF^-1 TF x, Xmin, 1);
+ * the CG warm-starts from the previous solve's RX (PDEFilter.cpp:127). */
+int topo_filter_apply(topo_ctx* ctx, const double* x_d, double* xf_d, double Xmin);
+/* PDEFilter::ComputeFilteredSens (PDEFilter.cpp:167-183), in place. */
+int topo_filter_sens(topo_ctx* ctx, double* dfdx_d, double* dgdx_d, int m);
+/* PDEFilter::HeavisideFilter (PDEFilter.cpp:242-293); keeps beta state. */
+int topo_heaviside(topo_ctx* ctx, const double* xf_d, double* xp_d, double x0, double beta0,
+                   double betamax, int itr, double Xmin, int proj);
+/* PDEFilter::ComputeProjectedSens (PDEFilter.cpp:295-341), in place. */
+int topo_projected_sens(topo_ctx* ctx, const double* xf_d, double* dfdx_d, double* dgdx_d, int m,
+                        double x0);
+/* filter warm-start vector RX (n_nodes), read (set=0) or write (set=1) */
+int topo_filter_state(topo_ctx* ctx, double* rx_d, int set);
+
+/* ---------------------------------------------------------------- MMA */
+/* MMA::SetOuterMovelimit (MMA.h:43, MMA.cpp:370-389) */
+int topo_mma_set_outer_movelimit(topo_ctx* ctx, double Xmin, double Xmax, double movlim,
+                                 const double* x_d, double* xmin_d, double* xmax_d);
+/* MMA::Update (MMA.h:23, MMA.cpp:483-502): GenSub + dual interior point;
+ * xval_d updated in place.  gx: host, m values. */
+int topo_mma_update(topo_ctx* ctx, double* xval_d, const double* dfdx_d, const double* gx,
+                    const double* dgdx_d, const double* xmin_d, const double* xmax_d);
+/* MMA::DesignChange (MMA.h:52, MMA.cpp:391-410): ch = max|x - xold|, xold = x */
+int topo_mma_design_change(topo_ctx* ctx, const double* x_d, double* xold_d, double* ch);
+/* MMA::SetAsymptotes (MMA.h:29, MMA.cpp:345-353) */
+int topo_mma_set_asymptotes(topo_ctx* ctx, double init, double decrease, double increase);
+/* MMA::SetRobustAsymptotesType (MMA.h:39, MMA.cpp:355-368) */
+int topo_mma_set_robust_asymptotes_type(topo_ctx* ctx, int val);
+/* MMA::ConstraintModification (MMA.h:32-35) */
+int topo_mma_constraint_modification(topo_ctx* ctx, int on);
+/* MMA::Restart (MMA.h:26, MMA.cpp:302-342): export xo1, xo2, U, L; and the
+ * restart constructor's import (MMA.h:15-18): set=1 loads them with iteration k. */
+int topo_mma_restart(topo_ctx* ctx, double* xo1_d, double* xo2_d, double* U_d, double* L_d, int* k,
+                     int set);
+/* MMA::KKTresidual (MMA.h:47-48, MMA.cpp:412-480) */
+int topo_mma_kkt_residual(topo_ctx* ctx, const double* x_d, const double* dfdx_d, const double* gx,
+                          const double* dgdx_d, const double* xmin_d, const double* xmax_d,
+                          double* norm2, double* norm_inf);
+
+/* ---------------------------------------------------------------- main.cpp loop */
+/* Design state owned by the context (OptPara Vecs, OptPara.h:28-52):
+ * X = XFiled = XPhys = Xold = volfrac, then the initial Filter +
+ * HeavisideFilter of main.cpp:64-66. */
+int topo_opt_init(topo_ctx* ctx);
+/* One pass of the main.cpp:72-112 loop body.  fx, gx0, ch: host (may be NULL). */
+int topo_opt_step(topo_ctx* ctx, int* itr, double* fx, double* gx0, double* ch);
+/* Runs the loop `while (itr < maxItr && ch > ch_tol)` (main.cpp:70);
+ * hist (host, may be NULL) receives [fx, gx0, ch] per iteration. */
+int topo_opt_run(topo_ctx* ctx, int max_itr, double* hist, int* iterations);
+/* Host-buffer form used end to end: uploads X (host, n_elems), runs one
+ * iteration, downloads XPhys (host) and returns fx. */
+int topo_opt_step_host(topo_ctx* ctx, const double* x_in, double* xphys_out, double* fx);
+/* access to the context's design vectors; which: 0 X, 1 XPhys, 2 XFiled,
+ * 3 Xold, 4 dfdx, 5 dgdx (m*n_elems), 6 xmin, 7 xmax.  Device pointer out. */
+int topo_opt_vector(topo_ctx* ctx, int which, double** ptr_d);
+int topo_solve_info_get(topo_ctx* ctx, topo_solve_info* info);
+
+/* ---------------------------------------------------------------- mesh files, output */
+/* Synthetic jittered cantilever lattice in the reference's formats (host):
+ * nodes (nx+1)(ny+1)(nz+1) with id i + (nx+1)(j + (ny+1)k), splitmix64
+ * jitter, hex8 (diagonal numbering) or 6 tet4 per hex.  Pass NULL buffers
+ * to query sizes. load_mode 0: unit total -z force on nodes (nx, j, 0);
+ * 1: +1 y on nodes (nx, 0, k). */
+int topo_gen_cantilever(int nx, int ny, int nz, int nen, double jitter, uint64_t seed, int load_mode,
+                        double* vertex, int32_t* element, int32_t* fixed_dofs, int32_t* load_dofs,
+                        double* load_vals, int* n_nodes, int* n_elems, int* n_fixed, int* n_loads);
+/* k seeded unit point loads on the x = L face (3 DOFs per case). */
+int topo_gen_multiload(int nx, int ny, int nz, int k, uint64_t seed, int32_t* load_dofs,
+                       double* load_vals);
+/* Reads vertex.txt, element.txt, fixeddofs.txt, loaddof_<c>.txt, load_<c>.txt
+ * from dir (InputMeshData.cpp:97-149,228-285).  Two passes: NULL buffers
+ * query the sizes. */
+int topo_read_mesh_dir(const char* dir, int nen, int n_cases, double* vertex, int32_t* element,
+                       int32_t* fixed_dofs, int32_t* case_ptr, int32_t* load_dofs, double* load_vals,
+                       int* n_nodes, int* n_elems, int* n_fixed, int* n_loads);
+/* Write2Vtu::WriteResults (Write2Vtu.cpp:5-174): ASCII .vtu with the
+ * diagonal->VTK node reorder, cell type 12 (hex8) / 10 (tet4), point data
+ * ux uy uz and cell data xphys, from the context's last U and XPhys.
+ * itr 0 -> output_initial.vtu, -1 -> output_final.vtu, else output_<itr>.vtu. */
+int topo_write_vtu(topo_ctx* ctx, const char* dir, int itr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

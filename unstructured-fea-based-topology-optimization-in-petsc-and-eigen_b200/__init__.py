@@ -1,0 +1,476 @@
+"""Python front end of libtopo.so, the sm_100a SIMP design-iteration library.
+
+The library's product boundary is the C ABI in include/topo.h; this module
+binds it with ctypes so that Python callers (tests, the benchmark, serving
+drivers) can use it.  Device vectors are torch CUDA tensors (torch is used as
+the device-memory and stream plumbing only).  The classes SolveFem, PDEFilter
+and MMA mirror the reference's class interfaces (SolveFem.h, PDEFilter.h,
+MMA.h) on top of one `Context` (one topology-optimisation job).
+
+There is no CPU fallback: without a CUDA device every call that touches the
+GPU raises TopoError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtopo.so")
+
+TOPO_OK = 0
+TOPO_NOT_CONVERGED = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+class Params(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "Emin", "Emax", "nu", "penal", "volfrac", "rmin", "Xmin", "Xmax", "movlim", "x0", "beta0", "betamax")] + [
+        ("proj", C.c_int), ("maxItr", C.c_int), ("m", C.c_int), ("ch_tol", C.c_double),
+        ("fem_rtol", C.c_double), ("fem_restart", C.c_int), ("fem_maxit", C.c_int), ("precision", C.c_int),
+        ("amg_max_levels", C.c_int), ("amg_coarse_max", C.c_int), ("amg_smooth_p", C.c_int),
+        ("cheb_degree", C.c_int), ("fine_smoother_matfree", C.c_int),
+        ("filter_rtol", C.c_double), ("filter_atol", C.c_double), ("filter_dtol", C.c_double),
+        ("filter_maxit", C.c_int), ("verbose", C.c_int)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("fem_its", C.c_int), ("fem_relres", C.c_double), ("fem_status", C.c_int),
+                ("filter_its", C.c_int * 4), ("amg_levels", C.c_int), ("amg_dofs", C.c_int * 8),
+                ("mma_inner_its", C.c_int), ("last_fx", C.c_double), ("last_gx0", C.c_double),
+                ("last_ch", C.c_double), ("t_fem_ms", C.c_double), ("t_filter_ms", C.c_double),
+                ("t_mma_ms", C.c_double), ("t_setup_ms", C.c_double)]
+
+
+class TopoError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+# every symbol include/topo.h declares, with its ctypes signature
+_SIGS = {
+    "topo_last_error": ([], C.c_char_p),
+    "topo_version": ([], C.c_char_p),
+    "topo_params_default": ([C.POINTER(Params)], None),
+    "topo_device_alloc": ([C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
+    "topo_device_free": ([C.c_void_p], C.c_int),
+    "topo_memcpy_h2d": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "topo_memcpy_d2h": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "topo_sync": ([C.c_void_p], C.c_int),
+    "topo_create": ([C.POINTER(Params), C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                     C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
+    "topo_destroy": ([C.c_void_p], C.c_int),
+    "topo_get_params": ([C.c_void_p, C.POINTER(Params)], C.c_int),
+    "topo_set_params": ([C.c_void_p, C.POINTER(Params)], C.c_int),
+    "topo_sizes": ([C.c_void_p] + [C.POINTER(C.c_int)] * 4, C.c_int),
+    "topo_stream": ([C.c_void_p], C.c_void_p),
+    "topo_fem_volumes": ([C.c_void_p, C.c_void_p, _dp], C.c_int),
+    "topo_fem_element_matrix": ([C.c_void_p, C.c_int, C.c_void_p], C.c_int),
+    "topo_fem_apply": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "topo_fem_obj_sens": ([C.c_void_p, C.c_void_p, _dp, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "topo_fem_solve": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "topo_fem_displacement": ([C.c_void_p, C.c_void_p], C.c_int),
+    "topo_fem_von_mises": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "topo_filter_apply": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_double], C.c_int),
+    "topo_filter_sens": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "topo_heaviside": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int,
+                        C.c_double, C.c_int], C.c_int),
+    "topo_projected_sens": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double], C.c_int),
+    "topo_filter_state": ([C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "topo_mma_set_outer_movelimit": ([C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                      C.c_void_p], C.c_int),
+    "topo_mma_update": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+                        C.c_int),
+    "topo_mma_design_change": ([C.c_void_p, C.c_void_p, C.c_void_p, _dp], C.c_int),
+    "topo_mma_set_asymptotes": ([C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
+    "topo_mma_set_robust_asymptotes_type": ([C.c_void_p, C.c_int], C.c_int),
+    "topo_mma_constraint_modification": ([C.c_void_p, C.c_int], C.c_int),
+    "topo_mma_restart": ([C.c_void_p] + [C.c_void_p] * 4 + [C.POINTER(C.c_int), C.c_int], C.c_int),
+    "topo_mma_kkt_residual": ([C.c_void_p] + [C.c_void_p] * 6 + [_dp, _dp], C.c_int),
+    "topo_opt_init": ([C.c_void_p], C.c_int),
+    "topo_opt_step": ([C.c_void_p, C.POINTER(C.c_int), _dp, _dp, _dp], C.c_int),
+    "topo_opt_run": ([C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)], C.c_int),
+    "topo_opt_step_host": ([C.c_void_p, C.c_void_p, C.c_void_p, _dp], C.c_int),
+    "topo_opt_vector": ([C.c_void_p, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "topo_solve_info_get": ([C.c_void_p, C.POINTER(SolveInfo)], C.c_int),
+    "topo_gen_cantilever": ([C.c_int] * 4 + [C.c_double, C.c_uint64, C.c_int] + [C.c_void_p] * 5 +
+                            [C.POINTER(C.c_int)] * 4, C.c_int),
+    "topo_gen_multiload": ([C.c_int] * 4 + [C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
+    "topo_read_mesh_dir": ([C.c_char_p, C.c_int, C.c_int] + [C.c_void_p] * 6 + [C.POINTER(C.c_int)] * 4, C.c_int),
+    "topo_write_vtu": ([C.c_void_p, C.c_char_p, C.c_int], C.c_int),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libtopo.so (built in-tree by build.py) and bind every symbol."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise TopoError(-2, f"{LIB_PATH} is missing: run build.py (there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def symbols():
+    return list(_SIGS)
+
+
+def last_error() -> str:
+    return lib().topo_last_error().decode()
+
+
+def _check(rc, what):
+    if rc < 0:
+        raise TopoError(rc, f"{what}: {last_error()}")
+    return rc
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    lib().topo_params_default(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+# ---------------------------------------------------------------- meshes
+def gen_cantilever(nx, ny, nz, nen=8, jitter=None, seed=2024, load_mode=0):
+    """Seeded jittered cantilever lattice (host arrays)."""
+    if jitter is None:
+        jitter = 0.1 if nen == 8 else 0.2
+    nn, ne, nf, nl = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    L = lib()
+    _check(L.topo_gen_cantilever(nx, ny, nz, nen, jitter, seed, load_mode, None, None, None, None, None,
+                                 C.byref(nn), C.byref(ne), C.byref(nf), C.byref(nl)), "gen_cantilever")
+    v = np.zeros(nn.value * 3)
+    e = np.zeros(ne.value * nen, dtype=np.int32)
+    f = np.zeros(nf.value, dtype=np.int32)
+    ld = np.zeros(nl.value, dtype=np.int32)
+    lv = np.zeros(nl.value)
+    _check(L.topo_gen_cantilever(nx, ny, nz, nen, jitter, seed, load_mode, _ptr(v), _ptr(e), _ptr(f), _ptr(ld),
+                                 _ptr(lv), C.byref(nn), C.byref(ne), C.byref(nf), C.byref(nl)), "gen_cantilever")
+    return v.reshape(-1, 3), e.reshape(-1, nen), f, ld, lv
+
+
+def gen_multiload(nx, ny, nz, k, seed=2025):
+    ld = np.zeros(3 * k, dtype=np.int32)
+    lv = np.zeros(3 * k)
+    _check(lib().topo_gen_multiload(nx, ny, nz, k, seed, _ptr(ld), _ptr(lv)), "gen_multiload")
+    return ld, lv
+
+
+def read_mesh_dir(path, nen=8, n_cases=1):
+    nn, ne, nf, nl = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    L = lib()
+    b = path.encode()
+    _check(L.topo_read_mesh_dir(b, nen, n_cases, None, None, None, None, None, None, C.byref(nn), C.byref(ne),
+                                C.byref(nf), C.byref(nl)), "read_mesh_dir")
+    v = np.zeros(nn.value * 3)
+    e = np.zeros(ne.value * nen, dtype=np.int32)
+    f = np.zeros(nf.value, dtype=np.int32)
+    cp = np.zeros(n_cases + 1, dtype=np.int32)
+    ld = np.zeros(nl.value, dtype=np.int32)
+    lv = np.zeros(nl.value)
+    _check(L.topo_read_mesh_dir(b, nen, n_cases, _ptr(v), _ptr(e), _ptr(f), _ptr(cp), _ptr(ld), _ptr(lv),
+                                C.byref(nn), C.byref(ne), C.byref(nf), C.byref(nl)), "read_mesh_dir")
+    return v.reshape(-1, 3), e.reshape(-1, nen), f, ld, lv, cp
+
+
+# ---------------------------------------------------------------- context
+def _torch():
+    import torch
+    return torch
+
+
+def _dptr(t):
+    if t is None:
+        return None
+    assert t.is_cuda and t.is_contiguous(), "device tensors must be contiguous CUDA tensors"
+    return C.c_void_p(t.data_ptr())
+
+
+class Context:
+    """One job: device-resident mesh + SolveFem + PDEFilter + MMA state."""
+
+    def __init__(self, vertex, element, fixed, load_dofs, load_vals, case_ptr=None, params: Optional[Params] = None,
+                 stream=None, **kw):
+        torch = _torch()
+        self.params = params if params is not None else default_params(**kw)
+        vertex = np.ascontiguousarray(vertex, dtype=np.float64).reshape(-1)
+        element = np.ascontiguousarray(element, dtype=np.int32)
+        nen = element.shape[1] if element.ndim == 2 else 8
+        fixed = np.ascontiguousarray(fixed, dtype=np.int32)
+        ld = np.ascontiguousarray(load_dofs, dtype=np.int32)
+        lv = np.ascontiguousarray(load_vals, dtype=np.float64)
+        if case_ptr is None:
+            case_ptr = np.array([0, ld.size], dtype=np.int32)
+        case_ptr = np.ascontiguousarray(case_ptr, dtype=np.int32)
+        self.nen, self.nn, self.ne = nen, vertex.size // 3, element.size // nen
+        self.ndof, self.ncases = 3 * self.nn, case_ptr.size - 1
+        if stream is None:
+            stream = torch.cuda.current_stream().cuda_stream
+        self.stream = stream
+        h = C.c_void_p()
+        _check(lib().topo_create(C.byref(self.params), nen, self.nn, _ptr(vertex), self.ne, _ptr(element.reshape(-1)),
+                                 fixed.size, _ptr(fixed), self.ncases, _ptr(case_ptr), _ptr(ld), _ptr(lv),
+                                 C.c_void_p(stream), C.byref(h)), "topo_create")
+        self.h = h
+        self.m = self.params.m
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().topo_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---------------- helpers
+    def zeros(self, n):
+        torch = _torch()
+        return torch.zeros(n, dtype=torch.float64, device="cuda")
+
+    def set_params(self, **kw):
+        for k, v in kw.items():
+            setattr(self.params, k, v)
+        _check(lib().topo_set_params(self.h, C.byref(self.params)), "topo_set_params")
+
+    def info(self) -> SolveInfo:
+        s = SolveInfo()
+        _check(lib().topo_solve_info_get(self.h, C.byref(s)), "info")
+        return s
+
+    # ---------------- SolveFem
+    def volumes(self):
+        vol = self.zeros(self.ne)
+        tv = C.c_double()
+        _check(lib().topo_fem_volumes(self.h, _dptr(vol), C.byref(tv)), "volumes")
+        return vol, tv.value
+
+    def element_matrix(self, e):
+        nd = 3 * self.nen
+        k = np.zeros(nd * nd)
+        _check(lib().topo_fem_element_matrix(self.h, e, _ptr(k)), "element_matrix")
+        return k.reshape(nd, nd)
+
+    def fem_apply(self, xphys, u):
+        y = self.zeros(self.ndof)
+        _check(lib().topo_fem_apply(self.h, _dptr(xphys), _dptr(u), _dptr(y)), "fem_apply")
+        return y
+
+    def fem_obj_sens(self, xphys):
+        fx = C.c_double()
+        gx = np.zeros(self.m)
+        df = self.zeros(self.ne)
+        dg = self.zeros(self.ne * self.m)
+        rc = _check(lib().topo_fem_obj_sens(self.h, _dptr(xphys), C.byref(fx), gx.ctypes.data_as(_dp), _dptr(df),
+                                            _dptr(dg)), "fem_obj_sens")
+        return fx.value, gx, df, dg.view(self.m, self.ne), rc
+
+    def fem_solve(self, xphys):
+        U = self.zeros(self.ndof * self.ncases)
+        rc = _check(lib().topo_fem_solve(self.h, _dptr(xphys), _dptr(U)), "fem_solve")
+        return U, rc
+
+    def displacement(self):
+        U = self.zeros(self.ndof * self.ncases)
+        _check(lib().topo_fem_displacement(self.h, _dptr(U)), "displacement")
+        return U
+
+    def von_mises(self, xphys):
+        v = self.zeros(self.ne)
+        _check(lib().topo_fem_von_mises(self.h, _dptr(xphys), _dptr(v)), "von_mises")
+        return v
+
+    # ---------------- PDEFilter
+    def filter(self, x, Xmin=None):
+        xf = self.zeros(self.ne)
+        rc = _check(lib().topo_filter_apply(self.h, _dptr(x), _dptr(xf), self.params.Xmin if Xmin is None else Xmin),
+                    "filter")
+        return xf
+
+    def filter_sens(self, dfdx, dgdx):
+        df = dfdx.clone().contiguous()
+        dg = dgdx.clone().contiguous()
+        m = dg.numel() // self.ne
+        _check(lib().topo_filter_sens(self.h, _dptr(df), _dptr(dg), m), "filter_sens")
+        return df, dg.view(m, self.ne)
+
+    def filter_state(self, rx=None):
+        if rx is None:
+            out = self.zeros(self.nn)
+            _check(lib().topo_filter_state(self.h, _dptr(out), 0), "filter_state")
+            return out
+        _check(lib().topo_filter_state(self.h, _dptr(rx.contiguous()), 1), "filter_state")
+
+    def heaviside(self, xf, itr, x0=0.5, beta0=1.0, betamax=8.0, Xmin=0.01, proj=0):
+        xp = self.zeros(self.ne)
+        _check(lib().topo_heaviside(self.h, _dptr(xf), _dptr(xp), x0, beta0, betamax, itr, Xmin, proj), "heaviside")
+        return xp
+
+    def projected_sens(self, xf, dfdx, dgdx, x0=0.5):
+        df = dfdx.clone().contiguous()
+        dg = dgdx.clone().contiguous()
+        m = dg.numel() // self.ne
+        _check(lib().topo_projected_sens(self.h, _dptr(xf), _dptr(df), _dptr(dg), m, x0), "projected_sens")
+        return df, dg.view(m, self.ne)
+
+    # ---------------- MMA
+    def mma_movelimit(self, x, Xmin=0.01, Xmax=1.0, movlim=0.2):
+        a, b = self.zeros(self.ne), self.zeros(self.ne)
+        _check(lib().topo_mma_set_outer_movelimit(self.h, Xmin, Xmax, movlim, _dptr(x), _dptr(a), _dptr(b)),
+               "movelimit")
+        return a, b
+
+    def mma_update(self, x, dfdx, gx, dgdx, xmin, xmax):
+        xv = x.clone().contiguous()
+        g = np.ascontiguousarray(gx, dtype=np.float64)
+        _check(lib().topo_mma_update(self.h, _dptr(xv), _dptr(dfdx.contiguous()), _ptr(g),
+                                     _dptr(dgdx.contiguous()), _dptr(xmin), _dptr(xmax)), "mma_update")
+        return xv
+
+    def mma_design_change(self, x, xold):
+        xo = xold.clone().contiguous()
+        ch = C.c_double()
+        _check(lib().topo_mma_design_change(self.h, _dptr(x), _dptr(xo), C.byref(ch)), "design_change")
+        return ch.value, xo
+
+    def mma_state(self):
+        a = [self.zeros(self.ne) for _ in range(4)]
+        k = C.c_int()
+        _check(lib().topo_mma_restart(self.h, *[_dptr(t) for t in a], C.byref(k), 0), "mma_restart")
+        return a + [k.value]
+
+    def mma_kkt(self, x, dfdx, gx, dgdx, xmin, xmax):
+        n2, ni = C.c_double(), C.c_double()
+        g = np.ascontiguousarray(gx, dtype=np.float64)
+        _check(lib().topo_mma_kkt_residual(self.h, _dptr(x), _dptr(dfdx), _ptr(g), _dptr(dgdx), _dptr(xmin),
+                                           _dptr(xmax), C.byref(n2), C.byref(ni)), "kkt")
+        return n2.value, ni.value
+
+    # ---------------- main loop
+    def opt_init(self):
+        _check(lib().topo_opt_init(self.h), "opt_init")
+
+    def opt_step(self):
+        it, fx, gx, ch = C.c_int(), C.c_double(), C.c_double(), C.c_double()
+        rc = _check(lib().topo_opt_step(self.h, C.byref(it), C.byref(fx), C.byref(gx), C.byref(ch)), "opt_step")
+        return it.value, fx.value, gx.value, ch.value
+
+    def opt_run(self, max_itr):
+        hist = np.zeros(3 * max_itr)
+        n = C.c_int()
+        _check(lib().topo_opt_run(self.h, max_itr, _ptr(hist), C.byref(n)), "opt_run")
+        return hist.reshape(-1, 3)[:n.value]
+
+    def opt_step_host(self, x_in: np.ndarray, xphys_out: np.ndarray):
+        fx = C.c_double()
+        _check(lib().topo_opt_step_host(self.h, _ptr(x_in), _ptr(xphys_out), C.byref(fx)), "opt_step_host")
+        return fx.value
+
+    def opt_vector(self, which):
+        """Device pointer (int) of one of the context's design vectors."""
+        p = C.c_void_p()
+        _check(lib().topo_opt_vector(self.h, which, C.byref(p)), "opt_vector")
+        return p.value
+
+    def opt_tensor(self, which, n=None):
+        """Copy of a context design vector (0 X, 1 XPhys, 2 XFiled, 3 Xold,
+        4 dfdx, 5 dgdx, 6 xmin, 7 xmax) as a torch tensor."""
+        n = n or (self.ne * self.m if which == 5 else self.ne)
+        return device_view(self.opt_vector(which), n).clone()
+
+    def write_vtu(self, directory, itr):
+        _check(lib().topo_write_vtu(self.h, directory.encode(), itr), "write_vtu")
+
+
+def device_view(ptr, n):
+    """Zero-copy torch view of n doubles at a device pointer."""
+    torch = _torch()
+
+    class _Arr:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_Arr(), device="cuda")
+
+
+# ---------------------------------------------------------------- reference-shaped classes
+class SolveFem:
+    """SolveFem (SolveFem.h:12-55) over a Context."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.Vol, self.TV = ctx.volumes()
+
+    def ComputeObjectiveAndSensitivities(self, XPhys):
+        fx, gx, df, dg, _ = self.ctx.fem_obj_sens(XPhys)
+        return fx, gx, df, dg
+
+    @property
+    def U(self):
+        return self.ctx.displacement()
+
+
+class PDEFilter:
+    """PDEFilter (PDEFilter.h:12-56) over a Context."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def Filter(self, X, Xmin):
+        return self.ctx.filter(X, Xmin)
+
+    def ComputeFilteredSens(self, dfdx, dgdx):
+        return self.ctx.filter_sens(dfdx, dgdx)
+
+    def HeavisideFilter(self, XFiled, x0, beta0, betamax, itr, Xmin, proj):
+        return self.ctx.heaviside(XFiled, itr, x0, beta0, betamax, Xmin, proj)
+
+    def ComputeProjectedSens(self, XFiled, dfdx, dgdx, x0):
+        return self.ctx.projected_sens(XFiled, dfdx, dgdx, x0)
+
+
+class MMA:
+    """MMA (MMA.h:8-119) over a Context (a = 0, c = 1000, d = 0)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def SetOuterMovelimit(self, Xmin, Xmax, movlim, x):
+        return self.ctx.mma_movelimit(x, Xmin, Xmax, movlim)
+
+    def Update(self, xval, dfdx, gx, dgdx, xmin, xmax):
+        return self.ctx.mma_update(xval, dfdx, gx, dgdx, xmin, xmax)
+
+    def DesignChange(self, x, xold):
+        return self.ctx.mma_design_change(x, xold)

@@ -1,0 +1,756 @@
+// amg.cu -- numeric phase of the smoothed-aggregation AMG (rebuilt every
+// design iteration on the device) and its V-cycle.
+//
+// Replaces PCGAMG with PCGAMGSetNlevels(pc,4) + PCSetCoordinates
+// (SolveFem.cpp:130-132).  Per design iteration:
+//   A0  <- sum_e E_e Ke_e gathered node-row by node-row (deterministic),
+//          Dirichlet rows/columns identity (MatZeroRowsColumns, SolveFem.cpp:324)
+//   rho <- power iteration on D^-1 A (warm-started across design iterations)
+//   P   <- (I - 4/(3 rho) D^-1 A) Pt        (smoothed aggregation)
+//   A+  <- P^T (A P)                         (Galerkin, two fixed-pattern SpGEMMs)
+//   coarsest: explicit FP64 inverse (Gauss-Jordan, partial pivoting)
+// V-cycle: Chebyshev(k)-Jacobi pre/post smoothing on [0.1, 1.1] rho.
+//
+// BSR values are slot-interleaved (see ctx.h) so that the lanes of a warp
+// walking the blocks of one row read every block entry as a coalesced run.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "ctx.h"
+
+namespace topo {
+
+int kmatvec32(Ctx& c, const float* u, float* y, const float* b);
+int kmatvec64r(Ctx& c, const double* u, double* y, const double* b);
+
+__host__ __device__ __forceinline__ int pk_index_amg(int i, int j, int n) {
+    if (i > j) { int t = i; i = j; j = t; }
+    return i * n - (i * (i - 1)) / 2 + (j - i);
+}
+
+// ----------------------------------------------------------------- level-0 assembly
+// One warp per node row: for each incident element (sequential, so the sum
+// order is fixed) lanes own the element's 3*NEN columns and add the three
+// rows of that node into a shared-memory row buffer, then the row is written
+// out with the Dirichlet identity applied.
+template <class T, int NEN>
+__global__ void k_assemble_A0(int nn, const int* __restrict__ n2e_ptr, const int* __restrict__ n2e,
+                              const uint16_t* __restrict__ bpos, const T* __restrict__ ke, const T* __restrict__ Ee,
+                              const int* __restrict__ rp, const int* __restrict__ ci,
+                              const unsigned char* __restrict__ dfix, T* __restrict__ A, int maxdeg) {
+    constexpr int ND = 3 * NEN, NPK = ND * (ND + 1) / 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (blockDim.x >> 5) + wib;
+    if (i >= nn) return;
+    T* buf = reinterpret_cast<T*>(smem_raw) + (size_t)wib * maxdeg * 9;
+    const int r0 = rp[i], nb = rp[i + 1] - r0;
+    for (int q = lane; q < 9 * nb; q += 32) buf[q] = T(0);
+    __syncwarp();
+    for (int p = n2e_ptr[i]; p < n2e_ptr[i + 1]; p++) {
+        const int q = n2e[p], e = q / NEN, l = q % NEN;
+        const T E = Ee[e];
+        const int tile = e >> 5, el = e & 31;
+        const T* kp = ke + (size_t)tile * NPK * 32 + el;
+        for (int k = lane; k < ND; k += 32) {
+            const int m = k % NEN, d = k / NEN;
+            const int slot = bpos[((size_t)e * NEN + l) * NEN + m];
+#pragma unroll
+            for (int cc = 0; cc < 3; cc++) {
+                const int rl = cc * NEN + l;
+                buf[(cc * 3 + d) * nb + slot] += E * kp[(size_t)pk_index_amg(rl, k, ND) * 32];
+            }
+        }
+        __syncwarp();
+    }
+    for (int idx = lane; idx < 9 * nb; idx += 32) {
+        const int ent = idx / nb, slot = idx - ent * nb;
+        const int cc = ent / 3, d = ent % 3;
+        const int j = ci[r0 + slot];
+        T v = buf[idx];
+        const bool rf = dfix[3L * i + cc], cf = dfix[3L * j + d];
+        if (rf || cf) v = (rf && j == i && cc == d) ? T(1) : T(0);
+        A[(size_t)r0 * 9 + idx] = v;
+    }
+}
+
+// dinv[dof] = 1 / A_dof,dof (point Jacobi)
+template <class T, int BS>
+__global__ void k_diag_inv(int nnode, const int* __restrict__ rp, const int* __restrict__ diagpos,
+                           const T* __restrict__ A, T* __restrict__ dinv) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnode) return;
+    const int r0 = rp[i], nb = rp[i + 1] - r0, s = diagpos[i];
+#pragma unroll
+    for (int cc = 0; cc < BS; cc++) {
+        T a = A[(size_t)r0 * BS * BS + (cc * BS + cc) * nb + s];
+        dinv[(long)BS * i + cc] = a != T(0) ? T(1) / a : T(1);
+    }
+}
+
+// ----------------------------------------------------------------- BSR SpMV
+// G lanes per block row.  mode 0: y = A x; 1: y = b - A x; 2: y += A x;
+// 3 (power iteration): y = sigma * Dinv A x with sigma = *scal.
+template <class T, int BR, int BC, int G>
+__global__ void k_bsr_spmv(int nrows, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ A,
+                           const T* __restrict__ x, T* __restrict__ y, const T* __restrict__ b, int mode,
+                           const T* __restrict__ dinv, const double* __restrict__ scal) {
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int gl = threadIdx.x % G;
+    const bool active = gid < nrows;
+    T acc[BR];
+#pragma unroll
+    for (int r = 0; r < BR; r++) acc[r] = T(0);
+    if (active) {
+        const int r0 = rp[gid], nb = rp[gid + 1] - r0;
+        const T* Ar = A + (size_t)r0 * BR * BC;
+        for (int s = gl; s < nb; s += G) {
+            const int j = ci[r0 + s];
+            T xv[BC];
+#pragma unroll
+            for (int d = 0; d < BC; d++) xv[d] = x[(long)BC * j + d];
+#pragma unroll
+            for (int r = 0; r < BR; r++)
+#pragma unroll
+                for (int d = 0; d < BC; d++) acc[r] += Ar[(r * BC + d) * nb + s] * xv[d];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < BR; r++)
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+    if (active && gl < BR) {
+        T v = T(0);
+#pragma unroll
+        for (int r = 0; r < BR; r++)
+            if (r == gl) v = acc[r];
+        const long o = (long)BR * gid + gl;
+        if (mode == 0) y[o] = v;
+        else if (mode == 1) y[o] = b[o] - v;
+        else if (mode == 2) y[o] += v;
+        else y[o] = T(*scal) * dinv[o] * v;
+    }
+}
+
+// fused Chebyshev step on a BSR level: t = A dold; r -= t;
+// dnew = c1 dold + c2 Dinv r; x += dnew (c1, c2 from rho and the step's
+// recurrence numbers cr = rho_k rho_{k-1}, cq = 2 rho_k)
+template <class T, int BS, int G>
+__global__ void k_bsr_cheb(int nrows, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ A,
+                           const T* __restrict__ dold, T* __restrict__ dnew, T* __restrict__ r, T* __restrict__ x,
+                           const T* __restrict__ dinv, const double* __restrict__ rho, double cr, double cq) {
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int gl = threadIdx.x % G;
+    const bool active = gid < nrows;
+    T acc[BS];
+#pragma unroll
+    for (int q = 0; q < BS; q++) acc[q] = T(0);
+    if (active) {
+        const int r0 = rp[gid], nb = rp[gid + 1] - r0;
+        const T* Ar = A + (size_t)r0 * BS * BS;
+        for (int s = gl; s < nb; s += G) {
+            const int j = ci[r0 + s];
+            T xv[BS];
+#pragma unroll
+            for (int d = 0; d < BS; d++) xv[d] = dold[(long)BS * j + d];
+#pragma unroll
+            for (int q = 0; q < BS; q++)
+#pragma unroll
+                for (int d = 0; d < BS; d++) acc[q] += Ar[(q * BS + d) * nb + s] * xv[d];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < BS; q++)
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    if (active && gl < BS) {
+        T v = T(0);
+#pragma unroll
+        for (int q = 0; q < BS; q++)
+            if (q == gl) v = acc[q];
+        const long o = (long)BS * gid + gl;
+        const double delta = 0.5 * (*rho);
+        const T c2 = T(cq / delta);
+        T rn = r[o] - v;
+        T dn = T(cr) * dold[o] + c2 * dinv[o] * rn;
+        r[o] = rn;
+        dnew[o] = dn;
+        x[o] += dn;
+    }
+}
+
+// first Chebyshev step.  zero_init: r = b, d = Dinv b / theta, x = d.
+// otherwise (r already = b - A x): d = Dinv r / theta, x += d.
+template <class T>
+__global__ void k_cheb_first(long n, const T* __restrict__ b, T* __restrict__ r, T* __restrict__ d, T* __restrict__ x,
+                             const T* __restrict__ dinv, const double* __restrict__ rho, int zero_init) {
+    const double theta = 0.6 * (*rho);
+    const T it = T(1.0 / theta);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        if (zero_init) {
+            T bi = b[i];
+            r[i] = bi;
+            T di = dinv[i] * bi * it;
+            d[i] = di;
+            x[i] = di;
+        } else {
+            T di = dinv[i] * r[i] * it;
+            d[i] = di;
+            x[i] += di;
+        }
+    }
+}
+// later Chebyshev step when A d was formed separately (element operator)
+template <class T>
+__global__ void k_cheb_upd(long n, const T* __restrict__ t, T* __restrict__ r, T* __restrict__ d, T* __restrict__ x,
+                           const T* __restrict__ dinv, const double* __restrict__ rho, double cr, double cq) {
+    const double delta = 0.5 * (*rho);
+    const T c2 = T(cq / delta);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        T rn = r[i] - t[i];
+        T dn = T(cr) * d[i] + c2 * dinv[i] * rn;
+        r[i] = rn;
+        d[i] = dn;
+        x[i] += dn;
+    }
+}
+
+// ----------------------------------------------------------------- fixed-pattern SpGEMM
+// C = A * B, blocks A: BR x BK, B: BK x BC, C: BR x BC.  One warp per C row;
+// the row's column ids and an accumulator live in shared memory; lanes walk
+// the blocks of each B row (distinct columns, so no two lanes of one step
+// touch the same accumulator slot) and find their slot by binary search.
+template <class T, int BR, int BK, int BC>
+__global__ void k_spgemm(int nrows, const int* __restrict__ Arp, const int* __restrict__ Aci, const T* __restrict__ A,
+                         const int* __restrict__ Brp, const int* __restrict__ Bci, const T* __restrict__ B,
+                         const int* __restrict__ Crp, const int* __restrict__ Cci, T* __restrict__ C, int maxC) {
+    constexpr int BRK = BR * BK, BKC = BK * BC, BRC = BR * BC;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (blockDim.x >> 5) + wib;
+    if (i >= nrows) return;
+    const size_t accb = ((size_t)maxC * BRC * sizeof(T) + 15) & ~(size_t)15;
+    const size_t per = accb + (((size_t)maxC * sizeof(int) + 15) & ~(size_t)15);
+    unsigned char* base = smem_raw + wib * per;
+    T* acc = reinterpret_cast<T*>(base);
+    int* cci = reinterpret_cast<int*>(base + accb);
+    const int c0 = Crp[i], nC = Crp[i + 1] - c0;
+    for (int s = lane; s < nC; s += 32) cci[s] = Cci[c0 + s];
+    for (int q = lane; q < BRC * maxC; q += 32) acc[q] = T(0);
+    __syncwarp();
+    const int a0 = Arp[i], nA = Arp[i + 1] - a0;
+    for (int a = 0; a < nA; a++) {
+        const int k = Aci[a0 + a];
+        T ab[BRK];
+#pragma unroll
+        for (int e = 0; e < BRK; e++) ab[e] = A[(size_t)a0 * BRK + e * nA + a];
+        const int b0 = Brp[k], nB = Brp[k + 1] - b0;
+        for (int s = lane; s < nB; s += 32) {
+            const int J = Bci[b0 + s];
+            int lo = 0, hi = nC - 1;
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (cci[mid] < J) lo = mid + 1;
+                else hi = mid;
+            }
+            T bb[BKC];
+#pragma unroll
+            for (int e = 0; e < BKC; e++) bb[e] = B[(size_t)b0 * BKC + e * nB + s];
+#pragma unroll
+            for (int r = 0; r < BR; r++)
+#pragma unroll
+                for (int cc = 0; cc < BC; cc++) {
+                    T v = T(0);
+#pragma unroll
+                    for (int m = 0; m < BK; m++) v += ab[r * BK + m] * bb[m * BC + cc];
+                    acc[(r * BC + cc) * maxC + lo] += v;
+                }
+        }
+        __syncwarp();
+    }
+    for (int q = lane; q < BRC * nC; q += 32) {
+        const int e = q / nC, s = q - e * nC;
+        C[(size_t)c0 * BRC + q] = acc[e * maxC + s];
+    }
+}
+
+// P = Pt - (4 / (3 rho)) Dinv (A Pt), pattern of A Pt; Pt's block sits at ptpos
+template <class T, int BS>
+__global__ void k_smooth_p(int nnode, const int* __restrict__ rp, const int* __restrict__ ptpos,
+                           const int* __restrict__ ptrp, const T* __restrict__ Ptv, const T* __restrict__ Tv,
+                           const T* __restrict__ dinv, const double* __restrict__ rho, T* __restrict__ P) {
+    constexpr int BB = BS * 6;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= nnode) return;
+    const T w = T(4.0 / (3.0 * (*rho)));
+    const int r0 = rp[i], nb = rp[i + 1] - r0, pp = ptpos[i];
+    const bool haspt = ptrp[i + 1] > ptrp[i];
+    for (int q = lane; q < BB * nb; q += 32) {
+        const int e = q / nb, s = q - e * nb, r = e / 6;
+        T v = -w * dinv[(long)BS * i + r] * Tv[(size_t)r0 * BB + q];
+        if (haspt && s == pp) v += Ptv[(size_t)ptrp[i] * BB + e];
+        P[(size_t)r0 * BB + q] = v;
+    }
+}
+
+// R = P^T (blocks 6 x BR from BR x 6), one warp per R row
+template <class T, int BR>
+__global__ void k_transpose(int nrows, const int* __restrict__ Rrp, const int* __restrict__ Rci,
+                            const int* __restrict__ perm, const int* __restrict__ Prp, const T* __restrict__ P,
+                            T* __restrict__ R) {
+    constexpr int BB = 6 * BR;
+    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (I >= nrows) return;
+    const int r0 = Rrp[I], nb = Rrp[I + 1] - r0;
+    for (int q = lane; q < BB * nb; q += 32) {
+        const int e = q / nb, s = q - e * nb;
+        const int a = e / BR, b = e % BR;
+        const int j = Rci[r0 + s], pq = perm[r0 + s];
+        const int pb = Prp[j], nbp = Prp[j + 1] - pb;
+        R[(size_t)r0 * BB + q] = P[(size_t)pb * BB + (b * 6 + a) * nbp + (pq - pb)];
+    }
+}
+
+// ----------------------------------------------------------------- power iteration / reductions
+template <class T>
+__global__ void k_dot2(long n, const T* __restrict__ v, const T* __restrict__ w, const double* __restrict__ scal,
+                       double* __restrict__ part) {
+    __shared__ double sm[64];
+    double s[2] = {0.0, 0.0};
+    const double sc = *scal;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double wi = (double)w[i];
+        s[0] += sc * (double)v[i] * wi;
+        s[1] += wi * wi;
+    }
+    block_sum<2>(s, sm);
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = s[0]; part[2 * blockIdx.x + 1] = s[1]; }
+}
+__global__ void k_power_final(int nb, const double* __restrict__ part, double* __restrict__ lam,
+                              double* __restrict__ scal) {
+    __shared__ double sm[64];
+    double s[2] = {0.0, 0.0};
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) { s[0] += part[2 * i]; s[1] += part[2 * i + 1]; }
+    block_sum<2>(s, sm);
+    if (threadIdx.x == 0) {
+        *lam = s[0];
+        *scal = s[1] > 0.0 ? 1.0 / sqrt(s[1]) : 1.0;
+    }
+}
+template <class T>
+__global__ void k_power_seed(long n, T* __restrict__ v, double* __restrict__ scal) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        v[i] = T(1.0 + 0.1 * (double)((i * 7919) % 13) / 13.0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *scal = 1.0 / sqrt((double)n * 1.1);
+}
+
+// ----------------------------------------------------------------- coarsest level
+template <class T, int BS>
+__global__ void k_bsr_to_dense(int nnode, const int* __restrict__ rp, const int* __restrict__ ci,
+                               const T* __restrict__ A, double* __restrict__ M, int n) {
+    const int i = blockIdx.x;
+    if (i >= nnode) return;
+    const int r0 = rp[i], nb = rp[i + 1] - r0;
+    for (int q = threadIdx.x; q < BS * BS * nb; q += blockDim.x) {
+        const int e = q / nb, s = q - e * nb, r = e / BS, cc = e % BS;
+        const int j = ci[r0 + s];
+        M[(size_t)(BS * i + r) * (2 * n) + BS * j + cc] = (double)A[(size_t)r0 * BS * BS + q];
+    }
+}
+// [A | I] -> [I | A^-1] by Gauss-Jordan with partial pivoting, one CTA.
+// A zero pivot (singular coarse operator) is replaced by 1 and flagged.
+__global__ void k_gauss_jordan(int n, double* __restrict__ M, double* __restrict__ inv, int* __restrict__ flag) {
+    extern __shared__ double fk[];  // n column factors
+    __shared__ double s_val[32];
+    __shared__ int s_idx[32];
+    __shared__ double s_piv;
+    __shared__ int s_prow;
+    const int ld = 2 * n, tid = threadIdx.x, nt = blockDim.x;
+    for (int q = tid; q < n; q += nt) M[(size_t)q * ld + n + q] = 1.0;
+    __syncthreads();
+    for (int k = 0; k < n; k++) {
+        double best = -1.0;
+        int bi = k;
+        for (int i = k + tid; i < n; i += nt) {
+            double v = fabs(M[(size_t)i * ld + k]);
+            if (v > best) { best = v; bi = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if ((tid & 31) == 0) { s_val[tid >> 5] = best; s_idx[tid >> 5] = bi; }
+        __syncthreads();
+        if (tid == 0) {
+            double bv = -1.0;
+            int bidx = k;
+            for (int w = 0; w < (nt + 31) / 32; w++)
+                if (s_val[w] > bv || (s_val[w] == bv && s_idx[w] < bidx)) { bv = s_val[w]; bidx = s_idx[w]; }
+            s_prow = bidx;
+        }
+        __syncthreads();
+        const int pr = s_prow;
+        if (pr != k)
+            for (int j = tid; j < ld; j += nt) {
+                double t = M[(size_t)k * ld + j];
+                M[(size_t)k * ld + j] = M[(size_t)pr * ld + j];
+                M[(size_t)pr * ld + j] = t;
+            }
+        __syncthreads();
+        if (tid == 0) {
+            double pv = M[(size_t)k * ld + k];
+            if (pv == 0.0 || !isfinite(pv)) { pv = 1.0; *flag = 1; }
+            s_piv = pv;
+        }
+        __syncthreads();
+        const double ip = 1.0 / s_piv;
+        for (int j = tid; j < ld; j += nt) M[(size_t)k * ld + j] *= ip;
+        for (int i = tid; i < n; i += nt) fk[i] = M[(size_t)i * ld + k];
+        __syncthreads();
+        for (long q = tid; q < (long)n * ld; q += nt) {
+            const int i = (int)(q / ld), j = (int)(q % ld);
+            if (i != k) M[q] -= fk[i] * M[(size_t)k * ld + j];
+        }
+        __syncthreads();
+    }
+    for (long q = tid; q < (long)n * n; q += nt) {
+        const int i = (int)(q / n), j = (int)(q % n);
+        inv[q] = M[(size_t)i * ld + n + j];
+    }
+}
+template <class T>
+__global__ void k_dense_apply(int n, const double* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += inv[(size_t)i * n + j] * (double)b[j];
+    s = warp_sum(s);
+    if (lane == 0) x[i] = T(s);
+}
+
+template <class TI, class TO>
+__global__ void k_convert(long n, const TI* __restrict__ a, TO* __restrict__ b) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = TO(a[i]);
+}
+
+// ----------------------------------------------------------------- host orchestration
+template <class T>
+static AmgVals<T>& vals(Ctx& c);
+template <>
+AmgVals<double>& vals<double>(Ctx& c) { return c.v64; }
+template <>
+AmgVals<float>& vals<float>(Ctx& c) { return c.v32; }
+
+template <class T>
+static int alloc_vals(Ctx& c) {
+    AmgVals<T>& v = vals<T>(c);
+    if (v.allocated) return 0;
+    for (int l = 0; l < c.nlev; l++) {
+        AmgDevLevel& D = c.dl[l];
+        const int bs = D.bs;
+        TRET(v.A[l].alloc((size_t)D.A.nnzb * bs * bs));
+        TRET(v.dinv[l].alloc(D.ndof));
+        TRET(v.x[l].alloc(D.ndof));
+        TRET(v.b[l].alloc(D.ndof));
+        TRET(v.r[l].alloc(D.ndof));
+        TRET(v.d[l].alloc(D.ndof));
+        TRET(v.d2[l].alloc(D.ndof));
+        TRET(v.t[l].alloc(D.ndof));
+        TRET(v.pv[l].alloc(D.ndof));
+        TRET(v.pw[l].alloc(D.ndof));
+        if (l + 1 < c.nlev) {
+            TRET(v.P[l].alloc((size_t)D.P.nnzb * bs * 6));
+            TRET(v.T_[l].alloc((size_t)D.P.nnzb * bs * 6));
+            TRET(v.AP[l].alloc((size_t)D.AP.nnzb * bs * 6));
+            TRET(v.R[l].alloc((size_t)D.R.nnzb * bs * 6));
+        }
+        k_power_seed<T><<<grid_for(D.ndof, 256), 256, 0, c.s>>>(D.ndof, v.pv[l].p, c.rho.p + kMaxLevels + l);
+    }
+    TCK(cudaGetLastError());
+    v.allocated = true;
+    return 0;
+}
+
+int amg_alloc(Ctx& c) {
+    if (!c.rho.p) {
+        TRET(c.rho.alloc(4 * kMaxLevels));
+        TRET(c.rho.zero(c.s));
+    }
+    return 0;
+}
+
+template <class T>
+static const T* pt_vals(Ctx& c, int l) {
+    if (std::is_same<T, double>::value) return (const T*)c.dl[l].Pt64c.p;
+    return (const T*)c.dl[l].Pt32c.p;
+}
+
+template <int BR, int BK, int BC, class T>
+static int spgemm(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp, const T* B, const DevPattern& Cp,
+                  T* C) {
+    const size_t mc = (size_t)std::max(Cp.maxrow, 1);
+    const size_t per = ((mc * BR * BC * sizeof(T) + 15) & ~(size_t)15) + ((mc * sizeof(int) + 15) & ~(size_t)15);
+    int warps = (int)std::min<size_t>(8, std::max<size_t>(1, (200 * 1024) / per));
+    const size_t smem = per * warps;
+    if (smem > 227 * 1024) { set_error("SpGEMM row too long for shared memory (%d blocks)", Cp.maxrow); return TOPO_ERR_UNSUPPORTED; }
+    auto kern = k_spgemm<T, BR, BK, BC>;
+    TCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = (Cp.nrows + warps - 1) / warps;
+    kern<<<grid, warps * 32, smem, c.s>>>(Cp.nrows, Ap.rp.p, Ap.ci.p, A, Bp.rp.p, Bp.ci.p, B, Cp.rp.p, Cp.ci.p, C,
+                                          std::max(Cp.maxrow, 1));
+    TCK(cudaGetLastError());
+    return 0;
+}
+
+template <class T, int BR, int BC>
+static int spmv(Ctx& c, const DevPattern& Ap, const T* A, const T* x, T* y, const T* b, int mode, const T* dinv = nullptr,
+                const double* scal = nullptr) {
+    const long nrows = Ap.nrows;
+    const double avg = nrows ? (double)Ap.nnzb / nrows : 1.0;
+    if (avg <= 6.0) {
+        constexpr int G = 8;
+        k_bsr_spmv<T, BR, BC, G><<<(int)((nrows * G + 255) / 256), 256, 0, c.s>>>(
+            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal);
+    } else if (avg <= 20.0) {
+        constexpr int G = 16;
+        k_bsr_spmv<T, BR, BC, G><<<(int)((nrows * G + 255) / 256), 256, 0, c.s>>>(
+            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal);
+    } else {
+        constexpr int G = 32;
+        k_bsr_spmv<T, BR, BC, G><<<(int)((nrows * G + 255) / 256), 256, 0, c.s>>>(
+            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal);
+    }
+    TCK(cudaGetLastError());
+    return 0;
+}
+
+template <class T>
+static int level_spmv(Ctx& c, int l, const T* x, T* y, const T* b, int mode, const T* dinv = nullptr,
+                      const double* scal = nullptr) {
+    AmgVals<T>& v = vals<T>(c);
+    if (c.dl[l].bs == 3) return spmv<T, 3, 3>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal);
+    return spmv<T, 6, 6>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal);
+}
+
+template <class T>
+static int estimate_rho(Ctx& c, int l, int iters) {
+    AmgVals<T>& v = vals<T>(c);
+    AmgDevLevel& D = c.dl[l];
+    double* lam = c.rho.p + l;
+    double* scal = c.rho.p + kMaxLevels + l;
+    const int nb = grid_for(D.ndof, 256, 1024);
+    if ((long)c.red.n < 2L * nb) TRET(c.red.alloc(std::max<long>(2L * nb, 4096)));
+    for (int it = 0; it < iters; it++) {
+        // w = sigma Dinv A v with sigma = 1/||v||; lam = (sigma v).w; sigma' = 1/||w||
+        TRET(level_spmv<T>(c, l, v.pv[l].p, v.pw[l].p, (const T*)nullptr, 3, v.dinv[l].p, scal));
+        k_dot2<T><<<nb, 256, 0, c.s>>>(D.ndof, v.pv[l].p, v.pw[l].p, scal, c.red.p);
+        k_power_final<<<1, 1024, 0, c.s>>>(nb, c.red.p, lam, scal);
+        std::swap(v.pv[l], v.pw[l]);
+    }
+    TCK(cudaGetLastError());
+    return 0;
+}
+
+template <class T>
+static int numeric(Ctx& c) {
+    TRET(alloc_vals<T>(c));
+    AmgVals<T>& v = vals<T>(c);
+    const T* ke = std::is_same<T, double>::value ? (const T*)c.ke64.p : (const T*)c.ke32.p;
+    const T* Ee = std::is_same<T, double>::value ? (const T*)c.Ee64.p : (const T*)c.Ee32.p;
+    // level-0 assembly
+    {
+        AmgDevLevel& D = c.dl[0];
+        const int wpb = 4;
+        const size_t smem = (size_t)wpb * c.maxdeg * 9 * sizeof(T);
+        const int grid = (c.nn + wpb - 1) / wpb;
+        if (c.nen == 8) {
+            auto k = k_assemble_A0<T, 8>;
+            TCK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, ke, Ee, D.A.rp.p, D.A.ci.p,
+                                              c.dof_fixed.p, v.A[0].p, c.maxdeg);
+        } else {
+            auto k = k_assemble_A0<T, 4>;
+            TCK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, ke, Ee, D.A.rp.p, D.A.ci.p,
+                                              c.dof_fixed.p, v.A[0].p, c.maxdeg);
+        }
+        TCK(cudaGetLastError());
+    }
+    for (int l = 0; l < c.nlev; l++) {
+        AmgDevLevel& D = c.dl[l];
+        if (D.bs == 3)
+            k_diag_inv<T, 3><<<grid_for(D.nnode, 256, 1 << 20), 256, 0, c.s>>>(D.nnode, D.A.rp.p, D.diagpos.p, v.A[l].p,
+                                                                           v.dinv[l].p);
+        else
+            k_diag_inv<T, 6><<<grid_for(D.nnode, 256, 1 << 20), 256, 0, c.s>>>(D.nnode, D.A.rp.p, D.diagpos.p, v.A[l].p,
+                                                                           v.dinv[l].p);
+        TCK(cudaGetLastError());
+        if (l == c.nlev - 1) break;
+        TRET(estimate_rho<T>(c, l, l == 0 ? 6 : 10));
+        AmgDevLevel& N = c.dl[l + 1];
+        // T = A Pt ; P = Pt - w Dinv T
+        const T* ptv = pt_vals<T>(c, l);
+        if (D.bs == 3) {
+            if (c.p.amg_smooth_p) {
+                TRET((spgemm<3, 3, 6, T>(c, D.A, v.A[l].p, D.Ptp, ptv, D.P, v.T_[l].p)));
+                k_smooth_p<T, 3><<<(D.nnode * 32 + 255) / 256, 256, 0, c.s>>>(
+                    D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p);
+            } else {
+                TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 18, cudaMemcpyDeviceToDevice, c.s));
+            }
+            TRET((spgemm<3, 3, 6, T>(c, D.A, v.A[l].p, D.P, v.P[l].p, D.AP, v.AP[l].p)));
+            k_transpose<T, 3><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
+                                                                             D.P.rp.p, v.P[l].p, v.R[l].p);
+            TRET((spgemm<6, 3, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p)));
+        } else {
+            if (c.p.amg_smooth_p) {
+                TRET((spgemm<6, 6, 6, T>(c, D.A, v.A[l].p, D.Ptp, ptv, D.P, v.T_[l].p)));
+                k_smooth_p<T, 6><<<(D.nnode * 32 + 255) / 256, 256, 0, c.s>>>(
+                    D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p);
+            } else {
+                TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 36, cudaMemcpyDeviceToDevice, c.s));
+            }
+            TRET((spgemm<6, 6, 6, T>(c, D.A, v.A[l].p, D.P, v.P[l].p, D.AP, v.AP[l].p)));
+            k_transpose<T, 6><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
+                                                                             D.P.rp.p, v.P[l].p, v.R[l].p);
+            TRET((spgemm<6, 6, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p)));
+        }
+        TCK(cudaGetLastError());
+    }
+    // coarsest: dense FP64 inverse
+    {
+        const int L = c.nlev - 1;
+        AmgDevLevel& D = c.dl[L];
+        const int n = D.ndof;
+        if (!c.cinv.p || (long)c.cinv.n < (long)n * n) {
+            TRET(c.cinv.alloc((size_t)n * n));
+            TRET(c.cA.alloc((size_t)n * 2 * n));
+        }
+        TCK(cudaMemsetAsync(c.cA.p, 0, sizeof(double) * (size_t)n * 2 * n, c.s));
+        if (D.bs == 3)
+            k_bsr_to_dense<T, 3><<<D.nnode, 128, 0, c.s>>>(D.nnode, D.A.rp.p, D.A.ci.p, v.A[L].p, c.cA.p, n);
+        else
+            k_bsr_to_dense<T, 6><<<D.nnode, 128, 0, c.s>>>(D.nnode, D.A.rp.p, D.A.ci.p, v.A[L].p, c.cA.p, n);
+        const size_t sm = sizeof(double) * (size_t)n;
+        if (sm > 48 * 1024) TCK(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_gauss_jordan<<<1, 1024, sm, c.s>>>(n, c.cA.p, c.cinv.p, reinterpret_cast<int*>(c.rho.p + 3 * kMaxLevels));
+        TCK(cudaGetLastError());
+    }
+    return 0;
+}
+
+// Chebyshev recurrence numbers for sigma = theta/delta = 1.2
+static void cheb_coeffs(int deg, double* cr, double* cq) {
+    const double sigma = 1.2;
+    double rho_prev = 1.0 / sigma;
+    for (int k = 1; k < deg; k++) {
+        double rk = 1.0 / (2.0 * sigma - rho_prev);
+        cr[k] = rk * rho_prev;
+        cq[k] = 2.0 * rk;
+        rho_prev = rk;
+    }
+}
+
+template <class T>
+static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
+    AmgVals<T>& v = vals<T>(c);
+    AmgDevLevel& D = c.dl[l];
+    const long n = D.ndof;
+    const int deg = std::max(1, c.p.cheb_degree);
+    double cr[16] = {0}, cq[16] = {0};
+    cheb_coeffs(std::min(deg, 16), cr, cq);
+    const double* rho = c.rho.p + l;
+    const bool matfree = (l == 0) && c.p.fine_smoother_matfree;
+    if (!zero_init) {
+        // r = b - A x
+        if (matfree) {
+            if (std::is_same<T, float>::value) TRET(kmatvec32(c, (const float*)x, (float*)v.r[l].p, (const float*)b));
+            else TRET(kmatvec64r(c, (const double*)x, (double*)v.r[l].p, (const double*)b));
+        } else {
+            TRET(level_spmv<T>(c, l, x, v.r[l].p, b, 1));
+        }
+    }
+    k_cheb_first<T><<<grid_for(n, 256), 256, 0, c.s>>>(n, b, v.r[l].p, v.d[l].p, x, v.dinv[l].p, rho, zero_init ? 1 : 0);
+    T* dcur = v.d[l].p;
+    T* dnxt = v.d2[l].p;
+    for (int k = 1; k < deg && k < 16; k++) {
+        if (matfree) {
+            if (std::is_same<T, float>::value) TRET(kmatvec32(c, (const float*)dcur, (float*)v.t[l].p, nullptr));
+            else TRET(kmatvec64r(c, (const double*)dcur, (double*)v.t[l].p, nullptr));
+            k_cheb_upd<T><<<grid_for(n, 256), 256, 0, c.s>>>(n, v.t[l].p, v.r[l].p, dcur, x, v.dinv[l].p, rho, cr[k], cq[k]);
+        } else {
+            const int nrows = D.nnode;
+            if (D.bs == 3) {
+                constexpr int G = 32;
+                k_bsr_cheb<T, 3, G><<<(nrows * G + 255) / 256, 256, 0, c.s>>>(nrows, D.A.rp.p, D.A.ci.p, v.A[l].p, dcur,
+                                                                            dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr[k],
+                                                                            cq[k]);
+            } else {
+                constexpr int G = 32;
+                k_bsr_cheb<T, 6, G><<<(nrows * G + 255) / 256, 256, 0, c.s>>>(nrows, D.A.rp.p, D.A.ci.p, v.A[l].p, dcur,
+                                                                            dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr[k],
+                                                                            cq[k]);
+            }
+            std::swap(dcur, dnxt);
+        }
+        TCK(cudaGetLastError());
+    }
+    return 0;
+}
+
+template <class T>
+static int vcycle(Ctx& c, const T* b0, T* x0) {
+    AmgVals<T>& v = vals<T>(c);
+    const int L = c.nlev - 1;
+    const T* bl[kMaxLevels];
+    T* xl[kMaxLevels];
+    for (int l = 0; l <= L; l++) { bl[l] = v.b[l].p; xl[l] = v.x[l].p; }
+    bl[0] = b0;
+    xl[0] = x0;
+    for (int l = 0; l < L; l++) {
+        AmgDevLevel& D = c.dl[l];
+        TRET(smooth<T>(c, l, bl[l], xl[l], true));
+        if (l == 0 && c.p.fine_smoother_matfree) {
+            if (std::is_same<T, float>::value) TRET(kmatvec32(c, (const float*)xl[0], (float*)v.t[0].p, (const float*)bl[0]));
+            else TRET(kmatvec64r(c, (const double*)xl[0], (double*)v.t[0].p, (const double*)bl[0]));
+        } else {
+            TRET(level_spmv<T>(c, l, xl[l], v.t[l].p, bl[l], 1));
+        }
+        if (D.bs == 3) TRET((spmv<T, 6, 3>(c, D.R, v.R[l].p, v.t[l].p, v.b[l + 1].p, nullptr, 0)));
+        else TRET((spmv<T, 6, 6>(c, D.R, v.R[l].p, v.t[l].p, v.b[l + 1].p, nullptr, 0)));
+    }
+    {
+        const int n = c.dl[L].ndof;
+        k_dense_apply<T><<<(n * 32 + 255) / 256, 256, 0, c.s>>>(n, c.cinv.p, v.b[L].p, v.x[L].p);
+        TCK(cudaGetLastError());
+    }
+    for (int l = L - 1; l >= 0; l--) {
+        AmgDevLevel& D = c.dl[l];
+        if (D.bs == 3) TRET((spmv<T, 3, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 2)));
+        else TRET((spmv<T, 6, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 2)));
+        TRET(smooth<T>(c, l, bl[l], xl[l], false));
+    }
+    return 0;
+}
+
+int amg_numeric(Ctx& c) {
+    TRET(amg_alloc(c));
+    if (c.p.precision == TOPO_PREC_MIXED) return numeric<float>(c);
+    return numeric<double>(c);
+}
+
+int amg_vcycle64(Ctx& c, const double* b, double* x) { return vcycle<double>(c, b, x); }
+
+int amg_vcycle32(Ctx& c, const double* b64, float* x) {
+    AmgVals<float>& v = c.v32;
+    const long n = c.dl[0].ndof;
+    k_convert<double, float><<<grid_for(n, 256), 256, 0, c.s>>>(n, b64, v.b[0].p);
+    TCK(cudaGetLastError());
+    // level-0 rhs lives in v.b[0]; the smoother keeps b intact
+    return vcycle<float>(c, v.b[0].p, x);
+}
+
+}  // namespace topo

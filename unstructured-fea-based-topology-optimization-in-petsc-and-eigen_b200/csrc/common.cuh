@@ -1,0 +1,198 @@
+// common.cuh -- shared device/host helpers for the sm_100a topology-optimisation
+// library: error plumbing, device buffers, deterministic block reductions and a
+// bounded grid barrier for cooperative (persistent) kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/topo.h"
+
+namespace topo {
+
+// ----------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* file, int line);
+
+#define TCK(...)                                                         \
+    do {                                                                 \
+        cudaError_t e_ = (__VA_ARGS__);                                  \
+        if (e_ != cudaSuccess) return ::topo::cuda_fail(e_, __FILE__, __LINE__); \
+    } while (0)
+#define TRET(...)                     \
+    do {                              \
+        int r_ = (__VA_ARGS__);       \
+        if (r_ < 0) return r_;        \
+    } while (0)
+
+// ----------------------------------------------------------------- buffers
+// Owning device allocation (cudaMalloc); never copied, only moved.
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept {
+        if (this != &o) { reset(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DBuf() { reset(); }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    int alloc(size_t count) {
+        reset();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+            return TOPO_ERR_OOM;
+        }
+        n = count;
+        return 0;
+    }
+    int upload(const T* h, size_t count, cudaStream_t s) {
+        TRET(alloc(count));
+        if (count) TCK(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+        return 0;
+    }
+    int upload(const std::vector<T>& v, cudaStream_t s) { return upload(v.data(), v.size(), s); }
+    int zero(cudaStream_t s) {
+        if (p) TCK(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+        return 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// pinned host scratch for small device->host readbacks
+struct PinnedScalars {
+    double* h = nullptr;
+    size_t n = 0;
+    int alloc(size_t count) {
+        if (h) cudaFreeHost(h);
+        h = nullptr;
+        cudaError_t e = cudaMallocHost(&h, count * sizeof(double));
+        if (e != cudaSuccess) { cudaGetLastError(); h = nullptr; set_error("cudaMallocHost failed"); return TOPO_ERR_OOM; }
+        n = count;
+        return 0;
+    }
+    ~PinnedScalars() { if (h) cudaFreeHost(h); }
+};
+
+#ifdef __CUDACC__
+// ----------------------------------------------------------------- device helpers
+constexpr int kWarp = 32;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Deterministic block reduction of NV sums; result valid in thread 0.
+// smem must hold NV * 32 doubles.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* smem) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; k++) smem[k * 32 + wid] = v[k];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double t = lane < nw ? smem[k * 32 + lane] : 0.0;
+            v[k] = warp_sum(t);
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double block_max(double v, double* smem) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    v = warp_max(v);
+    __syncthreads();
+    if (lane == 0) smem[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        double t = lane < nw ? smem[lane] : 0.0;
+        v = warp_max(t);
+    }
+    __syncthreads();
+    return v;
+}
+
+// Bounded grid barrier for kernels launched with cudaLaunchCooperativeKernel
+// (co-residency guaranteed by the launch).  Every wait polls at most
+// kBarrierSpin times; on expiry it raises *err and returns false so the
+// kernel can unwind instead of hanging the device.
+constexpr unsigned kBarrierSpin = 1u << 24;
+
+struct GridBarrier {
+    unsigned* count;   // arrivals in the current generation
+    unsigned* gen;     // generation counter
+    int* err;          // set to 1 on timeout
+};
+
+__device__ __forceinline__ bool grid_sync(const GridBarrier& b) {
+    __syncthreads();
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        s_ok = 1;
+        volatile unsigned* vgen = b.gen;
+        unsigned g = *vgen;
+        __threadfence();
+        unsigned arrived = atomicAdd(b.count, 1u) + 1u;
+        if (arrived == gridDim.x) {
+            *b.count = 0;
+            __threadfence();
+            atomicAdd(b.gen, 1u);
+        } else {
+            unsigned spins = 0;
+            while (*vgen == g) {
+                if (++spins > kBarrierSpin || *(volatile int*)b.err) {
+                    atomicExch(b.err, 1);
+                    s_ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+#endif  // __CUDACC__
+
+inline int grid_for(long n, int block, int max_blocks = 148 * 64) {
+    long g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > max_blocks) g = max_blocks;
+    return (int)g;
+}
+
+}  // namespace topo

@@ -1,0 +1,205 @@
+// ctx.h -- internal state of one topology-optimisation job and the internal
+// (C++) interface between the host-side builders and the device stages.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace topo {
+
+constexpr int kMaxLevels = 8;
+constexpr int kMaxM = 4;        // constraints supported by the device MMA
+constexpr int kMaxCases = 16;   // load cases of the block solver
+
+// Block-sparse pattern (host).  Values of the device copies are stored
+// "slot-interleaved": entry e (0..BB-1) of the block in slot s of row i sits
+// at val[rp[i]*BB + e*nb_i + s] with nb_i = rp[i+1]-rp[i], so a warp whose
+// lanes walk the slots of one row reads each entry coalesced.
+struct Pattern {
+    int nrows = 0, ncols = 0;
+    std::vector<int> rp, ci;
+    long nnzb() const { return rp.empty() ? 0 : rp.back(); }
+    int max_row() const {
+        int m = 0;
+        for (int i = 0; i < nrows; i++) m = std::max(m, rp[i + 1] - rp[i]);
+        return m;
+    }
+};
+
+struct DevPattern {
+    int nrows = 0, ncols = 0, maxrow = 0;
+    long nnzb = 0;
+    DBuf<int> rp, ci;
+    int upload(const Pattern& p, cudaStream_t s) {
+        nrows = p.nrows; ncols = p.ncols; nnzb = p.nnzb(); maxrow = p.max_row();
+        TRET(rp.upload(p.rp, s));
+        TRET(ci.upload(p.ci, s));
+        return 0;
+    }
+};
+
+// Host-built, geometry-only hierarchy (aggregates, tentative prolongators,
+// patterns of every Galerkin product).  Built once per mesh.
+struct AmgHostLevel {
+    int bs = 3;                 // DOFs per node at this level (3, then 6)
+    int nnode = 0;
+    Pattern A;                  // bs x bs blocks (level 0: mesh node graph)
+    std::vector<int> agg;       // node -> aggregate, -1 none (excluded)
+    int nagg = 0;
+    std::vector<double> Pt;     // nnode x bs x 6 tentative prolongator blocks
+    Pattern P;                  // pattern of A * Pt (= pattern of smoothed P)
+    std::vector<int> ptpos;     // slot of agg(i) in P row i, -1 none
+    Pattern AP;                 // pattern of A * P
+    Pattern R;                  // P^T
+    std::vector<int> rperm;     // R block -> P block index
+};
+
+struct AmgDevLevel {
+    int bs = 3, nnode = 0, ndof = 0, nagg = 0;
+    DevPattern A, P, AP, R;
+    DBuf<int> diagpos;          // slot of the diagonal block in each A row
+    DBuf<int> ptpos, rperm;
+    DevPattern Ptp;             // tentative prolongator: one block per aggregated node
+    DBuf<double> Pt64c;         // its bs x 6 blocks (compact, FP64)
+    DBuf<float> Pt32c;          // (FP32 copy for the mixed form)
+};
+
+// numeric values of the hierarchy in precision T
+template <class T>
+struct AmgVals {
+    DBuf<T> A[kMaxLevels], P[kMaxLevels], T_[kMaxLevels], AP[kMaxLevels], R[kMaxLevels];
+    DBuf<T> dinv[kMaxLevels];
+    DBuf<T> x[kMaxLevels], b[kMaxLevels], r[kMaxLevels], d[kMaxLevels], d2[kMaxLevels], t[kMaxLevels];
+    DBuf<T> pv[kMaxLevels], pw[kMaxLevels];   // power-iteration vectors (warm start)
+    bool allocated = false;
+};
+
+struct Ctx {
+    topo_params p{};
+    cudaStream_t s = nullptr;
+    bool own_stream = false;
+
+    // ---- mesh
+    int nen = 8, nn = 0, ne = 0, ntiles = 0, ndof = 0, nde = 24, npk = 300, nkf = 36;
+    int ncases = 1;
+    std::vector<double> vertex_h;
+    std::vector<int> elem_h, fixed_h;
+    std::vector<unsigned char> dof_fixed_h;
+    DBuf<int> conn;             // AoSoA [tile][nen][32]
+    DBuf<int> elem;             // [ne][nen]
+    DBuf<double> vertex;        // [nn][3]
+    DBuf<uint32_t> emask;       // fixed local DOFs per element (bit c*nen+l)
+    DBuf<unsigned char> dof_fixed;
+    DBuf<int> fixed;
+    DBuf<double> ke64;          // AoSoA [tile][npk][32], E = 1
+    DBuf<float> ke32;
+    DBuf<double> vol;
+    double TV = 0.0;
+    DBuf<double> F;             // [ncases][ndof]
+    DBuf<int> n2e_ptr, n2e;     // node -> element*nen + local
+    DBuf<uint16_t> bpos;        // [ne][nen][nen] slot of node q in node p's row
+    int maxdeg = 0;
+
+    // ---- filter
+    DBuf<double> kf;            // AoSoA [tile][nkf][32]
+    DBuf<double> tf;            // AoSoA [tile][nen][32]
+    DBuf<double> fdiag_inv, RX, TX, fr, fz, fp, fw;
+
+    // ---- AMG
+    std::vector<AmgHostLevel> hl;
+    AmgDevLevel dl[kMaxLevels];
+    int nlev = 0;
+    DBuf<double> cinv;          // coarsest inverse (FP64, ncoarse^2)
+    DBuf<double> cA;            // coarsest dense matrix scratch
+    AmgVals<double> v64;
+    AmgVals<float> v32;
+    DBuf<double> rho;           // [kMaxLevels] spectral estimates of D^-1 A
+    bool amg_ready = false;
+
+    // ---- displacement solve
+    DBuf<double> Ee64;          // SIMP moduli of the current xphys
+    DBuf<float> Ee32;
+    DBuf<double> U;             // [ncases][ndof]
+    DBuf<double> uku;           // per-element u'Ke u summed over cases
+    DBuf<double> V;             // Krylov basis (restart+1) x ndof
+    DBuf<double> Z64;           // preconditioned directions (FP64 form)
+    DBuf<float> Z32;            // (mixed form)
+    DBuf<double> w, wtmp;
+    DBuf<double> red;           // reduction partials
+    DBuf<double> dsc;           // device scalars
+    PinnedScalars hsc;          // pinned host mirror for readbacks
+
+    // ---- MMA (MMA.cpp state)
+    int mma_k = 0;
+    double asyminit = 0.5, asymdec = 0.7, asyminc = 1.2;
+    int constraint_mod = 0, robust_type = 0;
+    std::vector<double> a, c, d;
+    DBuf<double> L, Uas, alpha, beta, p0, q0, pij, qij, xo1, xo2;
+    DBuf<double> mma_scal;      // lam, mu, y, z, b ... device side
+    DBuf<unsigned> bar;         // grid barrier words
+    DBuf<int> bar_err;
+
+    // ---- driver design vectors (OptPara)
+    DBuf<double> X, Xold, XF, XP, dfdx, dgdx, xmin, xmax;
+    int itr = 0;
+    double ch = 1.0, beta_proj = 1.0, beta_tmp = 1.0;
+    bool opt_ready = false;
+
+    topo_solve_info info{};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+// ---- host builders (setup.cpp)
+int build_mesh(Ctx& c, const double* vertex, const int32_t* element, int n_fixed, const int32_t* fixed,
+               int n_cases, const int32_t* case_ptr, const int32_t* load_dofs, const double* load_vals);
+int build_amg_host(Ctx& c);
+int aggregate_graph(int nn, const std::vector<int>& rp, const std::vector<int>& ci,
+                    const unsigned char* excl, std::vector<int>& agg);
+Pattern sym_spgemm(const Pattern& A, const Pattern& B);
+Pattern sym_transpose(const Pattern& A, std::vector<int>& perm);
+
+// ---- device stages
+int elem_setup(Ctx& c);                                            // kernels_elem.cu
+int kmatvec(Ctx& c, const double* Ee, const double* u, double* y, int ncase = 1);
+int kmatvec_f32in(Ctx& c, const double* Ee, const float* u, double* y);
+int compute_moduli(Ctx& c, const double* xphys);
+int fem_sensitivities(Ctx& c, const double* xphys, double* dfdx, double* dgdx);  // fx,gx -> dsc[0],[1]
+int filter_tf(Ctx& c, const double* x, double* tx);
+int filter_kf(Ctx& c, const double* r, double* y);
+int filter_tfxT(Ctx& c, const double* rx, double* xf, bool clamp, double xmin);
+int von_mises(Ctx& c, const double* xphys, double* vms);
+
+int amg_alloc(Ctx& c);                                             // amg.cu
+int amg_numeric(Ctx& c);
+int amg_vcycle64(Ctx& c, const double* b, double* x);
+int amg_vcycle32(Ctx& c, const double* b64, float* x);
+
+int fem_solve(Ctx& c, const double* xphys, double* u);             // solver.cu
+int filter_cg(Ctx& c, const double* b, double* x, int* its);
+int dev_dot(Ctx& c, const double* a, const double* b, long n, double* out_dev);
+int finalize_sum(Ctx& c, const double* partials, int nparts, int nv, double* out_dev);
+
+int mma_alloc(Ctx& c);                                             // mma.cu
+int mma_movelimit(Ctx& c, double Xmin, double Xmax, double movlim, const double* x, double* xmin, double* xmax);
+int mma_update(Ctx& c, double* x, const double* dfdx, const double* gx_dev, const double* dgdx,
+               const double* xmin, const double* xmax);
+int mma_design_change(Ctx& c, const double* x, double* xold, double* ch_dev);
+int mma_kkt(Ctx& c, const double* x, const double* dfdx, const double* gx_dev, const double* dgdx,
+            const double* xmin, const double* xmax, double* n2, double* ninf);
+
+// device scalar slots in Ctx::dsc
+enum DscSlot {
+    DS_FX = 0, DS_GX = 1,          // .. DS_GX + kMaxM - 1
+    DS_CH = 8, DS_TMP = 9,
+    DS_CG = 16,                    // CG scratch (16..31)
+    DS_GM = 32,                    // FGMRES column (32..127)
+    DS_KKT = 128,
+    DS_COUNT = 160
+};
+
+}  // namespace topo

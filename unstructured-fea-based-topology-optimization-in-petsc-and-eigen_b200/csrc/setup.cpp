@@ -1,0 +1,410 @@
+// setup.cpp -- host-side builders run once per mesh: validation, device
+// layouts of the connectivity (AoSoA tiles of 32 elements), boundary masks,
+// node graph, and the geometry-only part of the smoothed-aggregation AMG
+// hierarchy (aggregates, tentative prolongators, symbolic Galerkin patterns).
+// Only the numeric Galerkin products are recomputed per design iteration
+// (on the device).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <mutex>
+
+#include "ctx.h"
+
+namespace topo {
+
+// ----------------------------------------------------------------- errors
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+const char* last_error() { return g_err.c_str(); }
+
+int cuda_fail(cudaError_t e, const char* file, int line) {
+    set_error("CUDA error %s (%s) at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e), file, line);
+    return e == cudaErrorMemoryAllocation ? TOPO_ERR_OOM : TOPO_ERR_CUDA;
+}
+
+// ----------------------------------------------------------------- patterns
+Pattern sym_spgemm(const Pattern& A, const Pattern& B) {
+    Pattern C;
+    C.nrows = A.nrows;
+    C.ncols = B.ncols;
+    C.rp.assign(A.nrows + 1, 0);
+    std::vector<int> mark(B.ncols, -1);
+    std::vector<int> row;
+    std::vector<std::vector<int>> rows(A.nrows);
+    for (int i = 0; i < A.nrows; i++) {
+        row.clear();
+        for (int p = A.rp[i]; p < A.rp[i + 1]; p++) {
+            int k = A.ci[p];
+            for (int q = B.rp[k]; q < B.rp[k + 1]; q++) {
+                int j = B.ci[q];
+                if (mark[j] != i) { mark[j] = i; row.push_back(j); }
+            }
+        }
+        std::sort(row.begin(), row.end());
+        rows[i] = row;
+        C.rp[i + 1] = C.rp[i] + (int)row.size();
+    }
+    C.ci.resize(C.rp[A.nrows]);
+    for (int i = 0; i < A.nrows; i++) std::copy(rows[i].begin(), rows[i].end(), C.ci.begin() + C.rp[i]);
+    return C;
+}
+
+Pattern sym_transpose(const Pattern& A, std::vector<int>& perm) {
+    Pattern T;
+    T.nrows = A.ncols;
+    T.ncols = A.nrows;
+    T.rp.assign(T.nrows + 1, 0);
+    long nnz = A.nnzb();
+    for (long q = 0; q < nnz; q++) T.rp[A.ci[q] + 1]++;
+    for (int i = 0; i < T.nrows; i++) T.rp[i + 1] += T.rp[i];
+    T.ci.resize(nnz);
+    perm.resize(nnz);
+    std::vector<int> pos(T.rp.begin(), T.rp.end() - 1);
+    for (int i = 0; i < A.nrows; i++)
+        for (int q = A.rp[i]; q < A.rp[i + 1]; q++) {
+            int t = pos[A.ci[q]]++;
+            T.ci[t] = i;
+            perm[t] = q;
+        }
+    return T;
+}
+
+// Greedy aggregation of a node graph (rows sorted, self included):
+// phase 1 roots an aggregate at every node whose non-excluded neighbourhood
+// is still untouched and takes the whole neighbourhood; phase 2 attaches
+// each leftover node to the phase-1 aggregate of its first aggregated
+// neighbour; phase 3 turns what remains into singletons.  Excluded nodes
+// (all DOFs Dirichlet) belong to no aggregate (-1 on output).
+int aggregate_graph(int nn, const std::vector<int>& rp, const std::vector<int>& ci, const unsigned char* excl,
+                    std::vector<int>& agg) {
+    agg.assign(nn, -1);
+    for (int i = 0; i < nn; i++)
+        if (excl && excl[i]) agg[i] = -2;
+    int na = 0;
+    for (int i = 0; i < nn; i++) {
+        if (agg[i] != -1) continue;
+        bool ok = true;
+        for (int p = rp[i]; p < rp[i + 1]; p++) {
+            int j = ci[p];
+            if (j != i && agg[j] >= 0) { ok = false; break; }
+        }
+        if (!ok) continue;
+        for (int p = rp[i]; p < rp[i + 1]; p++) {
+            int j = ci[p];
+            if (agg[j] == -1) agg[j] = na;
+        }
+        agg[i] = na;
+        na++;
+    }
+    std::vector<int> a1(agg);
+    for (int i = 0; i < nn; i++) {
+        if (a1[i] != -1) continue;
+        for (int p = rp[i]; p < rp[i + 1]; p++) {
+            int j = ci[p];
+            if (a1[j] >= 0) { agg[i] = a1[j]; break; }
+        }
+    }
+    for (int i = 0; i < nn; i++)
+        if (agg[i] == -1) agg[i] = na++;
+    for (int i = 0; i < nn; i++)
+        if (agg[i] == -2) agg[i] = -1;
+    return na;
+}
+
+// ----------------------------------------------------------------- mesh
+int build_mesh(Ctx& c, const double* vertex, const int32_t* element, int n_fixed, const int32_t* fixed, int n_cases,
+               const int32_t* case_ptr, const int32_t* load_dofs, const double* load_vals) {
+    const int nen = c.nen, nn = c.nn, ne = c.ne;
+    c.nde = 3 * nen;
+    c.npk = c.nde * (c.nde + 1) / 2;
+    c.nkf = nen * (nen + 1) / 2;
+    c.ndof = 3 * nn;
+    c.ntiles = (ne + 31) / 32;
+    c.ncases = n_cases;
+    for (long q = 0; q < 3L * nn; q++)
+        if (!std::isfinite(vertex[q])) { set_error("vertex %ld is not finite", q / 3); return TOPO_ERR_MESH; }
+    for (long q = 0; q < (long)ne * nen; q++)
+        if (element[q] < 0 || element[q] >= nn) {
+            set_error("element %ld references node %d outside [0,%d)", q / nen, element[q], nn);
+            return TOPO_ERR_MESH;
+        }
+    for (int i = 0; i < n_fixed; i++)
+        if (fixed[i] < 0 || fixed[i] >= c.ndof) { set_error("fixed DOF %d out of range", fixed[i]); return TOPO_ERR_MESH; }
+    if (case_ptr[0] != 0) { set_error("case_ptr[0] must be 0"); return TOPO_ERR_ARG; }
+    for (int k = 0; k < n_cases; k++) {
+        if (case_ptr[k + 1] < case_ptr[k]) { set_error("case_ptr not monotone"); return TOPO_ERR_ARG; }
+        for (int q = case_ptr[k]; q < case_ptr[k + 1]; q++) {
+            if (load_dofs[q] < 0 || load_dofs[q] >= c.ndof) { set_error("load DOF %d out of range", load_dofs[q]); return TOPO_ERR_MESH; }
+            if (!std::isfinite(load_vals[q])) { set_error("load value %d not finite", q); return TOPO_ERR_MESH; }
+        }
+    }
+    c.vertex_h.assign(vertex, vertex + 3L * nn);
+    c.elem_h.assign(element, element + (long)ne * nen);
+    c.fixed_h.assign(fixed, fixed + n_fixed);
+    c.dof_fixed_h.assign(c.ndof, 0);
+    for (int i = 0; i < n_fixed; i++) c.dof_fixed_h[fixed[i]] = 1;
+
+    cudaStream_t s = c.s;
+    // AoSoA connectivity tiles + fixed masks
+    std::vector<int> conn((size_t)c.ntiles * nen * 32, 0);
+    std::vector<uint32_t> emask(ne, 0);
+    for (int e = 0; e < ne; e++) {
+        int t = e >> 5, lane = e & 31;
+        uint32_t m = 0;
+        for (int l = 0; l < nen; l++) {
+            int nd = element[(long)e * nen + l];
+            conn[((size_t)t * nen + l) * 32 + lane] = nd;
+            for (int cc = 0; cc < 3; cc++)
+                if (c.dof_fixed_h[3 * nd + cc]) m |= 1u << (cc * nen + l);
+        }
+        emask[e] = m;
+    }
+    TRET(c.conn.upload(conn, s));
+    TRET(c.emask.upload(emask, s));
+    TRET(c.elem.upload(c.elem_h, s));
+    TRET(c.vertex.upload(c.vertex_h, s));
+    TRET(c.dof_fixed.upload(c.dof_fixed_h, s));
+    TRET(c.fixed.upload(c.fixed_h, s));
+
+    // load vectors: VecSetValues(INSERT) then fixed DOFs zeroed (SolveFem.cpp:277-282,324-333)
+    std::vector<double> F((size_t)n_cases * c.ndof, 0.0);
+    for (int k = 0; k < n_cases; k++) {
+        for (int q = case_ptr[k]; q < case_ptr[k + 1]; q++) F[(size_t)k * c.ndof + load_dofs[q]] = load_vals[q];
+        for (int i = 0; i < n_fixed; i++) F[(size_t)k * c.ndof + fixed[i]] = 0.0;
+    }
+    TRET(c.F.upload(F, s));
+
+    // node -> element incidence
+    std::vector<int> n2e_ptr(nn + 1, 0), n2e((size_t)ne * nen);
+    for (long q = 0; q < (long)ne * nen; q++) n2e_ptr[element[q] + 1]++;
+    for (int i = 0; i < nn; i++) n2e_ptr[i + 1] += n2e_ptr[i];
+    {
+        std::vector<int> pos(n2e_ptr.begin(), n2e_ptr.end() - 1);
+        for (long q = 0; q < (long)ne * nen; q++) n2e[pos[element[q]]++] = (int)q;
+    }
+    // node graph (self included, sorted) = block pattern of K
+    Pattern G;
+    G.nrows = G.ncols = nn;
+    G.rp.assign(nn + 1, 0);
+    {
+        std::vector<int> mark(nn, -1), row;
+        std::vector<int> ci;
+        ci.reserve((size_t)nn * 27);
+        for (int i = 0; i < nn; i++) {
+            row.clear();
+            for (int p = n2e_ptr[i]; p < n2e_ptr[i + 1]; p++) {
+                int e = n2e[p] / nen;
+                for (int l = 0; l < nen; l++) {
+                    int j = element[(long)e * nen + l];
+                    if (mark[j] != i) { mark[j] = i; row.push_back(j); }
+                }
+            }
+            if (row.empty()) row.push_back(i);  // isolated node: keep its diagonal
+            std::sort(row.begin(), row.end());
+            ci.insert(ci.end(), row.begin(), row.end());
+            G.rp[i + 1] = (int)ci.size();
+        }
+        G.ci.swap(ci);
+    }
+    c.maxdeg = G.max_row();
+    if (c.maxdeg > 65535) { set_error("node degree too large"); return TOPO_ERR_MESH; }
+    std::vector<uint16_t> bpos((size_t)ne * nen * nen);
+    for (int e = 0; e < ne; e++)
+        for (int p = 0; p < nen; p++) {
+            int np = element[(long)e * nen + p];
+            const int* b = G.ci.data() + G.rp[np];
+            int len = G.rp[np + 1] - G.rp[np];
+            for (int q = 0; q < nen; q++) {
+                int nq = element[(long)e * nen + q];
+                int slot = (int)(std::lower_bound(b, b + len, nq) - b);
+                bpos[((size_t)e * nen + p) * nen + q] = (uint16_t)slot;
+            }
+        }
+    TRET(c.n2e_ptr.upload(n2e_ptr, s));
+    TRET(c.n2e.upload(n2e, s));
+    TRET(c.bpos.upload(bpos, s));
+
+    c.hl.clear();
+    c.hl.emplace_back();
+    c.hl[0].bs = 3;
+    c.hl[0].nnode = nn;
+    c.hl[0].A = std::move(G);
+    return 0;
+}
+
+// ----------------------------------------------------------------- AMG hierarchy (geometry only)
+// Tentative prolongator: per aggregate, modified Gram-Schmidt on the rows of
+// the near-null space (rigid-body modes about the aggregate centroid at
+// level 0; the previous level's R factors above), Dirichlet rows dropped.
+static void tentative(const Ctx& c, int lvl, const AmgHostLevel& L, const std::vector<double>& Bprev,
+                      std::vector<double>& Pt, std::vector<double>& Bnext) {
+    const int bs = L.bs, nnode = L.nnode, na = L.nagg;
+    Pt.assign((size_t)nnode * bs * 6, 0.0);
+    Bnext.assign((size_t)na * 6 * 6, 0.0);
+    std::vector<int> cnt(na + 1, 0), mem;
+    for (int i = 0; i < nnode; i++)
+        if (L.agg[i] >= 0) cnt[L.agg[i] + 1]++;
+    for (int a = 0; a < na; a++) cnt[a + 1] += cnt[a];
+    mem.resize(cnt[na]);
+    {
+        std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+        for (int i = 0; i < nnode; i++)
+            if (L.agg[i] >= 0) mem[fill[L.agg[i]]++] = i;
+    }
+    std::vector<double> Q;
+    std::vector<long> rid;
+    for (int a = 0; a < na; a++) {
+        int m0 = cnt[a], m1 = cnt[a + 1];
+        Q.clear();
+        rid.clear();
+        double cen[3] = {0, 0, 0};
+        if (lvl == 0) {
+            for (int t = m0; t < m1; t++)
+                for (int q = 0; q < 3; q++) cen[q] += c.vertex_h[3 * (size_t)mem[t] + q];
+            for (int q = 0; q < 3; q++) cen[q] /= (double)(m1 - m0);
+        }
+        for (int t = m0; t < m1; t++) {
+            int i = mem[t];
+            for (int q = 0; q < bs; q++) {
+                long row = (long)bs * i + q;
+                if (lvl == 0 && c.dof_fixed_h[row]) continue;
+                rid.push_back((long)i * bs + q);
+                if (lvl == 0) {
+                    double x = c.vertex_h[3 * (size_t)i] - cen[0], y = c.vertex_h[3 * (size_t)i + 1] - cen[1],
+                           z = c.vertex_h[3 * (size_t)i + 2] - cen[2];
+                    const double rb[3][6] = {{1, 0, 0, -y, 0, z}, {0, 1, 0, x, -z, 0}, {0, 0, 1, 0, y, -x}};
+                    for (int j = 0; j < 6; j++) Q.push_back(rb[q][j]);
+                } else {
+                    for (int j = 0; j < 6; j++) Q.push_back(Bprev[(size_t)row * 6 + j]);
+                }
+            }
+        }
+        int rows = (int)rid.size();
+        double R[36] = {0};
+        for (int j = 0; j < 6; j++) {
+            double n0 = 0.0;
+            for (int r = 0; r < rows; r++) n0 += Q[r * 6 + j] * Q[r * 6 + j];
+            n0 = std::sqrt(n0);
+            for (int i2 = 0; i2 < j; i2++) {
+                double h = 0.0;
+                for (int r = 0; r < rows; r++) h += Q[r * 6 + i2] * Q[r * 6 + j];
+                R[i2 * 6 + j] = h;
+                for (int r = 0; r < rows; r++) Q[r * 6 + j] -= h * Q[r * 6 + i2];
+            }
+            double nr = 0.0;
+            for (int r = 0; r < rows; r++) nr += Q[r * 6 + j] * Q[r * 6 + j];
+            nr = std::sqrt(nr);
+            if (nr <= 1e-10 * n0 || nr == 0.0) {
+                for (int r = 0; r < rows; r++) Q[r * 6 + j] = 0.0;
+                R[j * 6 + j] = 0.0;
+            } else {
+                for (int r = 0; r < rows; r++) Q[r * 6 + j] /= nr;
+                R[j * 6 + j] = nr;
+            }
+        }
+        for (int r = 0; r < rows; r++)
+            for (int j = 0; j < 6; j++) Pt[(size_t)rid[r] * 6 + j] = Q[r * 6 + j];
+        for (int i2 = 0; i2 < 6; i2++)
+            for (int j = 0; j < 6; j++) Bnext[((size_t)a * 6 + i2) * 6 + j] = R[i2 * 6 + j];
+    }
+}
+
+int build_amg_host(Ctx& c) {
+    const topo_params& p = c.p;
+    std::vector<unsigned char> excl(c.nn, 0);
+    for (int i = 0; i < c.nn; i++)
+        excl[i] = c.dof_fixed_h[3 * i] && c.dof_fixed_h[3 * i + 1] && c.dof_fixed_h[3 * i + 2];
+    std::vector<double> B, Bnext;
+    int maxlev = std::min(std::max(p.amg_max_levels, 1), kMaxLevels);
+    for (int lvl = 0;; lvl++) {
+        AmgHostLevel& L = c.hl[lvl];
+        long ndof = (long)L.nnode * L.bs;
+        if (lvl + 1 >= maxlev || ndof <= p.amg_coarse_max) break;
+        L.nagg = aggregate_graph(L.nnode, L.A.rp, L.A.ci, lvl == 0 ? excl.data() : nullptr, L.agg);
+        if (L.nagg == 0 || L.nagg >= L.nnode) { L.agg.clear(); L.nagg = 0; break; }
+        tentative(c, lvl, L, B, L.Pt, Bnext);
+        Pattern Ptp;
+        Ptp.nrows = L.nnode;
+        Ptp.ncols = L.nagg;
+        Ptp.rp.assign(L.nnode + 1, 0);
+        for (int i = 0; i < L.nnode; i++) {
+            Ptp.rp[i + 1] = Ptp.rp[i] + (L.agg[i] >= 0 ? 1 : 0);
+            if (L.agg[i] >= 0) Ptp.ci.push_back(L.agg[i]);
+        }
+        L.P = p.amg_smooth_p ? sym_spgemm(L.A, Ptp) : Ptp;
+        L.ptpos.assign(L.nnode, -1);
+        for (int i = 0; i < L.nnode; i++) {
+            if (L.agg[i] < 0) continue;
+            const int* b = L.P.ci.data() + L.P.rp[i];
+            int len = L.P.rp[i + 1] - L.P.rp[i];
+            const int* f = std::lower_bound(b, b + len, L.agg[i]);
+            L.ptpos[i] = (f != b + len && *f == L.agg[i]) ? (int)(f - b) : -1;
+        }
+        L.AP = sym_spgemm(L.A, L.P);
+        L.R = sym_transpose(L.P, L.rperm);
+        AmgHostLevel next;
+        next.bs = 6;
+        next.nnode = L.nagg;
+        next.A = sym_spgemm(L.R, L.AP);
+        B.swap(Bnext);
+        c.hl.push_back(std::move(next));
+    }
+    c.nlev = (int)c.hl.size();
+    // upload
+    cudaStream_t s = c.s;
+    for (int l = 0; l < c.nlev; l++) {
+        AmgHostLevel& H = c.hl[l];
+        AmgDevLevel& D = c.dl[l];
+        D.bs = H.bs;
+        D.nnode = H.nnode;
+        D.ndof = H.nnode * H.bs;
+        D.nagg = H.nagg;
+        TRET(D.A.upload(H.A, s));
+        std::vector<int> dp(H.nnode, -1);
+        for (int i = 0; i < H.nnode; i++)
+            for (int q = H.A.rp[i]; q < H.A.rp[i + 1]; q++)
+                if (H.A.ci[q] == i) dp[i] = q - H.A.rp[i];
+        for (int i = 0; i < H.nnode; i++)
+            if (dp[i] < 0) { set_error("AMG level %d row %d has no diagonal block", l, i); return TOPO_ERR_MESH; }
+        TRET(D.diagpos.upload(dp, s));
+        if (l + 1 < c.nlev) {
+            TRET(D.P.upload(H.P, s));
+            TRET(D.AP.upload(H.AP, s));
+            TRET(D.R.upload(H.R, s));
+            TRET(D.ptpos.upload(H.ptpos, s));
+            TRET(D.rperm.upload(H.rperm, s));
+            Pattern Ptp;
+            Ptp.nrows = H.nnode;
+            Ptp.ncols = H.nagg;
+            Ptp.rp.assign(H.nnode + 1, 0);
+            std::vector<double> pv;
+            std::vector<float> pv32;
+            for (int i = 0; i < H.nnode; i++) {
+                Ptp.rp[i + 1] = Ptp.rp[i];
+                if (H.agg[i] < 0) continue;
+                Ptp.rp[i + 1]++;
+                Ptp.ci.push_back(H.agg[i]);
+                for (int q = 0; q < H.bs * 6; q++) {
+                    pv.push_back(H.Pt[(size_t)i * H.bs * 6 + q]);
+                    pv32.push_back((float)H.Pt[(size_t)i * H.bs * 6 + q]);
+                }
+            }
+            TRET(D.Ptp.upload(Ptp, s));
+            TRET(D.Pt64c.upload(pv, s));
+            TRET(D.Pt32c.upload(pv32, s));
+        }
+    }
+    return 0;
+}
+
+}  // namespace topo

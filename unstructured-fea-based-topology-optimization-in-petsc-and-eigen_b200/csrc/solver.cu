@@ -1,0 +1,360 @@
+// solver.cu -- Krylov solvers of the design iteration:
+//   * FGMRES(restart), right-preconditioned by the AMG V-cycle, for K U = F
+//     (replaces KSPFGMRES + PCGAMG, SolveFem.cpp:124-139), FP64 Arnoldi and
+//     residuals, FP64 or FP32 V-cycle;
+//   * Jacobi-preconditioned CG for the Helmholtz filter (KSPCG + PCJACOBI,
+//     PDEFilter.cpp:117-137) with PETSc's preconditioned-norm convergence test.
+// All reductions are deterministic two-pass block sums.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "ctx.h"
+
+namespace topo {
+
+int kmatvec64r(Ctx& c, const double* u, double* y, const double* b);
+
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs
+
+// ----------------------------------------------------------------- reductions
+__global__ void k_dot(long n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ part) {
+    __shared__ double sm[32];
+    double v[1] = {0.0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) v[0] += a[i] * b[i];
+    block_sum<1>(v, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+// out[k] = sum_b part[b*nv + k]; optional sqrt of entry `sqrt_idx`
+__global__ void k_final(int nb, int nv, const double* __restrict__ part, double* __restrict__ out, int sqrt_idx) {
+    __shared__ double sm[32];
+    for (int k = 0; k < nv; k++) {
+        double v[1] = {0.0};
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) v[0] += part[(long)i * nv + k];
+        block_sum<1>(v, sm);
+        if (threadIdx.x == 0) out[k] = (k == sqrt_idx) ? sqrt(v[0]) : v[0];
+        __syncthreads();
+    }
+}
+
+int finalize_sum(Ctx& c, const double* partials, int nparts, int nv, double* out_dev) {
+    k_final<<<1, 512, 0, c.s>>>(nparts, nv, partials, out_dev, -1);
+    TCK(cudaGetLastError());
+    return 0;
+}
+int dev_dot(Ctx& c, const double* a, const double* b, long n, double* out_dev) {
+    if ((long)c.red.n < kRedBlocks * 40L) TRET(c.red.alloc(std::max<long>(kRedBlocks * 40L, 4096)));
+    k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, a, b, c.red.p);
+    return finalize_sum(c, c.red.p, kRedBlocks, 1, out_dev);
+}
+
+// ----------------------------------------------------------------- FGMRES kernels
+// h_j = V_j . w for j < nv (classical Gram-Schmidt: one pass over w)
+template <int NV>
+__global__ void __launch_bounds__(256) k_mdot(long n, int nv, const double* __restrict__ V, long ld,
+                                              const double* __restrict__ w, double* __restrict__ part) {
+    __shared__ double sm[NV * 32];
+    double acc[NV];
+#pragma unroll
+    for (int j = 0; j < NV; j++) acc[j] = 0.0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double wi = w[i];
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < nv) acc[j] += V[j * ld + i] * wi;
+    }
+    block_sum<NV>(acc, sm);
+    if (threadIdx.x == 0)
+        for (int j = 0; j < nv; j++) part[(long)blockIdx.x * nv + j] = acc[j];
+}
+// w -= sum_j h_j V_j ; partial ||w||^2
+template <int NV>
+__global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __restrict__ V, long ld,
+                                              const double* __restrict__ h, double* __restrict__ w,
+                                              double* __restrict__ part) {
+    __shared__ double sm[32];
+    __shared__ double hs[NV];
+    if (threadIdx.x < nv) hs[threadIdx.x] = h[threadIdx.x];
+    __syncthreads();
+    double v[1] = {0.0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double wi = w[i];
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < nv) wi -= hs[j] * V[j * ld + i];
+        w[i] = wi;
+        v[0] += wi * wi;
+    }
+    block_sum<1>(v, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+__global__ void k_scale_to(long n, const double* __restrict__ w, const double* __restrict__ s, double* __restrict__ v,
+                           int invert) {
+    const double f = invert ? 1.0 / (*s) : (*s);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) v[i] = w[i] * f;
+}
+// x += sum_k y_k Z_k
+template <class TZ>
+__global__ void k_update(long n, int kd, const TZ* __restrict__ Z, long ld, const double* __restrict__ y,
+                         double* __restrict__ x) {
+    __shared__ double ys[64];
+    if (threadIdx.x < kd) ys[threadIdx.x] = y[threadIdx.x];
+    __syncthreads();
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double s = x[i];
+        for (int k = 0; k < kd; k++) s += ys[k] * (double)Z[k * ld + i];
+        x[i] = s;
+    }
+}
+
+static int mdot(Ctx& c, int nv, const double* V, long ld, const double* w, double* out) {
+    long n = c.ndof;
+    if (nv <= 8) k_mdot<8><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p);
+    else if (nv <= 16) k_mdot<16><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p);
+    else k_mdot<32><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p);
+    TCK(cudaGetLastError());
+    return finalize_sum(c, c.red.p, kRedBlocks, nv, out);
+}
+static int orth(Ctx& c, int nv, const double* V, long ld, const double* h, double* w, double* hn_out) {
+    long n = c.ndof;
+    if (nv <= 8) k_orth<8><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p);
+    else if (nv <= 16) k_orth<16><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p);
+    else k_orth<32><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p);
+    k_final<<<1, 512, 0, c.s>>>(kRedBlocks, 1, c.red.p, hn_out, 0);
+    TCK(cudaGetLastError());
+    return 0;
+}
+
+static int precond_apply(Ctx& c, const double* v, int j) {
+    const long n = c.ndof;
+    if (c.p.precision == TOPO_PREC_MIXED) return amg_vcycle32(c, v, c.Z32.p + (size_t)j * n);
+    return amg_vcycle64(c, v, c.Z64.p + (size_t)j * n);
+}
+
+// FGMRES(restart) on K(Ee64) u = b, x in/out.  Converged when the Arnoldi
+// residual estimate |g_{j+1}| <= max(rtol ||b||, 1e-50) (KSPConvergedDefault
+// with a nonzero initial guess: rnorm0 = ||b||).
+static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status) {
+    const long n = c.ndof;
+    const int m = std::max(1, std::min(c.p.fem_restart, 30));
+    const int maxit = c.p.fem_maxit;
+    if (!c.V.p) {
+        TRET(c.V.alloc((size_t)(m + 1) * n));
+        if (c.p.precision == TOPO_PREC_MIXED) TRET(c.Z32.alloc((size_t)m * n));
+        else TRET(c.Z64.alloc((size_t)m * n));
+        TRET(c.w.alloc(n));
+        TRET(c.wtmp.alloc(64));
+    }
+    if (c.p.precision == TOPO_PREC_MIXED && !c.Z32.p) TRET(c.Z32.alloc((size_t)m * n));
+    if (c.p.precision != TOPO_PREC_MIXED && !c.Z64.p) TRET(c.Z64.alloc((size_t)m * n));
+    if ((long)c.red.n < kRedBlocks * 40L) TRET(c.red.alloc(std::max<long>(kRedBlocks * 40L, 4096)));
+    double* hs = c.hsc.h;   // pinned: [0..m+1] column, [64] misc
+    double* gm = c.dsc.p + DS_GM;
+    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), yv(m);
+    // ||b||
+    TRET(dev_dot(c, b, b, n, gm));
+    TCK(cudaMemcpyAsync(hs, gm, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    TCK(cudaStreamSynchronize(c.s));
+    const double bnorm = std::sqrt(hs[0]);
+    const double ttol = std::max(c.p.fem_rtol * bnorm, 1e-50);
+    int its = 0;
+    bool conv = false;
+    while (!conv && its < maxit) {
+        // v0 = (b - K x) / beta
+        TRET(kmatvec64r(c, x, c.w.p, b));
+        TRET(dev_dot(c, c.w.p, c.w.p, n, gm));
+        TCK(cudaMemcpyAsync(hs, gm, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+        TCK(cudaStreamSynchronize(c.s));
+        const double beta = std::sqrt(hs[0]);
+        if (!std::isfinite(beta)) { set_error("FGMRES residual is not finite"); return TOPO_ERR_NAN; }
+        if (beta <= ttol) { conv = true; break; }
+        hs[70] = beta;
+        TCK(cudaMemcpyAsync(c.wtmp.p, hs + 70, sizeof(double), cudaMemcpyHostToDevice, c.s));
+        k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, c.wtmp.p, c.V.p, 1);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int kdone = 0;
+        for (int j = 0; j < m && its < maxit; j++) {
+            const double* vj = c.V.p + (size_t)j * n;
+            TRET(precond_apply(c, vj, j));
+            if (c.p.precision == TOPO_PREC_MIXED) TRET(kmatvec_f32in(c, c.Ee64.p, c.Z32.p + (size_t)j * n, c.w.p));
+            else TRET(kmatvec(c, c.Ee64.p, c.Z64.p + (size_t)j * n, c.w.p));
+            TRET(mdot(c, j + 1, c.V.p, n, c.w.p, gm));
+            TRET(orth(c, j + 1, c.V.p, n, gm, c.w.p, gm + j + 1));
+            TCK(cudaMemcpyAsync(hs, gm, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, c.s));
+            k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, gm + j + 1, c.V.p + (size_t)(j + 1) * n, 1);
+            TCK(cudaStreamSynchronize(c.s));
+            for (int i = 0; i <= j + 1; i++) H[(size_t)i * m + j] = hs[i];
+            const double hn = hs[j + 1];
+            for (int i = 0; i < j; i++) {
+                double t1 = H[(size_t)i * m + j], t2 = H[(size_t)(i + 1) * m + j];
+                H[(size_t)i * m + j] = cs[i] * t1 + sn[i] * t2;
+                H[(size_t)(i + 1) * m + j] = -sn[i] * t1 + cs[i] * t2;
+            }
+            double hjj = H[(size_t)j * m + j], hj1 = H[(size_t)(j + 1) * m + j];
+            double den = std::sqrt(hjj * hjj + hj1 * hj1);
+            if (den == 0.0) { cs[j] = 1.0; sn[j] = 0.0; }
+            else { cs[j] = hjj / den; sn[j] = hj1 / den; }
+            H[(size_t)j * m + j] = cs[j] * hjj + sn[j] * hj1;
+            H[(size_t)(j + 1) * m + j] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            its++;
+            kdone = j + 1;
+            const double res = std::fabs(g[j + 1]);
+            if (!std::isfinite(res)) { set_error("FGMRES breakdown (non-finite residual)"); return TOPO_ERR_NAN; }
+            if (res <= ttol || hn == 0.0) { conv = res <= ttol; break; }
+        }
+        for (int i = kdone - 1; i >= 0; i--) {
+            double s = g[i];
+            for (int k = i + 1; k < kdone; k++) s -= H[(size_t)i * m + k] * yv[k];
+            yv[i] = s / H[(size_t)i * m + i];
+        }
+        for (int k = 0; k < kdone; k++) hs[80 + k] = yv[k];
+        TCK(cudaMemcpyAsync(c.wtmp.p, hs + 80, sizeof(double) * kdone, cudaMemcpyHostToDevice, c.s));
+        if (c.p.precision == TOPO_PREC_MIXED)
+            k_update<float><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z32.p, n, c.wtmp.p, x);
+        else
+            k_update<double><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z64.p, n, c.wtmp.p, x);
+        TCK(cudaGetLastError());
+        TCK(cudaStreamSynchronize(c.s));  // pinned y buffer reused next cycle
+    }
+    *its_out = its;
+    *status = conv ? 0 : 1;
+    return 0;
+}
+
+// SolveFem::ComputeFem (SolveFem.cpp:91-157): moduli, AMG numeric setup,
+// U = 0, FGMRES, then the true relative residual.
+int fem_solve(Ctx& c, const double* xphys, double* u) {
+    TRET(compute_moduli(c, xphys));
+    TRET(amg_numeric(c));
+    const long n = c.ndof;
+    int worst = 0, its_total = 0;
+    double rel_worst = 0.0;
+    for (int k = 0; k < c.ncases; k++) {
+        double* uk = u + (size_t)k * n;
+        const double* fk = c.F.p + (size_t)k * n;
+        TCK(cudaMemsetAsync(uk, 0, sizeof(double) * n, c.s));
+        int its = 0, st = 0;
+        TRET(fgmres(c, fk, uk, &its, &st));
+        its_total += its;
+        worst = std::max(worst, st);
+        // true residual ||F - K U|| / ||F||
+        TRET(kmatvec64r(c, uk, c.w.p, fk));
+        double* gm = c.dsc.p + DS_GM;
+        TRET(dev_dot(c, c.w.p, c.w.p, n, gm));
+        TRET(dev_dot(c, fk, fk, n, gm + 1));
+        TCK(cudaMemcpyAsync(c.hsc.h, gm, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+        TCK(cudaStreamSynchronize(c.s));
+        double rel = c.hsc.h[1] > 0 ? std::sqrt(c.hsc.h[0] / c.hsc.h[1]) : std::sqrt(c.hsc.h[0]);
+        rel_worst = std::max(rel_worst, rel);
+        if (c.p.verbose) printf("Norm of error %e, Iterations %d\n", rel, its);
+    }
+    c.info.fem_its = its_total;
+    c.info.fem_relres = rel_worst;
+    c.info.fem_status = worst;
+    return worst ? TOPO_NOT_CONVERGED : 0;
+}
+
+// ----------------------------------------------------------------- filter CG
+__global__ void k_cg_start(long n, const double* __restrict__ b, const double* __restrict__ w,
+                           const double* __restrict__ dinv, double* __restrict__ r, double* __restrict__ z,
+                           double* __restrict__ part) {
+    __shared__ double sm[3 * 32];
+    double v[3] = {0.0, 0.0, 0.0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double ri = b[i] - w[i], zi = dinv[i] * ri, zb = dinv[i] * b[i];
+        r[i] = ri;
+        z[i] = zi;
+        v[0] += zi * zi;
+        v[1] += zi * ri;
+        v[2] += zb * zb;
+    }
+    block_sum<3>(v, sm);
+    if (threadIdx.x == 0) for (int k = 0; k < 3; k++) part[3L * blockIdx.x + k] = v[k];
+}
+// p = z (first) or p = z + (beta/betaold) p
+__global__ void k_cg_p(long n, const double* __restrict__ z, double* __restrict__ p, const double* __restrict__ sc,
+                       int first) {
+    const double bb = first ? 0.0 : sc[2] / sc[3];
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        p[i] = first ? z[i] : z[i] + bb * p[i];
+}
+// a = beta/dpi; x += a p; r -= a w; z = Dinv r; partial (z.z, z.r)
+__global__ void k_cg_step(long n, const double* __restrict__ p, const double* __restrict__ w,
+                          const double* __restrict__ dinv, double* __restrict__ x, double* __restrict__ r,
+                          double* __restrict__ z, const double* __restrict__ sc, double* __restrict__ part) {
+    __shared__ double sm[2 * 32];
+    const double a = sc[2] / sc[4];
+    double v[2] = {0.0, 0.0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        x[i] += a * p[i];
+        double ri = r[i] - a * w[i];
+        r[i] = ri;
+        double zi = dinv[i] * ri;
+        z[i] = zi;
+        v[0] += zi * zi;
+        v[1] += zi * ri;
+    }
+    block_sum<2>(v, sm);
+    if (threadIdx.x == 0) { part[2L * blockIdx.x] = v[0]; part[2L * blockIdx.x + 1] = v[1]; }
+}
+// sc[1] = dp = sqrt(z.z); sc[3] = betaold = sc[2]; sc[2] = beta = z.r (+ sc[0] = snorm on start)
+__global__ void k_cg_final(int nb, int nv, const double* __restrict__ part, double* __restrict__ sc, int start) {
+    __shared__ double sm[3 * 32];
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < nb; i += blockDim.x)
+        for (int k = 0; k < nv; k++) v[k] += part[(long)i * nv + k];
+    block_sum<3>(v, sm);
+    if (threadIdx.x == 0) {
+        sc[1] = sqrt(v[0]);
+        sc[3] = start ? 0.0 : sc[2];
+        sc[2] = v[1];
+        if (start) sc[0] = sqrt(v[2]);
+    }
+}
+
+// KSPCG + PCJACOBI with a nonzero initial guess x (PDEFilter.cpp:117-137):
+// preconditioned residual norm, converged when ||D^-1 r|| <= max(rtol
+// ||D^-1 b||, atol), diverged when it exceeds dtol ||D^-1 b||.
+int filter_cg(Ctx& c, const double* b, double* x, int* its_out) {
+    const long n = c.nn;
+    double* sc = c.dsc.p + DS_CG;
+    double* hs = c.hsc.h + 96;
+    if ((long)c.red.n < kRedBlocks * 40L) TRET(c.red.alloc(std::max<long>(kRedBlocks * 40L, 4096)));
+    TRET(filter_kf(c, x, c.fw.p));
+    k_cg_start<<<kRedBlocks, 256, 0, c.s>>>(n, b, c.fw.p, c.fdiag_inv.p, c.fr.p, c.fz.p, c.red.p);
+    k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 3, c.red.p, sc, 1);
+    TCK(cudaMemcpyAsync(hs, sc, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    TCK(cudaStreamSynchronize(c.s));
+    const double snorm = hs[0];
+    const double ttol = std::max(c.p.filter_rtol * snorm, c.p.filter_atol);
+    double dp = hs[1];
+    *its_out = 0;
+    if (!std::isfinite(dp)) { set_error("filter CG residual is not finite"); return TOPO_ERR_NAN; }
+    if (dp <= ttol) return 0;
+    int i = 0;
+    do {
+        *its_out = i + 1;
+        if (hs[2] == 0.0) return 0;  // beta == 0
+        k_cg_p<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.fz.p, c.fp.p, sc, i == 0);
+        TRET(filter_kf(c, c.fp.p, c.fw.p));
+        k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.red.p);
+        k_final<<<1, 512, 0, c.s>>>(kRedBlocks, 1, c.red.p, sc + 4, -1);
+        k_cg_step<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.fdiag_inv.p, x, c.fr.p, c.fz.p, sc, c.red.p);
+        k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 2, c.red.p, sc, 0);
+        TCK(cudaMemcpyAsync(hs, sc, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+        TCK(cudaStreamSynchronize(c.s));
+        dp = hs[1];
+        if (!std::isfinite(dp)) { set_error("filter CG residual is not finite"); return TOPO_ERR_NAN; }
+        if (dp <= ttol) return 0;
+        if (dp >= c.p.filter_dtol * snorm) { set_error("filter CG diverged"); return TOPO_NOT_CONVERGED; }
+        i++;
+    } while (i < c.p.filter_maxit);
+    return TOPO_NOT_CONVERGED;
+}
+
+}  // namespace topo
