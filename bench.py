@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Benchmark: SIMP design iterations per second on one B200.
+
+Workload (default): the reference-scale hex8 cantilever, 140 x 70 x 40 jittered
+unit-cube elements (392,000 hex8, 410,451 nodes, 1,231,353 DOF), E0 = 1,
+Emin = 1e-9, nu = 0.3, penal 3, volfrac 0.12, filter radius 1.5 h, FGMRES
+rtol 1e-5, seeded synthetic mesh.  One step = one full design iteration of
+the reference's main loop (FEA solve + sensitivities, filtered
+sensitivities, MMA update, design change, filter, projection).
+
+The headline `value` is the mixed-precision form (FP32 AMG V-cycle inside
+FP64 FGMRES) with all data resident in HBM; the plain FP64 form is reported
+beside it.  `e2e` runs the same iterations through the host-buffer entry
+point topo_opt_step_host (design uploaded and results downloaded every step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload hex8-392k|hex8-8k|tet4-2.35M] [--serve]
+
+Under torchrun (N > 1) every rank runs an independent replica of the
+workload (the path does not shard): value = N * K / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "hex8-392k": dict(nx=140, ny=70, nz=40, nen=8),
+    "hex8-8k": dict(nx=40, ny=20, nz=10, nen=8),
+    "tet4-2.35M": dict(nx=140, ny=70, nz=40, nen=4),
+    "hex8-1.2M": dict(nx=200, ny=100, nz=60, nen=8),
+}
+PARAMS = dict(Emax=1.0, Emin=1e-9, nu=0.3, penal=3.0, volfrac=0.12, rmin=1.5, fem_rtol=1e-5, ch_tol=0.0)
+METRIC = "design iters/s, 392k hex8 (FP32-AMG vs FP64, rtol 1e-5); p50/p99 serve latency"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax = float(p[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, p[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU side
+def cpu_run(wl, steps, time_cap_s, warmup=1):
+    """The CPU restatement (oracle port, OpenMP over all host threads) on the
+    same workload: setup untimed, `warmup` iterations untimed, then up to
+    `steps` timed design iterations or until time_cap_s elapses."""
+    from oracle import oracle as O
+    O.build()
+    T = _pkg()
+    v, e, f, ld, lv = T.gen_cantilever(wl["nx"], wl["ny"], wl["nz"], wl["nen"])
+    orc = O.Oracle(v, e, f, ld, lv, **{k: val for k, val in PARAMS.items() if k != "ch_tol"})
+    import numpy as np
+    ne = e.shape[0]
+    m = 1
+    X = np.full(ne, PARAMS["volfrac"]); Xold = X.copy()
+    XF = orc.filter(X, 0.01)
+    XP = XF.copy()
+
+    def step(X, Xold, XF, XP, itr):
+        fx, gx, df, dg = orc.fem_obj_sens(XP)
+        df, dg = orc.filter_sens(df, dg)
+        xmn, xmx = orc.mma_movelimit(X)
+        X = orc.mma_update(X, df, gx, dg, xmn, xmx)
+        ch, Xold = orc.mma_design_change(X, Xold)
+        XF = orc.filter(X, 0.01)
+        return X, Xold, XF, XF.copy(), fx
+
+    itr = 0
+    for _ in range(warmup):
+        itr += 1
+        X, Xold, XF, XP, fx = step(X, Xold, XF, XP, itr)
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        itr += 1
+        X, Xold, XF, XP, fx = step(X, Xold, XF, XP, itr)
+        done += 1
+        if time.perf_counter() - t0 > time_cap_s:
+            break
+    dt = time.perf_counter() - t0
+    orc.close()
+    return done, dt, os.cpu_count()
+
+
+def _pkg():
+    import __graft_entry__ as G
+    return G.package()
+
+
+# ------------------------------------------------------------------ GPU side
+def run_device(ctx, T, torch, steps, warmup, stream, dist=None, profile=True):
+    """W untimed + K timed design iterations with resident data; CUDA events on
+    the context's stream, barrier + synchronize on both sides."""
+    ctx.opt_init()
+    for _ in range(warmup):
+        ctx.opt_step()
+    for s in range(4):
+        ctx.profile_read(s)
+    if profile:
+        ctx.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = T.kernel_launches()
+    e0.record(stream)
+    its = []
+    for _ in range(steps):
+        ctx.opt_step()
+        its.append(ctx.info().fem_its)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    l1 = T.kernel_launches()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    prof = {}
+    if profile:
+        for s, name in enumerate(["kmv", "cheb0", "res0", "filter_kf"]):
+            n, t = ctx.profile_read(s)
+            prof[name] = (n, t)
+        ctx.profile(False)
+    return ms, l1 - l0, prof, its
+
+
+def run_e2e(ctx, T, torch, steps, warmup, stream, dist=None):
+    import numpy as np
+    ne = ctx.ne
+    ctx.opt_init()
+    x = torch.empty(ne, dtype=torch.float64).pin_memory().numpy()
+    x[:] = PARAMS["volfrac"]
+    xo = torch.empty(ne, dtype=torch.float64).pin_memory().numpy()
+    xp = torch.empty(ne, dtype=torch.float64).pin_memory().numpy()
+    for _ in range(warmup):
+        ctx.opt_step_host(x, xo, xp)
+        x[:] = xo
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.opt_step_host(x, xo, xp)
+        x[:] = xo
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    return e0.elapsed_time(e1), ne * 8, 2 * ne * 8 + 72
+
+
+def kmv_bytes(ctx, u_bytes):
+    """Algorithmic bytes of one element-operator launch: per element the 8
+    connectivity ids, the fixed mask, E_e and the 300 packed FP64 Ke entries;
+    per node the 3 input and 3 output values."""
+    npk = 300 if ctx.nen == 8 else 78
+    return ctx.ne * (4 * ctx.nen + 4 + 8 + npk * 8) + ctx.nn * 3 * (u_bytes + 8)
+
+
+def cheb0_bytes(ctx, nnzb, val_bytes):
+    """One fused level-0 Chebyshev sweep (BSR 3x3): A values, column ids, row
+    pointers, and per DOF: d_old read, d_new write, r read+write, x
+    read+write, D^-1 read."""
+    n = ctx.ndof
+    return nnzb * (9 * val_bytes + 4) + (ctx.nn + 1) * 4 + n * 7 * val_bytes
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="hex8-392k", choices=list(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--serve", action="store_true", help="also run the serving stream (p50/p99)")
+    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
+                    help="time one precision only (used for short profiling runs)")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cfg = {"workload": f"{args.workload} cantilever {wl['nx']}x{wl['ny']}x{wl['nz']} {'hex8' if wl['nen'] == 8 else 'tet4'}",
+           "elements": wl["nx"] * wl["ny"] * wl["nz"] * (1 if wl["nen"] == 8 else 6),
+           "fem_rtol": 1e-5, "filter_radius_h": 1.5, "volfrac": 0.12,
+           "l2": "inputs larger than L2 (element matrices alone exceed 126 MB); no flush",
+           "parallelism": f"replicas x{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cap = 150.0
+        done, dt, cores = cpu_run(wl, args.steps, cap, warmup=min(args.warmup, 1))
+        val = done / dt
+        line = {"metric": METRIC, "value": val, "unit": "design iters/s", "n_gpus": args.gpus, "steps": done,
+                "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * dt / max(done, 1), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                "impl": "reference",
+                "cpu_baseline": {"value": val, "unit": "design iters/s", "cores": cores, "kind": "port",
+                                 "sample": f"{done} of {args.steps} requested design iterations after 1 untimed "
+                                           f"warm-up (time cap {cap:.0f} s); PETSc reference not buildable here, "
+                                           f"oracle port on all host threads"},
+                "e2e": {"value": val, "unit": "design iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = dist_mod
+    T = _pkg()
+    stream = torch.cuda.current_stream()
+    v, e, f, ld, lv = T.gen_cantilever(wl["nx"], wl["ny"], wl["nz"], wl["nen"])
+    t0 = time.perf_counter()
+    ctx = T.Context(v, e, f, ld, lv, precision=T.PREC_MIXED, **PARAMS)
+    setup_s = time.perf_counter() - t0
+    info0 = ctx.info()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    if args.only == "fp64":
+        ctx.set_params(precision=T.PREC_FP64)
+    ms, launches, prof, its = run_device(ctx, T, torch, args.steps, args.warmup, stream, dist)
+    clocks = sampler.stop()
+    if args.only:
+        ctx.close()
+        if rank == 0:
+            print(json.dumps({"only": args.only, "value": world * args.steps / (ms / 1e3), "ms": ms,
+                              "fgmres_its": its, "gpu_launches": launches}), flush=True)
+        return
+    e2e_ms, h2d, d2h = run_e2e(ctx, T, torch, args.steps, args.warmup, stream, dist)
+    ctx.set_params(precision=T.PREC_FP64)
+    ms64, _, prof64, its64 = run_device(ctx, T, torch, args.steps, args.warmup, stream, dist)
+
+    def maxr(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms, e2e_ms, ms64 = maxr(ms), maxr(e2e_ms), maxr(ms64)
+    value = world * args.steps / (ms / 1e3)
+    e2e_val = world * args.steps / (e2e_ms / 1e3)
+    val64 = world * args.steps / (ms64 / 1e3)
+
+    peak, peak_kind = peaks()
+    info = ctx.info()
+    kern = {}
+    n_kmv, t_kmv = prof.get("kmv", (0, 0.0))
+    if n_kmv:
+        b = kmv_bytes(ctx, 4)
+        kern["kmv_fp64_operator"] = {"launches": n_kmv, "avg_us": 1e3 * t_kmv / n_kmv,
+                                     "bytes": b, "gbs": b / (t_kmv / n_kmv * 1e-3) / 1e9}
+    n_c, t_c = prof.get("cheb0", (0, 0.0))
+    nnz0 = _graph_nnzb(e, ctx.nn)
+    if n_c:
+        b = cheb0_bytes(ctx, nnz0, 4)
+        kern["cheb0_bsr_fp32"] = {"launches": n_c, "avg_us": 1e3 * t_c / n_c, "bytes": b,
+                                  "gbs": b / (t_c / n_c * 1e-3) / 1e9}
+    n_r, t_r = prof.get("res0", (0, 0.0))
+    if n_r:
+        b = nnz0 * (9 * 4 + 4) + (ctx.nn + 1) * 4 + ctx.ndof * 3 * 4
+        kern["res0_bsr_fp32"] = {"launches": n_r, "avg_us": 1e3 * t_r / n_r, "bytes": b,
+                                 "gbs": b / (t_r / n_r * 1e-3) / 1e9}
+    dom_name, dom = max(kern.items(), key=lambda kv: kv[1]["launches"] * kv[1]["avg_us"])
+    traffic = _traffic(dom_name, ctx)
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
+                "frac": dom["gbs"] / peak, "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": dom["bytes"], "avg_launch_us": dom["avg_us"]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        done, dt, cores = cpu_run(wl, args.cpu_steps, 60.0, warmup=1)
+        cpu = {"value": done / dt, "unit": "design iters/s", "cores": cores, "kind": "port",
+               "sample": f"{done} design iteration(s) of the same workload after 1 untimed warm-up "
+                         f"(oracle port, OpenMP on {cores} threads)"}
+    ctx.close()
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    line = {"metric": METRIC, "value": value, "unit": "design iters/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (FGMRES, sensitivities, MMA) + f32 (AMG V-cycle)",
+            "data": "synthetic seeded jittered cantilever mesh", "config": cfg,
+            "fp64": {"value": val64, "ms_per_step": ms64 / args.steps, "fgmres_its": its64},
+            "mixed_over_fp64": value / val64, "fgmres_its": its, "setup_s": setup_s,
+            "amg_dofs": list(info.amg_dofs)[:info.amg_levels],
+            "e2e": {"value": e2e_val, "unit": "design iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "roofline": roofline, "kernels": kern, "clocks": clocks,
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def _graph_nnzb(element, nn):
+    """Number of 3x3 blocks of the level-0 operator (node pairs sharing an element)."""
+    import numpy as np
+    nen = element.shape[1]
+    a = np.repeat(element, nen, axis=1).ravel().astype(np.int64)
+    b = np.tile(element, (1, nen)).ravel().astype(np.int64)
+    return int(np.unique(a * nn + b).size)
+
+
+def _traffic(kernel, ctx):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    capture (profiles/traffic.json), scaled to this workload's element count."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            d = json.load(f)
+        rec = d[kernel]
+        return rec["dram_bytes_per_launch"] * ctx.ne / rec["elements"]
+    except Exception:
+        return None
+
+
+if __name__ == "__main__":
+    main()

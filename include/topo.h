@@ -198,13 +198,27 @@ int topo_opt_step(topo_ctx* ctx, int* itr, double* fx, double* gx0, double* ch);
 /* Runs the loop `while (itr < maxItr && ch > ch_tol)` (main.cpp:70);
  * hist (host, may be NULL) receives [fx, gx0, ch] per iteration. */
 int topo_opt_run(topo_ctx* ctx, int max_itr, double* hist, int* iterations);
-/* Host-buffer form used end to end: uploads X (host, n_elems), runs one
- * iteration, downloads XPhys (host) and returns fx. */
-int topo_opt_step_host(topo_ctx* ctx, const double* x_in, double* xphys_out, double* fx);
+/* Host-buffer form used end to end: uploads the design X (host, n_elems),
+ * runs one iteration, downloads the updated X and XPhys (host) and fx. */
+int topo_opt_step_host(topo_ctx* ctx, const double* x_in, double* x_out, double* xphys_out, double* fx);
 /* access to the context's design vectors; which: 0 X, 1 XPhys, 2 XFiled,
  * 3 Xold, 4 dfdx, 5 dgdx (m*n_elems), 6 xmin, 7 xmax.  Device pointer out. */
 int topo_opt_vector(topo_ctx* ctx, int which, double** ptr_d);
 int topo_solve_info_get(topo_ctx* ctx, topo_solve_info* info);
+
+/* ---------------------------------------------------------------- instrumentation */
+/* Kernel launches issued by this library in this process (all contexts). */
+long topo_kernel_launches(void);
+/* CUDA-event timing of the hot kernels on the context's stream (no host
+ * syncs added): slot 0 element operator K(x)u, 1 level-0 Chebyshev sweep,
+ * 2 level-0 residual, 3 Helmholtz-filter operator. */
+int topo_profile_enable(topo_ctx* ctx, int on);
+/* Synchronises, returns launches and summed milliseconds of a slot, resets it. */
+int topo_profile_read(topo_ctx* ctx, int slot, long* launches, double* total_ms);
+/* Greedy graph aggregation used for the AMG hierarchy (host only): rows
+ * (rp, ci; sorted, self included) of an n-node graph; excl[i] != 0 leaves
+ * node i out (-1).  Returns the aggregate count, agg[] the membership. */
+int topo_graph_aggregate(int n, const int32_t* rp, const int32_t* ci, const unsigned char* excl, int32_t* agg);
 
 /* ---------------------------------------------------------------- mesh files, output */
 /* Synthetic jittered cantilever lattice in the reference's formats (host):

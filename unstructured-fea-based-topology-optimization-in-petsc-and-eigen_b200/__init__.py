@@ -98,7 +98,11 @@ _SIGS = {
     "topo_opt_init": ([C.c_void_p], C.c_int),
     "topo_opt_step": ([C.c_void_p, C.POINTER(C.c_int), _dp, _dp, _dp], C.c_int),
     "topo_opt_run": ([C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)], C.c_int),
-    "topo_opt_step_host": ([C.c_void_p, C.c_void_p, C.c_void_p, _dp], C.c_int),
+    "topo_opt_step_host": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _dp], C.c_int),
+    "topo_kernel_launches": ([], C.c_long),
+    "topo_profile_enable": ([C.c_void_p, C.c_int], C.c_int),
+    "topo_profile_read": ([C.c_void_p, C.c_int, C.POINTER(C.c_long), _dp], C.c_int),
+    "topo_graph_aggregate": ([C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "topo_opt_vector": ([C.c_void_p, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "topo_solve_info_get": ([C.c_void_p, C.POINTER(SolveInfo)], C.c_int),
     "topo_gen_cantilever": ([C.c_int] * 4 + [C.c_double, C.c_uint64, C.c_int] + [C.c_void_p] * 5 +
@@ -128,6 +132,22 @@ def lib():
 
 def symbols():
     return list(_SIGS)
+
+
+def kernel_launches() -> int:
+    return lib().topo_kernel_launches()
+
+
+def graph_aggregate(rp, ci, excl=None):
+    """Greedy aggregation of a node graph (host; same routine the AMG uses)."""
+    rp = np.ascontiguousarray(rp, dtype=np.int32)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    n = rp.size - 1
+    agg = np.zeros(n, dtype=np.int32)
+    ex = None if excl is None else np.ascontiguousarray(excl, dtype=np.uint8)
+    na = _check(lib().topo_graph_aggregate(n, _ptr(rp), _ptr(ci), None if ex is None else _ptr(ex), _ptr(agg)),
+                "graph_aggregate")
+    return na, agg
 
 
 def last_error() -> str:
@@ -393,10 +413,20 @@ class Context:
         _check(lib().topo_opt_run(self.h, max_itr, _ptr(hist), C.byref(n)), "opt_run")
         return hist.reshape(-1, 3)[:n.value]
 
-    def opt_step_host(self, x_in: np.ndarray, xphys_out: np.ndarray):
+    def opt_step_host(self, x_in: np.ndarray, x_out: np.ndarray, xphys_out: np.ndarray):
+        """One design iteration with host buffers (x_in -> x_out, xphys_out)."""
         fx = C.c_double()
-        _check(lib().topo_opt_step_host(self.h, _ptr(x_in), _ptr(xphys_out), C.byref(fx)), "opt_step_host")
+        _check(lib().topo_opt_step_host(self.h, _ptr(x_in), _ptr(x_out), _ptr(xphys_out), C.byref(fx)),
+               "opt_step_host")
         return fx.value
+
+    def profile(self, on=True):
+        _check(lib().topo_profile_enable(self.h, 1 if on else 0), "profile_enable")
+
+    def profile_read(self, slot):
+        n, ms = C.c_long(), C.c_double()
+        _check(lib().topo_profile_read(self.h, slot, C.byref(n), C.byref(ms)), "profile_read")
+        return n.value, ms.value
 
     def opt_vector(self, which):
         """Device pointer (int) of one of the context's design vectors."""

@@ -102,14 +102,14 @@ int heaviside(Ctx& c, const double* xf, double* xp, double x0, double beta0, dou
     }
     if (itr < 30) c.beta_proj = beta0;
     else if (itr % 10 == 0) c.beta_proj = std::min(betamax, c.beta_tmp + 1);
-    k_heaviside<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, xf, xp, c.beta_proj, x0, Xmin);
+    k_heaviside<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, xf, xp, c.beta_proj, x0, Xmin), note_launch();
     c.beta_tmp = c.beta_proj;
     TCK(cudaGetLastError());
     return 0;
 }
 
 int projected_sens(Ctx& c, const double* xf, double* df, double* dg, int m, double x0) {
-    k_projsens<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, m, xf, df, dg, c.beta_proj, x0);
+    k_projsens<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, m, xf, df, dg, c.beta_proj, x0), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -175,10 +175,15 @@ int opt_init(Ctx& c) {
     TRET(opt_alloc(c));
     TRET(mma_alloc(c));
     const int n = c.ne;
-    for (double* v : {c.X.p, c.XF.p, c.XP.p, c.Xold.p}) k_fill<<<grid_for(n, 256), 256, 0, c.s>>>(n, v, c.p.volfrac);
+    for (double* v : {c.X.p, c.XF.p, c.XP.p, c.Xold.p}) k_fill<<<grid_for(n, 256), 256, 0, c.s>>>(n, v, c.p.volfrac), note_launch();
     TCK(cudaGetLastError());
     c.itr = 0;
     c.ch = 1.0;
+    // a fresh optimisation: MMA history, filter warm start and beta state
+    // start over as in a new process (MMA.cpp:178-224, PDEFilter.cpp:64-67)
+    c.mma_k = 0;
+    for (DBuf<double>* b : {&c.xo1, &c.xo2, &c.L, &c.Uas, &c.RX}) TRET(b->zero(c.s));
+    c.beta_proj = c.beta_tmp = c.p.beta0;
     TRET(filter_apply(c, c.X.p, c.XF.p, c.p.Xmin));
     TRET(heaviside(c, c.XF.p, c.XP.p, c.p.x0, c.p.beta0, c.p.betamax, c.itr, c.p.Xmin, c.p.proj));
     c.opt_ready = true;
@@ -200,7 +205,7 @@ int create(Ctx& c, int nen, int n_nodes, const double* vertex, int n_elems, cons
     TRET(sum_device(c, c.vol.p, c.ne, &c.TV));
     // filter: Jacobi diagonal of KF, work vectors, RX = 0 (VecDuplicate)
     TRET(c.fdiag_inv.alloc(c.nn));
-    k_filter_diag<<<(c.nn + 255) / 256, 256, 0, c.s>>>(c.nn, c.nen, c.nkf, c.n2e_ptr.p, c.n2e.p, c.kf.p, c.fdiag_inv.p);
+    k_filter_diag<<<(c.nn + 255) / 256, 256, 0, c.s>>>(c.nn, c.nen, c.nkf, c.n2e_ptr.p, c.n2e.p, c.kf.p, c.fdiag_inv.p), note_launch();
     TCK(cudaGetLastError());
     for (DBuf<double>* b : {&c.RX, &c.TX, &c.fr, &c.fz, &c.fp, &c.fw}) { TRET(b->alloc(c.nn)); TRET(b->zero(c.s)); }
     TRET(build_amg_host(c));
@@ -238,6 +243,19 @@ using namespace topo;
 struct topo_ctx {
     Ctx c;
 };
+
+namespace topo {
+cudaEvent_t prof_event(Ctx& c) {
+    if (c.prof.pool.empty()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+        return e;
+    }
+    cudaEvent_t e = c.prof.pool.back();
+    c.prof.pool.pop_back();
+    return e;
+}
+}  // namespace topo
 
 extern "C" {
 
@@ -349,6 +367,9 @@ int topo_destroy(topo_ctx* ctx) {
     cudaGetLastError();
     for (int i = 0; i < 4; i++)
         if (ctx->c.ev[i]) cudaEventDestroy(ctx->c.ev[i]);
+    for (auto e : ctx->c.prof.pool) cudaEventDestroy(e);
+    for (auto& r : ctx->c.prof.rec)
+        for (auto& pr : r) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     cudaStream_t s = ctx->c.s;
     bool own = ctx->c.own_stream;
     delete ctx;
@@ -632,14 +653,15 @@ int topo_opt_run(topo_ctx* ctx, int max_itr, double* hist, int* iterations) {
     return worst;
     GUARD_END
 }
-int topo_opt_step_host(topo_ctx* ctx, const double* x_in, double* xphys_out, double* fx) {
-    if (!ctx || !x_in || !xphys_out) { set_error("null argument"); return TOPO_ERR_ARG; }
+int topo_opt_step_host(topo_ctx* ctx, const double* x_in, double* x_out, double* xphys_out, double* fx) {
+    if (!ctx || !x_in || !x_out || !xphys_out) { set_error("null argument"); return TOPO_ERR_ARG; }
     GUARD_BEGIN
     Ctx& c = ctx->c;
     if (!c.opt_ready) TRET(opt_init(c));
     TCK(cudaMemcpyAsync(c.X.p, x_in, sizeof(double) * c.ne, cudaMemcpyHostToDevice, c.s));
     int rc = opt_step(c);
     TRET(rc);
+    TCK(cudaMemcpyAsync(x_out, c.X.p, sizeof(double) * c.ne, cudaMemcpyDeviceToHost, c.s));
     TCK(cudaMemcpyAsync(xphys_out, c.XP.p, sizeof(double) * c.ne, cudaMemcpyDeviceToHost, c.s));
     TCK(cudaStreamSynchronize(c.s));
     if (fx) *fx = c.info.last_fx;
@@ -662,6 +684,43 @@ int topo_solve_info_get(topo_ctx* ctx, topo_solve_info* info) {
     for (int l = 0; l < 8; l++) c.info.amg_dofs[l] = l < c.nlev ? c.dl[l].ndof : 0;
     *info = c.info;
     return 0;
+}
+
+// ---------------------------------------------------------------- instrumentation
+long topo_kernel_launches(void) { return __atomic_load_n(&launch_counter(), __ATOMIC_RELAXED); }
+
+int topo_profile_enable(topo_ctx* ctx, int on) {
+    if (!ctx) { set_error("null context"); return TOPO_ERR_ARG; }
+    ctx->c.prof.on = on != 0;
+    return 0;
+}
+
+int topo_profile_read(topo_ctx* ctx, int slot, long* launches, double* total_ms) {
+    if (!ctx || !launches || !total_ms || slot < 0 || slot >= PS_COUNT) { set_error("bad argument"); return TOPO_ERR_ARG; }
+    Ctx& c = ctx->c;
+    TCK(cudaStreamSynchronize(c.s));
+    double tot = 0.0;
+    for (auto& pr : c.prof.rec[slot]) {
+        float ms = 0.f;
+        TCK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        tot += ms;
+        c.prof.pool.push_back(pr.first);
+        c.prof.pool.push_back(pr.second);
+    }
+    *launches = (long)c.prof.rec[slot].size();
+    *total_ms = tot;
+    c.prof.rec[slot].clear();
+    return 0;
+}
+
+int topo_graph_aggregate(int n, const int32_t* rp, const int32_t* ci, const unsigned char* excl, int32_t* agg) {
+    if (n < 0 || !rp || !ci || !agg) { set_error("bad argument"); return TOPO_ERR_ARG; }
+    GUARD_BEGIN
+    std::vector<int> r(rp, rp + n + 1), cc(ci, ci + rp[n]), a;
+    int na = aggregate_graph(n, r, cc, excl, a);
+    std::copy(a.begin(), a.end(), agg);
+    return na;
+    GUARD_END
 }
 
 // ---------------------------------------------------------------- generator + files

@@ -467,7 +467,7 @@ static int alloc_vals(Ctx& c) {
             TRET(v.AP[l].alloc((size_t)D.AP.nnzb * bs * 6));
             TRET(v.R[l].alloc((size_t)D.R.nnzb * bs * 6));
         }
-        k_power_seed<T><<<grid_for(D.ndof, 256), 256, 0, c.s>>>(D.ndof, v.pv[l].p, c.rho.p + kMaxLevels + l);
+        k_power_seed<T><<<grid_for(D.ndof, 256), 256, 0, c.s>>>(D.ndof, v.pv[l].p, c.rho.p + kMaxLevels + l), note_launch();
     }
     TCK(cudaGetLastError());
     v.allocated = true;
@@ -500,7 +500,7 @@ static int spgemm(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp
     TCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (Cp.nrows + warps - 1) / warps;
     kern<<<grid, warps * 32, smem, c.s>>>(Cp.nrows, Ap.rp.p, Ap.ci.p, A, Bp.rp.p, Bp.ci.p, B, Cp.rp.p, Cp.ci.p, C,
-                                          std::max(Cp.maxrow, 1));
+                                          std::max(Cp.maxrow, 1)), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -513,15 +513,15 @@ static int spmv(Ctx& c, const DevPattern& Ap, const T* A, const T* x, T* y, cons
     if (avg <= 6.0) {
         constexpr int G = 8;
         k_bsr_spmv<T, BR, BC, G><<<(int)((nrows * G + 255) / 256), 256, 0, c.s>>>(
-            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal);
+            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal), note_launch();
     } else if (avg <= 20.0) {
         constexpr int G = 16;
         k_bsr_spmv<T, BR, BC, G><<<(int)((nrows * G + 255) / 256), 256, 0, c.s>>>(
-            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal);
+            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal), note_launch();
     } else {
         constexpr int G = 32;
         k_bsr_spmv<T, BR, BC, G><<<(int)((nrows * G + 255) / 256), 256, 0, c.s>>>(
-            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal);
+            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal), note_launch();
     }
     TCK(cudaGetLastError());
     return 0;
@@ -531,7 +531,14 @@ template <class T>
 static int level_spmv(Ctx& c, int l, const T* x, T* y, const T* b, int mode, const T* dinv = nullptr,
                       const double* scal = nullptr) {
     AmgVals<T>& v = vals<T>(c);
-    if (c.dl[l].bs == 3) return spmv<T, 3, 3>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal);
+    if (c.dl[l].bs == 3) {
+        cudaEvent_t e0;
+        const bool rec = l == 0 && mode == 1;
+        if (rec) prof_begin(c, PS_RES0, &e0);
+        int rc = spmv<T, 3, 3>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal);
+        if (rec) prof_end(c, PS_RES0, e0);
+        return rc;
+    }
     return spmv<T, 6, 6>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal);
 }
 
@@ -546,8 +553,8 @@ static int estimate_rho(Ctx& c, int l, int iters) {
     for (int it = 0; it < iters; it++) {
         // w = sigma Dinv A v with sigma = 1/||v||; lam = (sigma v).w; sigma' = 1/||w||
         TRET(level_spmv<T>(c, l, v.pv[l].p, v.pw[l].p, (const T*)nullptr, 3, v.dinv[l].p, scal));
-        k_dot2<T><<<nb, 256, 0, c.s>>>(D.ndof, v.pv[l].p, v.pw[l].p, scal, c.red.p);
-        k_power_final<<<1, 1024, 0, c.s>>>(nb, c.red.p, lam, scal);
+        k_dot2<T><<<nb, 256, 0, c.s>>>(D.ndof, v.pv[l].p, v.pw[l].p, scal, c.red.p), note_launch();
+        k_power_final<<<1, 1024, 0, c.s>>>(nb, c.red.p, lam, scal), note_launch();
         std::swap(v.pv[l], v.pw[l]);
     }
     TCK(cudaGetLastError());
@@ -570,12 +577,12 @@ static int numeric(Ctx& c) {
             auto k = k_assemble_A0<T, 8>;
             TCK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, ke, Ee, D.A.rp.p, D.A.ci.p,
-                                              c.dof_fixed.p, v.A[0].p, c.maxdeg);
+                                              c.dof_fixed.p, v.A[0].p, c.maxdeg), note_launch();
         } else {
             auto k = k_assemble_A0<T, 4>;
             TCK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, ke, Ee, D.A.rp.p, D.A.ci.p,
-                                              c.dof_fixed.p, v.A[0].p, c.maxdeg);
+                                              c.dof_fixed.p, v.A[0].p, c.maxdeg), note_launch();
         }
         TCK(cudaGetLastError());
     }
@@ -583,10 +590,10 @@ static int numeric(Ctx& c) {
         AmgDevLevel& D = c.dl[l];
         if (D.bs == 3)
             k_diag_inv<T, 3><<<grid_for(D.nnode, 256, 1 << 20), 256, 0, c.s>>>(D.nnode, D.A.rp.p, D.diagpos.p, v.A[l].p,
-                                                                           v.dinv[l].p);
+                                                                           v.dinv[l].p), note_launch();
         else
             k_diag_inv<T, 6><<<grid_for(D.nnode, 256, 1 << 20), 256, 0, c.s>>>(D.nnode, D.A.rp.p, D.diagpos.p, v.A[l].p,
-                                                                           v.dinv[l].p);
+                                                                           v.dinv[l].p), note_launch();
         TCK(cudaGetLastError());
         if (l == c.nlev - 1) break;
         TRET(estimate_rho<T>(c, l, l == 0 ? 6 : 10));
@@ -597,25 +604,25 @@ static int numeric(Ctx& c) {
             if (c.p.amg_smooth_p) {
                 TRET((spgemm<3, 3, 6, T>(c, D.A, v.A[l].p, D.Ptp, ptv, D.P, v.T_[l].p)));
                 k_smooth_p<T, 3><<<(D.nnode * 32 + 255) / 256, 256, 0, c.s>>>(
-                    D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p);
+                    D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p), note_launch();
             } else {
                 TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 18, cudaMemcpyDeviceToDevice, c.s));
             }
             TRET((spgemm<3, 3, 6, T>(c, D.A, v.A[l].p, D.P, v.P[l].p, D.AP, v.AP[l].p)));
             k_transpose<T, 3><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
-                                                                             D.P.rp.p, v.P[l].p, v.R[l].p);
+                                                                             D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();
             TRET((spgemm<6, 3, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p)));
         } else {
             if (c.p.amg_smooth_p) {
                 TRET((spgemm<6, 6, 6, T>(c, D.A, v.A[l].p, D.Ptp, ptv, D.P, v.T_[l].p)));
                 k_smooth_p<T, 6><<<(D.nnode * 32 + 255) / 256, 256, 0, c.s>>>(
-                    D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p);
+                    D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p), note_launch();
             } else {
                 TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 36, cudaMemcpyDeviceToDevice, c.s));
             }
             TRET((spgemm<6, 6, 6, T>(c, D.A, v.A[l].p, D.P, v.P[l].p, D.AP, v.AP[l].p)));
             k_transpose<T, 6><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
-                                                                             D.P.rp.p, v.P[l].p, v.R[l].p);
+                                                                             D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();
             TRET((spgemm<6, 6, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p)));
         }
         TCK(cudaGetLastError());
@@ -631,12 +638,12 @@ static int numeric(Ctx& c) {
         }
         TCK(cudaMemsetAsync(c.cA.p, 0, sizeof(double) * (size_t)n * 2 * n, c.s));
         if (D.bs == 3)
-            k_bsr_to_dense<T, 3><<<D.nnode, 128, 0, c.s>>>(D.nnode, D.A.rp.p, D.A.ci.p, v.A[L].p, c.cA.p, n);
+            k_bsr_to_dense<T, 3><<<D.nnode, 128, 0, c.s>>>(D.nnode, D.A.rp.p, D.A.ci.p, v.A[L].p, c.cA.p, n), note_launch();
         else
-            k_bsr_to_dense<T, 6><<<D.nnode, 128, 0, c.s>>>(D.nnode, D.A.rp.p, D.A.ci.p, v.A[L].p, c.cA.p, n);
+            k_bsr_to_dense<T, 6><<<D.nnode, 128, 0, c.s>>>(D.nnode, D.A.rp.p, D.A.ci.p, v.A[L].p, c.cA.p, n), note_launch();
         const size_t sm = sizeof(double) * (size_t)n;
         if (sm > 48 * 1024) TCK(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_gauss_jordan<<<1, 1024, sm, c.s>>>(n, c.cA.p, c.cinv.p, reinterpret_cast<int*>(c.rho.p + 3 * kMaxLevels));
+        k_gauss_jordan<<<1, 1024, sm, c.s>>>(n, c.cA.p, c.cinv.p, reinterpret_cast<int*>(c.rho.p + 3 * kMaxLevels)), note_launch();
         TCK(cudaGetLastError());
     }
     return 0;
@@ -673,26 +680,29 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
             TRET(level_spmv<T>(c, l, x, v.r[l].p, b, 1));
         }
     }
-    k_cheb_first<T><<<grid_for(n, 256), 256, 0, c.s>>>(n, b, v.r[l].p, v.d[l].p, x, v.dinv[l].p, rho, zero_init ? 1 : 0);
+    k_cheb_first<T><<<grid_for(n, 256), 256, 0, c.s>>>(n, b, v.r[l].p, v.d[l].p, x, v.dinv[l].p, rho, zero_init ? 1 : 0), note_launch();
     T* dcur = v.d[l].p;
     T* dnxt = v.d2[l].p;
     for (int k = 1; k < deg && k < 16; k++) {
         if (matfree) {
             if (std::is_same<T, float>::value) TRET(kmatvec32(c, (const float*)dcur, (float*)v.t[l].p, nullptr));
             else TRET(kmatvec64r(c, (const double*)dcur, (double*)v.t[l].p, nullptr));
-            k_cheb_upd<T><<<grid_for(n, 256), 256, 0, c.s>>>(n, v.t[l].p, v.r[l].p, dcur, x, v.dinv[l].p, rho, cr[k], cq[k]);
+            k_cheb_upd<T><<<grid_for(n, 256), 256, 0, c.s>>>(n, v.t[l].p, v.r[l].p, dcur, x, v.dinv[l].p, rho, cr[k], cq[k]), note_launch();
         } else {
             const int nrows = D.nnode;
             if (D.bs == 3) {
                 constexpr int G = 32;
+                cudaEvent_t e0;
+                if (l == 0) prof_begin(c, PS_CHEB0, &e0);
                 k_bsr_cheb<T, 3, G><<<(nrows * G + 255) / 256, 256, 0, c.s>>>(nrows, D.A.rp.p, D.A.ci.p, v.A[l].p, dcur,
                                                                             dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr[k],
-                                                                            cq[k]);
+                                                                            cq[k]), note_launch();
+                if (l == 0) prof_end(c, PS_CHEB0, e0);
             } else {
                 constexpr int G = 32;
                 k_bsr_cheb<T, 6, G><<<(nrows * G + 255) / 256, 256, 0, c.s>>>(nrows, D.A.rp.p, D.A.ci.p, v.A[l].p, dcur,
                                                                             dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr[k],
-                                                                            cq[k]);
+                                                                            cq[k]), note_launch();
             }
             std::swap(dcur, dnxt);
         }
@@ -724,7 +734,7 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
     }
     {
         const int n = c.dl[L].ndof;
-        k_dense_apply<T><<<(n * 32 + 255) / 256, 256, 0, c.s>>>(n, c.cinv.p, v.b[L].p, v.x[L].p);
+        k_dense_apply<T><<<(n * 32 + 255) / 256, 256, 0, c.s>>>(n, c.cinv.p, v.b[L].p, v.x[L].p), note_launch();
         TCK(cudaGetLastError());
     }
     for (int l = L - 1; l >= 0; l--) {
@@ -747,7 +757,7 @@ int amg_vcycle64(Ctx& c, const double* b, double* x) { return vcycle<double>(c, 
 int amg_vcycle32(Ctx& c, const double* b64, float* x) {
     AmgVals<float>& v = c.v32;
     const long n = c.dl[0].ndof;
-    k_convert<double, float><<<grid_for(n, 256), 256, 0, c.s>>>(n, b64, v.b[0].p);
+    k_convert<double, float><<<grid_for(n, 256), 256, 0, c.s>>>(n, b64, v.b[0].p), note_launch();
     TCK(cudaGetLastError());
     // level-0 rhs lives in v.b[0]; the smoother keeps b intact
     return vcycle<float>(c, v.b[0].p, x);

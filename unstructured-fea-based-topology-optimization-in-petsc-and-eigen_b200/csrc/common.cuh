@@ -27,6 +27,12 @@ int cuda_fail(cudaError_t e, const char* file, int line);
         if (r_ < 0) return r_;        \
     } while (0)
 
+// ----------------------------------------------------------------- launch accounting
+// Process-wide count of kernel launches issued by this library (every launch
+// site is followed by note_launch()); read through topo_kernel_launches().
+long& launch_counter();
+inline void note_launch() { __atomic_fetch_add(&launch_counter(), 1L, __ATOMIC_RELAXED); }
+
 // ----------------------------------------------------------------- buffers
 // Owning device allocation (cudaMalloc); never copied, only moved.
 template <class T>

@@ -152,7 +152,29 @@ struct Ctx {
 
     topo_solve_info info{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    // per-kernel CUDA-event timing of the hot kernels (off unless enabled)
+    struct Prof {
+        bool on = false;
+        std::vector<cudaEvent_t> pool;                 // free events
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rec[8];
+    } prof;
 };
+
+// profiler slots
+enum ProfSlot { PS_KMV = 0, PS_CHEB0 = 1, PS_RES0 = 2, PS_FILTER = 3, PS_SPGEMM = 4, PS_COUNT = 8 };
+cudaEvent_t prof_event(Ctx& c);
+inline void prof_begin(Ctx& c, int slot, cudaEvent_t* e0) {
+    *e0 = nullptr;
+    if (c.prof.on) { *e0 = prof_event(c); cudaEventRecord(*e0, c.s); }
+    (void)slot;
+}
+inline void prof_end(Ctx& c, int slot, cudaEvent_t e0) {
+    if (!c.prof.on || !e0) return;
+    cudaEvent_t e1 = prof_event(c);
+    cudaEventRecord(e1, c.s);
+    c.prof.rec[slot].push_back({e0, e1});
+}
 
 // ---- host builders (setup.cpp)
 int build_mesh(Ctx& c, const double* vertex, const int32_t* element, int n_fixed, const int32_t* fixed,

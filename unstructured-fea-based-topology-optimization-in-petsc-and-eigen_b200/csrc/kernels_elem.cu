@@ -261,10 +261,10 @@ int elem_setup(Ctx& c) {
     int grid = (int)(((long)c.ne * 32 + block - 1) / block);
     if (c.nen == 8)
         k_hex8_setup<<<grid, block, 0, c.s>>>(c.ne, c.elem.p, c.vertex.p, c.p.nu, c.p.rmin, c.ke64.p, c.ke32.p, c.vol.p,
-                                              c.kf.p, c.tf.p);
+                                              c.kf.p, c.tf.p), note_launch();
     else
         k_tet4_setup<<<grid, block, 0, c.s>>>(c.ne, c.elem.p, c.vertex.p, c.p.nu, c.p.rmin, c.ke64.p, c.ke32.p, c.vol.p,
-                                              c.kf.p, c.tf.p);
+                                              c.kf.p, c.tf.p), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -284,7 +284,7 @@ int compute_moduli(Ctx& c, const double* xphys) {
     int npad = c.ntiles * 32;
     if (!c.Ee64.p) { TRET(c.Ee64.alloc(npad)); TRET(c.Ee32.alloc(npad)); }
     k_moduli<<<grid_for(npad, 256, 1 << 20), 256, 0, c.s>>>(c.ne, npad, xphys, c.p.Emin, c.p.Emax, c.p.penal, c.Ee64.p,
-                                                           c.Ee32.p);
+                                                           c.Ee32.p), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -399,9 +399,9 @@ template <class TK, class TU, class TY>
 static int launch_kmv(Ctx& c, const TK* ke, const TK* Ee, const TU* u, TY* y, TK alpha) {
     int block = 128, grid = c.ntiles * 32 / block + 1;
     if (c.nen == 8)
-        k_kmv<8, TK, TU, TY><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, y, alpha);
+        k_kmv<8, TK, TU, TY><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, y, alpha), note_launch();
     else
-        k_kmv<4, TK, TU, TY><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, y, alpha);
+        k_kmv<4, TK, TU, TY><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, y, alpha), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -411,11 +411,14 @@ int kmatvec(Ctx& c, const double* Ee, const double* u, double* y, int ncase) {
     for (int k = 0; k < ncase; k++) {
         const double* uk = u + (size_t)k * c.ndof;
         double* yk = y + (size_t)k * c.ndof;
-        k_init_y<double><<<grid_for(c.ndof, 256), 256, 0, c.s>>>(c.ndof, yk, nullptr, 0.0);
+        k_init_y<double><<<grid_for(c.ndof, 256), 256, 0, c.s>>>(c.ndof, yk, nullptr, 0.0), note_launch();
+        cudaEvent_t e0;
+        prof_begin(c, PS_KMV, &e0);
         TRET(launch_kmv<double, double, double>(c, c.ke64.p, Ee, uk, yk, 1.0));
+        prof_end(c, PS_KMV, e0);
         if (!c.fixed_h.empty())
             k_fix_rows<double, double><<<grid_for((long)c.fixed_h.size(), 256), 256, 0, c.s>>>(
-                (int)c.fixed_h.size(), c.fixed.p, uk, yk, nullptr, 1.0, 0.0);
+                (int)c.fixed_h.size(), c.fixed.p, uk, yk, nullptr, 1.0, 0.0), note_launch();
     }
     TCK(cudaGetLastError());
     return 0;
@@ -423,11 +426,14 @@ int kmatvec(Ctx& c, const double* Ee, const double* u, double* y, int ncase) {
 
 // y = K(E) u with an FP32 input vector (the mixed form's preconditioned directions)
 int kmatvec_f32in(Ctx& c, const double* Ee, const float* u, double* y) {
-    k_init_y<double><<<grid_for(c.ndof, 256), 256, 0, c.s>>>(c.ndof, y, nullptr, 0.0);
+    k_init_y<double><<<grid_for(c.ndof, 256), 256, 0, c.s>>>(c.ndof, y, nullptr, 0.0), note_launch();
+    cudaEvent_t e0;
+    prof_begin(c, PS_KMV, &e0);
     TRET(launch_kmv<double, float, double>(c, c.ke64.p, Ee, u, y, 1.0));
+    prof_end(c, PS_KMV, e0);
     if (!c.fixed_h.empty())
         k_fix_rows<float, double><<<grid_for((long)c.fixed_h.size(), 256), 256, 0, c.s>>>(
-            (int)c.fixed_h.size(), c.fixed.p, u, y, nullptr, 1.0, 0.0);
+            (int)c.fixed_h.size(), c.fixed.p, u, y, nullptr, 1.0, 0.0), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -435,20 +441,20 @@ int kmatvec_f32in(Ctx& c, const double* Ee, const float* u, double* y) {
 // FP32 element operator for the mixed-precision fine-level smoother:
 // y = b - K u (residual form) or y = K u.
 int kmatvec32(Ctx& c, const float* u, float* y, const float* b) {
-    k_init_y<float><<<grid_for(c.ndof, 256), 256, 0, c.s>>>(c.ndof, y, b, 1.0f);
+    k_init_y<float><<<grid_for(c.ndof, 256), 256, 0, c.s>>>(c.ndof, y, b, 1.0f), note_launch();
     TRET(launch_kmv<float, float, float>(c, c.ke32.p, c.Ee32.p, u, y, b ? -1.0f : 1.0f));
     if (!c.fixed_h.empty())
         k_fix_rows<float, float><<<grid_for((long)c.fixed_h.size(), 256), 256, 0, c.s>>>(
-            (int)c.fixed_h.size(), c.fixed.p, u, y, b, b ? -1.0f : 1.0f, 1.0f);
+            (int)c.fixed_h.size(), c.fixed.p, u, y, b, b ? -1.0f : 1.0f, 1.0f), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
 int kmatvec64r(Ctx& c, const double* u, double* y, const double* b) {
-    k_init_y<double><<<grid_for(c.ndof, 256), 256, 0, c.s>>>(c.ndof, y, b, 1.0);
+    k_init_y<double><<<grid_for(c.ndof, 256), 256, 0, c.s>>>(c.ndof, y, b, 1.0), note_launch();
     TRET(launch_kmv<double, double, double>(c, c.ke64.p, c.Ee64.p, u, y, b ? -1.0 : 1.0));
     if (!c.fixed_h.empty())
         k_fix_rows<double, double><<<grid_for((long)c.fixed_h.size(), 256), 256, 0, c.s>>>(
-            (int)c.fixed_h.size(), c.fixed.p, u, y, b, b ? -1.0 : 1.0, 1.0);
+            (int)c.fixed_h.size(), c.fixed.p, u, y, b, b ? -1.0 : 1.0, 1.0), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -536,11 +542,11 @@ int fem_sensitivities(Ctx& c, const double* xphys, double* dfdx, double* dgdx) {
     if (!c.uku.p) TRET(c.uku.alloc(c.ne));
     for (int cs = 0; cs < c.ncases; cs++) {
         const double* Uc = c.U.p + (size_t)cs * c.ndof;
-        if (c.nen == 8) k_uku<8><<<(c.ne + 127) / 128, 128, 0, c.s>>>(c.ne, c.ndof, c.conn.p, c.ke64.p, Uc, c.uku.p, cs > 0);
-        else k_uku<4><<<(c.ne + 127) / 128, 128, 0, c.s>>>(c.ne, c.ndof, c.conn.p, c.ke64.p, Uc, c.uku.p, cs > 0);
+        if (c.nen == 8) k_uku<8><<<(c.ne + 127) / 128, 128, 0, c.s>>>(c.ne, c.ndof, c.conn.p, c.ke64.p, Uc, c.uku.p, cs > 0), note_launch();
+        else k_uku<4><<<(c.ne + 127) / 128, 128, 0, c.s>>>(c.ne, c.ndof, c.conn.p, c.ke64.p, Uc, c.uku.p, cs > 0), note_launch();
     }
-    k_sens<<<nb, block, 0, c.s>>>(c.ne, c.uku.p, xphys, c.vol.p, c.p.Emin, c.p.Emax, c.p.penal, c.TV, dfdx, dgdx, c.red.p);
-    k_sens_final<<<1, 1024, 0, c.s>>>(nb, c.red.p, c.TV, c.p.volfrac, c.p.m, c.dsc.p);
+    k_sens<<<nb, block, 0, c.s>>>(c.ne, c.uku.p, xphys, c.vol.p, c.p.Emin, c.p.Emax, c.p.penal, c.TV, dfdx, dgdx, c.red.p), note_launch();
+    k_sens_final<<<1, 1024, 0, c.s>>>(nb, c.red.p, c.TV, c.p.volfrac, c.p.m, c.dsc.p), note_launch();
     // additional constraints (m > 1) get zero sensitivities, like dgdx[j>0]
     // that the reference never writes after VecDuplicateVecs
     if (c.p.m > 1) TCK(cudaMemsetAsync(dgdx + c.ne, 0, sizeof(double) * (size_t)c.ne * (c.p.m - 1), c.s));
@@ -613,23 +619,26 @@ __global__ void k_tfxT(int ne, const int* __restrict__ conn, const double* __res
 int filter_tf(Ctx& c, const double* x, double* tx) {
     TCK(cudaMemsetAsync(tx, 0, sizeof(double) * c.nn, c.s));
     int g = (c.ne + 127) / 128;
-    if (c.nen == 8) k_tf<8><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.tf.p, x, tx);
-    else k_tf<4><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.tf.p, x, tx);
+    if (c.nen == 8) k_tf<8><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.tf.p, x, tx), note_launch();
+    else k_tf<4><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.tf.p, x, tx), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
 int filter_kf(Ctx& c, const double* r, double* y) {
     TCK(cudaMemsetAsync(y, 0, sizeof(double) * c.nn, c.s));
     int g = (c.ne + 127) / 128;
-    if (c.nen == 8) k_kf<8><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.kf.p, r, y);
-    else k_kf<4><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.kf.p, r, y);
+    cudaEvent_t e0;
+    prof_begin(c, PS_FILTER, &e0);
+    if (c.nen == 8) k_kf<8><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.kf.p, r, y), note_launch();
+    else k_kf<4><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.kf.p, r, y), note_launch();
+    prof_end(c, PS_FILTER, e0);
     TCK(cudaGetLastError());
     return 0;
 }
 int filter_tfxT(Ctx& c, const double* rx, double* xf, bool clamp, double xmin) {
     int g = (c.ne + 127) / 128;
-    if (c.nen == 8) k_tfxT<8><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, rx, xf, clamp ? 1 : 0, xmin);
-    else k_tfxT<4><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, rx, xf, clamp ? 1 : 0, xmin);
+    if (c.nen == 8) k_tfxT<8><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, rx, xf, clamp ? 1 : 0, xmin), note_launch();
+    else k_tfxT<4><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, rx, xf, clamp ? 1 : 0, xmin), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -682,7 +691,7 @@ __global__ void k_vm_hex8(int ne, const int* __restrict__ elem, const double* __
 
 int von_mises(Ctx& c, const double* xphys, double* vms) {
     if (c.nen != 8) { set_error("von Mises stress is implemented for hex8 meshes"); return TOPO_ERR_UNSUPPORTED; }
-    k_vm_hex8<<<(c.ne + 127) / 128, 128, 0, c.s>>>(c.ne, c.elem.p, c.vertex.p, c.U.p, xphys, c.p.nu, c.p.Emax, vms);
+    k_vm_hex8<<<(c.ne + 127) / 128, 128, 0, c.s>>>(c.ne, c.elem.p, c.vertex.p, c.U.p, xphys, c.p.nu, c.p.Emax, vms), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }

@@ -440,7 +440,7 @@ int mma_alloc(Ctx& c) {
 }
 
 int mma_movelimit(Ctx& c, double Xmin, double Xmax, double movlim, const double* x, double* xmin, double* xmax) {
-    k_movelimit<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, Xmin, Xmax, movlim, x, xmin, xmax);
+    k_movelimit<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, Xmin, Xmax, movlim, x, xmin, xmax), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -454,8 +454,8 @@ static int update_m(Ctx& c, double* x, const double* dfdx, const double* gx_dev,
     c.mma_k++;
     k_gensub<M><<<kMmaBlocks, 256, 0, c.s>>>(n, c.mma_k, c.asyminit, c.asymdec, c.asyminc, c.robust_type,
                                             c.constraint_mod, x, c.xo1.p, c.xo2.p, xmin, xmax, dfdx, dgdx, c.L.p,
-                                            c.Uas.p, c.alpha.p, c.beta.p, c.p0.p, c.q0.p, c.pij.p, c.qij.p, part);
-    k_gensub_final<<<1, 256, 0, c.s>>>(kMmaBlocks, M, part, gx_dev, ms);
+                                            c.Uas.p, c.alpha.p, c.beta.p, c.p0.p, c.q0.p, c.pij.p, c.qij.p, part), note_launch();
+    k_gensub_final<<<1, 256, 0, c.s>>>(kMmaBlocks, M, part, gx_dev, ms), note_launch();
     TCK(cudaGetLastError());
     // Update: xo2 <- xo1, xo1 <- xval (MMA.cpp:496-497)
     TCK(cudaMemcpyAsync(c.xo2.p, c.xo1.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c.s));
@@ -481,6 +481,7 @@ static int update_m(Ctx& c, double* x, const double* dfdx, const double* gx_dev,
     int nn = n;
     void* args[] = {&nn, &x, &p0, &q0, &pij, &qij, &Lp, &Up, &al, &be, &ms, &kc, &tol, &part1, &part2, &gb};
     TCK(cudaLaunchCooperativeKernel((void*)k_solvedip<M>, dim3(blocks), dim3(256), args, 0, c.s));
+    note_launch();
     // barrier status + iteration count
     TCK(cudaMemcpyAsync(c.hsc.h + 200, ms + MS_ITS, sizeof(double), cudaMemcpyDeviceToHost, c.s));
     int herr = 0;
@@ -506,8 +507,8 @@ int mma_update(Ctx& c, double* x, const double* dfdx, const double* gx_dev, cons
 int mma_design_change(Ctx& c, const double* x, double* xold, double* ch_dev) {
     TRET(mma_alloc(c));
     double* part = c.mma_scal.p + kMmaSlots;
-    k_design_change<<<kMmaBlocks, 256, 0, c.s>>>(c.ne, x, xold, part);
-    k_max_final<<<1, 256, 0, c.s>>>(kMmaBlocks, part, ch_dev);
+    k_design_change<<<kMmaBlocks, 256, 0, c.s>>>(c.ne, x, xold, part), note_launch();
+    k_max_final<<<1, 256, 0, c.s>>>(kMmaBlocks, part, ch_dev), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -518,12 +519,12 @@ int mma_kkt(Ctx& c, const double* x, const double* dfdx, const double* gx_dev, c
     double* part = c.mma_scal.p + kMmaSlots;
     double* out = c.dsc.p + DS_KKT;
     switch (c.p.m) {
-        case 1: k_kkt<1><<<kMmaBlocks, 256, 0, c.s>>>(c.ne, x, xmin, xmax, dfdx, dgdx, c.mma_scal.p, part); break;
-        case 2: k_kkt<2><<<kMmaBlocks, 256, 0, c.s>>>(c.ne, x, xmin, xmax, dfdx, dgdx, c.mma_scal.p, part); break;
-        case 3: k_kkt<3><<<kMmaBlocks, 256, 0, c.s>>>(c.ne, x, xmin, xmax, dfdx, dgdx, c.mma_scal.p, part); break;
-        default: k_kkt<4><<<kMmaBlocks, 256, 0, c.s>>>(c.ne, x, xmin, xmax, dfdx, dgdx, c.mma_scal.p, part); break;
+        case 1: k_kkt<1><<<kMmaBlocks, 256, 0, c.s>>>(c.ne, x, xmin, xmax, dfdx, dgdx, c.mma_scal.p, part), note_launch(); break;
+        case 2: k_kkt<2><<<kMmaBlocks, 256, 0, c.s>>>(c.ne, x, xmin, xmax, dfdx, dgdx, c.mma_scal.p, part), note_launch(); break;
+        case 3: k_kkt<3><<<kMmaBlocks, 256, 0, c.s>>>(c.ne, x, xmin, xmax, dfdx, dgdx, c.mma_scal.p, part), note_launch(); break;
+        default: k_kkt<4><<<kMmaBlocks, 256, 0, c.s>>>(c.ne, x, xmin, xmax, dfdx, dgdx, c.mma_scal.p, part), note_launch(); break;
     }
-    k_kkt_final<<<1, 256, 0, c.s>>>(kMmaBlocks, part, out);
+    k_kkt_final<<<1, 256, 0, c.s>>>(kMmaBlocks, part, out), note_launch();
     TCK(cudaGetLastError());
     double h[2 + 3 * kMaxM + 1], gxh[kMaxM];
     TCK(cudaMemcpyAsync(c.hsc.h + 210, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));

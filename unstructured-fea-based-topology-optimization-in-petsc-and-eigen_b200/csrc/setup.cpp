@@ -27,6 +27,11 @@ void set_error(const char* fmt, ...) {
 }
 const char* last_error() { return g_err.c_str(); }
 
+long& launch_counter() {
+    static long n = 0;
+    return n;
+}
+
 int cuda_fail(cudaError_t e, const char* file, int line) {
     set_error("CUDA error %s (%s) at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e), file, line);
     return e == cudaErrorMemoryAllocation ? TOPO_ERR_OOM : TOPO_ERR_CUDA;

@@ -40,13 +40,13 @@ __global__ void k_final(int nb, int nv, const double* __restrict__ part, double*
 }
 
 int finalize_sum(Ctx& c, const double* partials, int nparts, int nv, double* out_dev) {
-    k_final<<<1, 512, 0, c.s>>>(nparts, nv, partials, out_dev, -1);
+    k_final<<<1, 512, 0, c.s>>>(nparts, nv, partials, out_dev, -1), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
 int dev_dot(Ctx& c, const double* a, const double* b, long n, double* out_dev) {
     if ((long)c.red.n < kRedBlocks * 40L) TRET(c.red.alloc(std::max<long>(kRedBlocks * 40L, 4096)));
-    k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, a, b, c.red.p);
+    k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, a, b, c.red.p), note_launch();
     return finalize_sum(c, c.red.p, kRedBlocks, 1, out_dev);
 }
 
@@ -111,18 +111,18 @@ __global__ void k_update(long n, int kd, const TZ* __restrict__ Z, long ld, cons
 
 static int mdot(Ctx& c, int nv, const double* V, long ld, const double* w, double* out) {
     long n = c.ndof;
-    if (nv <= 8) k_mdot<8><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p);
-    else if (nv <= 16) k_mdot<16><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p);
-    else k_mdot<32><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p);
+    if (nv <= 8) k_mdot<8><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p), note_launch();
+    else if (nv <= 16) k_mdot<16><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p), note_launch();
+    else k_mdot<32><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p), note_launch();
     TCK(cudaGetLastError());
     return finalize_sum(c, c.red.p, kRedBlocks, nv, out);
 }
 static int orth(Ctx& c, int nv, const double* V, long ld, const double* h, double* w, double* hn_out) {
     long n = c.ndof;
-    if (nv <= 8) k_orth<8><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p);
-    else if (nv <= 16) k_orth<16><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p);
-    else k_orth<32><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p);
-    k_final<<<1, 512, 0, c.s>>>(kRedBlocks, 1, c.red.p, hn_out, 0);
+    if (nv <= 8) k_orth<8><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p), note_launch();
+    else if (nv <= 16) k_orth<16><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p), note_launch();
+    else k_orth<32><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p), note_launch();
+    k_final<<<1, 512, 0, c.s>>>(kRedBlocks, 1, c.red.p, hn_out, 0), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -172,7 +172,7 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
         if (beta <= ttol) { conv = true; break; }
         hs[70] = beta;
         TCK(cudaMemcpyAsync(c.wtmp.p, hs + 70, sizeof(double), cudaMemcpyHostToDevice, c.s));
-        k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, c.wtmp.p, c.V.p, 1);
+        k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, c.wtmp.p, c.V.p, 1), note_launch();
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
         int kdone = 0;
@@ -184,7 +184,7 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
             TRET(mdot(c, j + 1, c.V.p, n, c.w.p, gm));
             TRET(orth(c, j + 1, c.V.p, n, gm, c.w.p, gm + j + 1));
             TCK(cudaMemcpyAsync(hs, gm, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, c.s));
-            k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, gm + j + 1, c.V.p + (size_t)(j + 1) * n, 1);
+            k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, gm + j + 1, c.V.p + (size_t)(j + 1) * n, 1), note_launch();
             TCK(cudaStreamSynchronize(c.s));
             for (int i = 0; i <= j + 1; i++) H[(size_t)i * m + j] = hs[i];
             const double hn = hs[j + 1];
@@ -215,9 +215,9 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
         for (int k = 0; k < kdone; k++) hs[80 + k] = yv[k];
         TCK(cudaMemcpyAsync(c.wtmp.p, hs + 80, sizeof(double) * kdone, cudaMemcpyHostToDevice, c.s));
         if (c.p.precision == TOPO_PREC_MIXED)
-            k_update<float><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z32.p, n, c.wtmp.p, x);
+            k_update<float><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z32.p, n, c.wtmp.p, x), note_launch();
         else
-            k_update<double><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z64.p, n, c.wtmp.p, x);
+            k_update<double><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z64.p, n, c.wtmp.p, x), note_launch();
         TCK(cudaGetLastError());
         TCK(cudaStreamSynchronize(c.s));  // pinned y buffer reused next cycle
     }
@@ -326,8 +326,8 @@ int filter_cg(Ctx& c, const double* b, double* x, int* its_out) {
     double* hs = c.hsc.h + 96;
     if ((long)c.red.n < kRedBlocks * 40L) TRET(c.red.alloc(std::max<long>(kRedBlocks * 40L, 4096)));
     TRET(filter_kf(c, x, c.fw.p));
-    k_cg_start<<<kRedBlocks, 256, 0, c.s>>>(n, b, c.fw.p, c.fdiag_inv.p, c.fr.p, c.fz.p, c.red.p);
-    k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 3, c.red.p, sc, 1);
+    k_cg_start<<<kRedBlocks, 256, 0, c.s>>>(n, b, c.fw.p, c.fdiag_inv.p, c.fr.p, c.fz.p, c.red.p), note_launch();
+    k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 3, c.red.p, sc, 1), note_launch();
     TCK(cudaMemcpyAsync(hs, sc, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
     TCK(cudaStreamSynchronize(c.s));
     const double snorm = hs[0];
@@ -340,12 +340,12 @@ int filter_cg(Ctx& c, const double* b, double* x, int* its_out) {
     do {
         *its_out = i + 1;
         if (hs[2] == 0.0) return 0;  // beta == 0
-        k_cg_p<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.fz.p, c.fp.p, sc, i == 0);
+        k_cg_p<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.fz.p, c.fp.p, sc, i == 0), note_launch();
         TRET(filter_kf(c, c.fp.p, c.fw.p));
-        k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.red.p);
-        k_final<<<1, 512, 0, c.s>>>(kRedBlocks, 1, c.red.p, sc + 4, -1);
-        k_cg_step<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.fdiag_inv.p, x, c.fr.p, c.fz.p, sc, c.red.p);
-        k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 2, c.red.p, sc, 0);
+        k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.red.p), note_launch();
+        k_final<<<1, 512, 0, c.s>>>(kRedBlocks, 1, c.red.p, sc + 4, -1), note_launch();
+        k_cg_step<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.fdiag_inv.p, x, c.fr.p, c.fz.p, sc, c.red.p), note_launch();
+        k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 2, c.red.p, sc, 0), note_launch();
         TCK(cudaMemcpyAsync(hs, sc, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
         TCK(cudaStreamSynchronize(c.s));
         dp = hs[1];
