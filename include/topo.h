@@ -242,7 +242,8 @@ int topo_read_mesh_dir(const char* dir, int nen, int n_cases, double* vertex, in
  * diagonal->VTK node reorder, cell type 12 (hex8) / 10 (tet4), point data
  * ux uy uz and cell data xphys, from the context's last U and XPhys.
  * itr 0 -> output_initial.vtu, -1 -> output_final.vtu, else output_<itr>.vtu. */
-int topo_write_vtu(topo_ctx* ctx, const char* dir, int itr);
+int topo_write_vtu(topo_ctx* ctx, const char* dir, int itr, const double* xphys_d);
+/* (xphys_d: element densities to write, device; NULL = the context's own XPhys) */
 
 #ifdef __cplusplus
 }

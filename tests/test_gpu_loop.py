@@ -1,0 +1,96 @@
+"""The main.cpp loop on the GPU against the oracle's loop, and the
+mixed-precision form against the FP64 form.
+
+Bars: per-iteration compliance within 1e-3 relative over a 50-iteration
+trajectory at FGMRES rtol 1e-5 (solver iterates differ at the 1e-5 level
+and the design evolves from them); the mixed-precision form's compliance
+within 1e-6 relative of FP64 on a fixed density, and its trajectory within
+1e-3."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(Emax=1.0, rmin=1.5, volfrac=0.12, fem_rtol=1e-5, ch_tol=0.0)
+
+
+@pytest.fixture(scope="module")
+def mesh(T):
+    return T.gen_cantilever(40, 20, 10, 8)
+
+
+def test_trajectory_50_iterations(T, O, cuda, mesh):
+    v, e, f, ld, lv = mesh
+    ctx = T.Context(v, e, f, ld, lv, **KW)
+    ctx.opt_init()
+    hist = ctx.opt_run(50)
+    orc = O.Oracle(v, e, f, ld, lv, **{k: x for k, x in KW.items() if k != "ch_tol"})
+    ohist, oxp = orc.run(50, ch_tol=0.0)
+    assert hist.shape == (50, 3) and ohist.shape == (50, 3)
+    relf = np.abs(hist[:, 0] - ohist[:, 0]) / np.abs(ohist[:, 0])
+    assert relf.max() < 1e-3, relf
+    assert np.abs(hist[:, 1] - ohist[:, 1]).max() < 1e-3  # volume constraint
+    assert hist[-1, 0] < 0.05 * hist[0, 0]  # the optimiser makes progress
+    xp = ctx.opt_tensor(1).cpu().numpy()
+    assert np.abs(xp - oxp).max() < 5e-2  # final designs agree pointwise
+    ctx.close()
+
+
+def test_mixed_precision_compliance(T, cuda, mesh):
+    v, e, f, ld, lv = mesh
+    x = cuda.tensor(np.random.default_rng(11).uniform(0.01, 1.0, e.shape[0]), device="cuda")
+    out = {}
+    for prec in (T.PREC_FP64, T.PREC_MIXED):
+        ctx = T.Context(v, e, f, ld, lv, precision=prec, **KW)
+        fx, gx, df, dg, rc = ctx.fem_obj_sens(x)
+        assert rc == 0 and ctx.info().fem_relres < 1e-5
+        out[prec] = (fx, df.cpu().numpy())
+        ctx.close()
+    assert abs(out[1][0] - out[0][0]) <= 1e-6 * abs(out[0][0])
+    assert rel(out[1][1], out[0][1]) < 1e-4
+
+
+def test_mixed_trajectory(T, cuda, mesh):
+    v, e, f, ld, lv = mesh
+    h = {}
+    for prec in (T.PREC_FP64, T.PREC_MIXED):
+        ctx = T.Context(v, e, f, ld, lv, precision=prec, **KW)
+        ctx.opt_init()
+        h[prec] = ctx.opt_run(20)
+        ctx.close()
+    relf = np.abs(h[1][:, 0] - h[0][:, 0]) / np.abs(h[0][:, 0])
+    assert relf.max() < 1e-3
+
+
+def test_stop_rule_and_restart(T, cuda, mesh):
+    """`while (itr < maxItr && ch > 0.01)` (main.cpp:70) and a fresh
+    opt_init reproduce the same trajectory."""
+    v, e, f, ld, lv = mesh
+    ctx = T.Context(v, e, f, ld, lv, **dict(KW, ch_tol=0.05))
+    ctx.opt_init()
+    h1 = ctx.opt_run(200)
+    assert h1.shape[0] < 200 and h1[-1, 2] <= 0.05 and np.all(h1[:-1, 2] > 0.05)
+    ctx.opt_init()
+    h2 = ctx.opt_run(200)
+    assert h2.shape == h1.shape and rel(h2[:, 0], h1[:, 0]) < 1e-6
+    ctx.close()
+
+
+def test_host_buffer_step_matches_device_step(T, cuda, mesh):
+    v, e, f, ld, lv = mesh
+    a = T.Context(v, e, f, ld, lv, **KW)
+    b = T.Context(v, e, f, ld, lv, **KW)
+    a.opt_init()
+    b.opt_init()
+    x = np.full(e.shape[0], 0.12)
+    xo, xp = np.zeros_like(x), np.zeros_like(x)
+    for _ in range(3):
+        _, fxa, _, _ = a.opt_step()
+        fxb = b.opt_step_host(x, xo, xp)
+        x = xo.copy()
+        assert abs(fxa - fxb) <= 1e-9 * abs(fxa)
+    assert rel(xp, a.opt_tensor(1).cpu().numpy()) < 1e-9
+    a.close()
+    b.close()

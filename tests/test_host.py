@@ -1,0 +1,127 @@
+"""Host-side logic and the C-ABI boundary, without a GPU: the library loads,
+exports every symbol include/topo.h declares, its host routines (mesh
+generator, graph aggregation, mesh-file reader, argument validation) agree
+with the oracle and fail loudly on bad input."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "topo.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(topo_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol(T):
+    L = T.lib()
+    syms = header_symbols()
+    assert len(syms) >= 40
+    for s in syms:
+        assert hasattr(L, s), s
+    assert sorted(T.symbols()) == syms  # the ctypes bindings cover the header exactly
+
+
+def test_version_and_defaults(T):
+    assert b"sm_100a" in T.lib().topo_version()
+    p = T.default_params()
+    # OptPara.cpp:66-78, SolveFem.cpp:11,134, PDEFilter.cpp:117-120
+    assert (p.Emin, p.Emax, p.volfrac, p.penal, p.rmin, p.Xmin, p.Xmax, p.movlim) == \
+        (1e-9, 1e6, 0.12, 3.0, 0.01, 0.01, 1.0, 0.2)
+    assert (p.x0, p.beta0, p.betamax, p.proj, p.maxItr, p.m, p.nu) == (0.5, 1.0, 8.0, 0, 200, 1, 0.3)
+    assert (p.fem_rtol, p.filter_rtol, p.filter_atol, p.filter_dtol, p.filter_maxit) == (1e-5, 1e-5, 1e-50, 1e5, 10000)
+
+
+@pytest.mark.parametrize("nen", [8, 4])
+def test_generator_matches_oracle_bit_exact(T, O, nen):
+    v, e, f, ld, lv = T.gen_cantilever(9, 5, 4, nen)
+    v2, e2, f2, ld2, lv2 = O.cantilever(9, 5, 4, elem="hex8" if nen == 8 else "tet4")
+    for a, b in [(v, v2), (e, e2), (f, f2), (ld, ld2), (lv, lv2)]:
+        assert np.array_equal(a, b)
+    m1 = T.gen_multiload(9, 5, 4, 8)
+    m2 = O.multiload(9, 5, 4, 8)
+    assert np.array_equal(m1[0], m2[0]) and np.array_equal(m1[1], m2[1])
+
+
+def test_generator_lattice_layout(T):
+    nx, ny, nz = 5, 3, 2
+    v, e, f, ld, lv = T.gen_cantilever(nx, ny, nz, 8, jitter=0.0)
+    assert v.shape == ((nx + 1) * (ny + 1) * (nz + 1), 3) and e.shape == (nx * ny * nz, 8)
+    # diagonal local numbering: local l = a + 2b + 4c -> offset (a, b, c)
+    co = v[e[0]]
+    assert np.array_equal(co, [[l & 1, (l >> 1) & 1, (l >> 2) & 1] for l in range(8)])
+    # x = 0 face clamped, unit total -z load on the x = L, z = 0 edge
+    assert f.size == 3 * (ny + 1) * (nz + 1) and np.all(v[f // 3, 0] == 0)
+    assert np.all(ld % 3 == 2) and abs(lv.sum() + 1.0) < 1e-15
+    assert np.all(v[ld // 3, 0] == nx) and np.all(v[ld // 3, 2] == 0)
+
+
+def test_aggregation_matches_oracle(T, O):
+    """Integer work, compared bit-exactly: the library's greedy aggregation of
+    the level-0 node graph equals the oracle's."""
+    v, e, f, ld, lv = T.gen_cantilever(14, 7, 5, 8)
+    orc = O.Oracle(v, e, f, ld, lv, Emax=1.0, rmin=1.5)
+    orc.assemble(np.full(e.shape[0], 0.5))
+    na_o, agg_o = orc.amg_aggregates(0)
+    nn = v.shape[0]
+    # node graph from the mesh (self included, sorted)
+    nbr = [set() for _ in range(nn)]
+    for el in e:
+        for a in el:
+            nbr[a].update(el.tolist())
+    rp = np.zeros(nn + 1, dtype=np.int32)
+    rp[1:] = np.cumsum([len(s) for s in nbr])
+    ci = np.concatenate([sorted(s) for s in nbr]).astype(np.int32)
+    fixed_nodes = np.zeros(nn, dtype=np.uint8)
+    fixed_nodes[np.unique(f // 3)] = 1
+    na, agg = T.graph_aggregate(rp, ci, fixed_nodes)
+    agg_o = agg_o[:nn].copy()
+    agg_o[agg_o == -2] = -1
+    assert na == na_o
+    assert np.array_equal(agg, agg_o)
+    assert np.all(agg[fixed_nodes == 1] == -1)
+    sizes = np.bincount(agg[agg >= 0])
+    assert sizes.min() >= 2 and abs(sizes.mean() - 27) < 12
+
+
+def test_mesh_dir_roundtrip(T, tmp_path):
+    v, e, f, ld, lv = T.gen_cantilever(3, 2, 2, 8)
+    np.savetxt(tmp_path / "vertex.txt", v, fmt="%.17g")
+    np.savetxt(tmp_path / "element.txt", e, fmt="%d")
+    np.savetxt(tmp_path / "fixeddofs.txt", f, fmt="%d")
+    np.savetxt(tmp_path / "loaddof_1.txt", ld[None, :], fmt="%d", delimiter="\t")
+    np.savetxt(tmp_path / "load_1.txt", lv[None, :], fmt="%.17g", delimiter="\t")
+    v2, e2, f2, ld2, lv2, cp = T.read_mesh_dir(str(tmp_path), 8, 1)
+    assert np.array_equal(v, v2) and np.array_equal(e, e2) and np.array_equal(f, f2)
+    assert np.array_equal(ld, ld2) and np.array_equal(lv, lv2) and list(cp) == [0, ld.size]
+    with pytest.raises(T.TopoError) as ei:
+        T.read_mesh_dir(str(tmp_path / "missing"), 8, 1)
+    assert ei.value.code == -8  # TOPO_ERR_IO ("Can't found document")
+
+
+def _create(T, v, e, f, ld, lv, **kw):
+    return T.Context(v, e, f, ld, lv, stream=0, **kw)
+
+
+def test_invalid_mesh_rejected_before_any_device_work(T):
+    v, e, f, ld, lv = T.gen_cantilever(3, 2, 2, 8)
+    bad = e.copy()
+    bad[1, 3] = v.shape[0] + 5
+    with pytest.raises(T.TopoError) as ei:
+        _create(T, v, bad, f, ld, lv)
+    assert ei.value.code == -4 and "outside" in str(ei.value)
+    vn = v.copy()
+    vn[2, 1] = np.nan
+    with pytest.raises(T.TopoError) as ei:
+        _create(T, vn, e, f, ld, lv)
+    assert ei.value.code == -4 and "not finite" in str(ei.value)
+    with pytest.raises(T.TopoError) as ei:
+        _create(T, v, e, f, ld, lv * np.nan)
+    assert ei.value.code == -4
+    with pytest.raises(T.TopoError) as ei:
+        _create(T, v, e, f, ld, lv, m=9)
+    assert ei.value.code == -1

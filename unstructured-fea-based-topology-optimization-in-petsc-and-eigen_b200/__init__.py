@@ -109,7 +109,7 @@ _SIGS = {
                             [C.POINTER(C.c_int)] * 4, C.c_int),
     "topo_gen_multiload": ([C.c_int] * 4 + [C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
     "topo_read_mesh_dir": ([C.c_char_p, C.c_int, C.c_int] + [C.c_void_p] * 6 + [C.POINTER(C.c_int)] * 4, C.c_int),
-    "topo_write_vtu": ([C.c_void_p, C.c_char_p, C.c_int], C.c_int),
+    "topo_write_vtu": ([C.c_void_p, C.c_char_p, C.c_int, C.c_void_p], C.c_int),
 }
 
 _lib = None
@@ -440,8 +440,8 @@ class Context:
         n = n or (self.ne * self.m if which == 5 else self.ne)
         return device_view(self.opt_vector(which), n).clone()
 
-    def write_vtu(self, directory, itr):
-        _check(lib().topo_write_vtu(self.h, directory.encode(), itr), "write_vtu")
+    def write_vtu(self, directory, itr, xphys=None):
+        _check(lib().topo_write_vtu(self.h, directory.encode(), itr, _dptr(xphys)), "write_vtu")
 
 
 def device_view(ptr, n):

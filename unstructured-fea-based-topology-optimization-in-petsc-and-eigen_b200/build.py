@@ -57,6 +57,16 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    # the main.cpp-shaped driver program over the C++ classes (include/topopt.hpp)
+    exe = os.path.join(HERE, "topopt")
+    src = os.path.join(HERE, "host", "topopt_main.cpp")
+    hdrs = [os.path.join(INCLUDE, h) for h in ("topo.h", "topopt.hpp")]
+    if force or not os.path.exists(exe) or any(os.path.getmtime(p) > os.path.getmtime(exe) for p in [src, LIB] + hdrs):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, src, "-L", HERE, "-ltopo", "-Wl,-rpath,$ORIGIN",
+               "-o", exe]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"topopt build failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

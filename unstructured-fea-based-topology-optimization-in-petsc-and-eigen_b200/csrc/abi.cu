@@ -269,7 +269,7 @@ void topo_params_default(topo_params* p) {
     p->Xmin = 0.01; p->Xmax = 1.0; p->movlim = 0.2; p->x0 = 0.5; p->beta0 = 1.0; p->betamax = 8.0;
     p->proj = 0; p->maxItr = 200; p->m = 1; p->ch_tol = 0.01;
     p->fem_rtol = 1.0e-5; p->fem_restart = 30; p->fem_maxit = 10000;
-    p->precision = TOPO_PREC_FP64; p->amg_max_levels = 8; p->amg_coarse_max = 500; p->amg_smooth_p = 1;
+    p->precision = TOPO_PREC_FP64; p->amg_max_levels = 8; p->amg_coarse_max = 100; p->amg_smooth_p = 1;
     p->cheb_degree = 2; p->fine_smoother_matfree = 0;
     p->filter_rtol = 1.0e-5; p->filter_atol = 1.0e-50; p->filter_dtol = 1.0e5; p->filter_maxit = 10000;
     p->verbose = 0;
@@ -334,6 +334,26 @@ int topo_create(const topo_params* p, int nen, int n_nodes, const double* vertex
     if (p) pp = *p;
     else topo_params_default(&pp);
     TRET(check_params(&pp));
+    // host-side validation first, so a corrupt mesh is reported as such
+    // whether or not a device is present
+    for (long q = 0; q < 3L * n_nodes; q++)
+        if (!std::isfinite(vertex[q])) { set_error("vertex %ld is not finite", q / 3); return TOPO_ERR_MESH; }
+    for (long q = 0; q < (long)n_elems * nen; q++)
+        if (element[q] < 0 || element[q] >= n_nodes) {
+            set_error("element %ld references node %d outside [0,%d)", q / nen, element[q], n_nodes);
+            return TOPO_ERR_MESH;
+        }
+    for (int i = 0; i < n_fixed; i++)
+        if (fixed_dofs[i] < 0 || fixed_dofs[i] >= 3 * n_nodes) { set_error("fixed DOF %d out of range", fixed_dofs[i]); return TOPO_ERR_MESH; }
+    if (case_ptr[0] != 0) { set_error("case_ptr[0] must be 0"); return TOPO_ERR_ARG; }
+    for (int k = 0; k < n_cases; k++) {
+        if (case_ptr[k + 1] < case_ptr[k]) { set_error("case_ptr not monotone"); return TOPO_ERR_ARG; }
+        for (int q = case_ptr[k]; q < case_ptr[k + 1]; q++)
+            if (load_dofs[q] < 0 || load_dofs[q] >= 3 * n_nodes || !std::isfinite(load_vals[q])) {
+                set_error("load entry %d invalid (DOF %d)", q, load_dofs[q]);
+                return TOPO_ERR_MESH;
+            }
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -368,6 +388,7 @@ int topo_destroy(topo_ctx* ctx) {
     for (int i = 0; i < 4; i++)
         if (ctx->c.ev[i]) cudaEventDestroy(ctx->c.ev[i]);
     for (auto e : ctx->c.prof.pool) cudaEventDestroy(e);
+    for (auto e : ctx->c.gm_ev) cudaEventDestroy(e);
     for (auto& r : ctx->c.prof.rec)
         for (auto& pr : r) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     cudaStream_t s = ctx->c.s;
@@ -869,13 +890,14 @@ int topo_read_mesh_dir(const char* dir, int nen, int n_cases, double* vertex, in
     GUARD_END
 }
 
-int topo_write_vtu(topo_ctx* ctx, const char* dir, int itr) {
+int topo_write_vtu(topo_ctx* ctx, const char* dir, int itr, const double* xphys_d) {
     if (!ctx || !dir) { set_error("null argument"); return TOPO_ERR_ARG; }
     GUARD_BEGIN
     Ctx& c = ctx->c;
     std::vector<double> U(c.ndof, 0.0), X(c.ne, 0.0);
     if (c.U.p) TCK(cudaMemcpyAsync(U.data(), c.U.p, sizeof(double) * c.ndof, cudaMemcpyDeviceToHost, c.s));
-    if (c.XP.p) TCK(cudaMemcpyAsync(X.data(), c.XP.p, sizeof(double) * c.ne, cudaMemcpyDeviceToHost, c.s));
+    const double* xsrc = xphys_d ? xphys_d : c.XP.p;
+    if (xsrc) TCK(cudaMemcpyAsync(X.data(), xsrc, sizeof(double) * c.ne, cudaMemcpyDeviceToHost, c.s));
     TCK(cudaStreamSynchronize(c.s));
     std::string name = itr == 0 ? "output_initial" : (itr == -1 ? "output_final" : "output_" + std::to_string(itr));
     std::string path = std::string(dir) + "/" + name + ".vtu";

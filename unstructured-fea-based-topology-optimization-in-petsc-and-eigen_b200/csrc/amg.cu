@@ -181,6 +181,92 @@ __global__ void k_bsr_cheb(int nrows, const int* __restrict__ rp, const int* __r
     }
 }
 
+// ----------------------------------------------------------------- level-0 sliced ELLPACK
+// One thread per node row; block k of the rows of slice s is entry
+// sp[s] + 32k + lane, its 9 values sit at ((sp[s]/32 + k)*9 + e)*32 + lane, so
+// every value and column-id load of a warp is one contiguous line.
+template <class T>
+__global__ void k_bsr_to_sell(int nrows, int nslices, const int* __restrict__ rp, const int* __restrict__ sp,
+                              const T* __restrict__ A, T* __restrict__ S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = i >> 5, lane = i & 31;
+    if (s >= nslices) return;
+    const int base = sp[s] >> 5, w = (sp[s + 1] - sp[s]) >> 5;
+    int r0 = 0, nb = 0;
+    if (i < nrows) { r0 = rp[i]; nb = rp[i + 1] - r0; }
+    for (int k = 0; k < w; k++)
+#pragma unroll
+        for (int e = 0; e < 9; e++)
+            S[((size_t)(base + k) * 9 + e) * 32 + lane] = k < nb ? A[(size_t)r0 * 9 + e * nb + k] : T(0);
+}
+
+// mode 0: y = A x; 1: y = b - A x; 3: y = sigma Dinv A x
+template <class T>
+__global__ void __launch_bounds__(256) k_sell_spmv(int nrows, const int* __restrict__ sp, const int* __restrict__ sci,
+                                                   const T* __restrict__ S, const T* __restrict__ x,
+                                                   T* __restrict__ y, const T* __restrict__ b, int mode,
+                                                   const T* __restrict__ dinv, const double* __restrict__ scal) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrows) return;
+    const int s = i >> 5, lane = i & 31;
+    const int b0 = sp[s], w = (sp[s + 1] - b0) >> 5;
+    const T* a = S + (size_t)(b0 >> 5) * 288 + lane;
+    const int* cp = sci + b0 + lane;
+    T a0 = T(0), a1 = T(0), a2 = T(0);
+#pragma unroll 3
+    for (int k = 0; k < w; k++) {
+        const int j = __ldg(cp + 32 * k);
+        const T x0 = x[3L * j], x1 = x[3L * j + 1], x2 = x[3L * j + 2];
+        const T* ak = a + (size_t)k * 288;
+        a0 += __ldg(ak) * x0 + __ldg(ak + 32) * x1 + __ldg(ak + 64) * x2;
+        a1 += __ldg(ak + 96) * x0 + __ldg(ak + 128) * x1 + __ldg(ak + 160) * x2;
+        a2 += __ldg(ak + 192) * x0 + __ldg(ak + 224) * x1 + __ldg(ak + 256) * x2;
+    }
+    const long o = 3L * i;
+    if (mode == 0) { y[o] = a0; y[o + 1] = a1; y[o + 2] = a2; }
+    else if (mode == 1) { y[o] = b[o] - a0; y[o + 1] = b[o + 1] - a1; y[o + 2] = b[o + 2] - a2; }
+    else {
+        const T sc = T(*scal);
+        y[o] = sc * dinv[o] * a0; y[o + 1] = sc * dinv[o + 1] * a1; y[o + 2] = sc * dinv[o + 2] * a2;
+    }
+}
+
+// fused Chebyshev step on the sliced-ELLPACK level-0 operator
+template <class T>
+__global__ void __launch_bounds__(256) k_sell_cheb(int nrows, const int* __restrict__ sp, const int* __restrict__ sci,
+                                                   const T* __restrict__ S, const T* __restrict__ dold,
+                                                   T* __restrict__ dnew, T* __restrict__ r, T* __restrict__ x,
+                                                   const T* __restrict__ dinv, const double* __restrict__ rho,
+                                                   double cr, double cq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrows) return;
+    const int s = i >> 5, lane = i & 31;
+    const int b0 = sp[s], w = (sp[s + 1] - b0) >> 5;
+    const T* a = S + (size_t)(b0 >> 5) * 288 + lane;
+    const int* cp = sci + b0 + lane;
+    T t[3] = {T(0), T(0), T(0)};
+#pragma unroll 3
+    for (int k = 0; k < w; k++) {
+        const int j = __ldg(cp + 32 * k);
+        const T x0 = dold[3L * j], x1 = dold[3L * j + 1], x2 = dold[3L * j + 2];
+        const T* ak = a + (size_t)k * 288;
+        t[0] += __ldg(ak) * x0 + __ldg(ak + 32) * x1 + __ldg(ak + 64) * x2;
+        t[1] += __ldg(ak + 96) * x0 + __ldg(ak + 128) * x1 + __ldg(ak + 160) * x2;
+        t[2] += __ldg(ak + 192) * x0 + __ldg(ak + 224) * x1 + __ldg(ak + 256) * x2;
+    }
+    const double delta = 0.5 * (*rho);
+    const T c2 = T(cq / delta), c1 = T(cr);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const long o = 3L * i + q;
+        const T rn = r[o] - t[q];
+        const T dn = c1 * dold[o] + c2 * dinv[o] * rn;
+        r[o] = rn;
+        dnew[o] = dn;
+        x[o] += dn;
+    }
+}
+
 // first Chebyshev step.  zero_init: r = b, d = Dinv b / theta, x = d.
 // otherwise (r already = b - A x): d = Dinv r / theta, x += d.
 template <class T>
@@ -361,13 +447,23 @@ __global__ void k_bsr_to_dense(int nnode, const int* __restrict__ rp, const int*
 }
 // [A | I] -> [I | A^-1] by Gauss-Jordan with partial pivoting, one CTA.
 // A zero pivot (singular coarse operator) is replaced by 1 and flagged.
-__global__ void k_gauss_jordan(int n, double* __restrict__ M, double* __restrict__ inv, int* __restrict__ flag) {
-    extern __shared__ double fk[];  // n column factors
+// When in_smem, [A | I] is staged in shared memory (n <= 112 fits in 227 KB):
+// a single CTA is then bound by shared-memory rather than L2 bandwidth.
+__global__ void k_gauss_jordan(int n, double* __restrict__ Mg, double* __restrict__ inv, int* __restrict__ flag,
+                               int in_smem) {
+    extern __shared__ double dyn[];  // n column factors [+ staged matrix]
+    double* fk = dyn;
     __shared__ double s_val[32];
     __shared__ int s_idx[32];
     __shared__ double s_piv;
     __shared__ int s_prow;
     const int ld = 2 * n, tid = threadIdx.x, nt = blockDim.x;
+    double* M = Mg;
+    if (in_smem) {
+        M = dyn + ((n + 1) & ~1);
+        for (long q = tid; q < (long)n * ld; q += nt) M[q] = Mg[q];
+    }
+    __syncthreads();
     for (int q = tid; q < n; q += nt) M[(size_t)q * ld + n + q] = 1.0;
     __syncthreads();
     for (int k = 0; k < n; k++) {
@@ -461,6 +557,7 @@ static int alloc_vals(Ctx& c) {
         TRET(v.t[l].alloc(D.ndof));
         TRET(v.pv[l].alloc(D.ndof));
         TRET(v.pw[l].alloc(D.ndof));
+        if (l == 0) TRET(v.A0s.alloc((size_t)D.sell_blocks * 9));
         if (l + 1 < c.nlev) {
             TRET(v.P[l].alloc((size_t)D.P.nnzb * bs * 6));
             TRET(v.T_[l].alloc((size_t)D.P.nnzb * bs * 6));
@@ -531,14 +628,18 @@ template <class T>
 static int level_spmv(Ctx& c, int l, const T* x, T* y, const T* b, int mode, const T* dinv = nullptr,
                       const double* scal = nullptr) {
     AmgVals<T>& v = vals<T>(c);
-    if (c.dl[l].bs == 3) {
+    if (l == 0 && mode != 2) {
+        const AmgDevLevel& D = c.dl[0];
         cudaEvent_t e0;
-        const bool rec = l == 0 && mode == 1;
+        const bool rec = mode == 1;
         if (rec) prof_begin(c, PS_RES0, &e0);
-        int rc = spmv<T, 3, 3>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal);
+        k_sell_spmv<T><<<(D.nnode + 255) / 256, 256, 0, c.s>>>(D.nnode, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, x, y, b,
+                                                               mode, dinv, scal), note_launch();
         if (rec) prof_end(c, PS_RES0, e0);
-        return rc;
+        TCK(cudaGetLastError());
+        return 0;
     }
+    if (c.dl[l].bs == 3) return spmv<T, 3, 3>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal);
     return spmv<T, 6, 6>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal);
 }
 
@@ -584,6 +685,11 @@ static int numeric(Ctx& c) {
             k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, ke, Ee, D.A.rp.p, D.A.ci.p,
                                               c.dof_fixed.p, v.A[0].p, c.maxdeg), note_launch();
         }
+        TCK(cudaGetLastError());
+        // sliced-ELLPACK copy of the level-0 operator for the smoother
+        AmgDevLevel& D0 = c.dl[0];
+        k_bsr_to_sell<T><<<D0.nslices * 32 / 256 + 1, 256, 0, c.s>>>(D0.nnode, D0.nslices, D0.A.rp.p, D0.sell_ptr.p,
+                                                                     v.A[0].p, v.A0s.p), note_launch();
         TCK(cudaGetLastError());
     }
     for (int l = 0; l < c.nlev; l++) {
@@ -641,9 +747,12 @@ static int numeric(Ctx& c) {
             k_bsr_to_dense<T, 3><<<D.nnode, 128, 0, c.s>>>(D.nnode, D.A.rp.p, D.A.ci.p, v.A[L].p, c.cA.p, n), note_launch();
         else
             k_bsr_to_dense<T, 6><<<D.nnode, 128, 0, c.s>>>(D.nnode, D.A.rp.p, D.A.ci.p, v.A[L].p, c.cA.p, n), note_launch();
-        const size_t sm = sizeof(double) * (size_t)n;
+        const size_t smg = sizeof(double) * (size_t)(((n + 1) & ~1) + (size_t)2 * n * n);
+        const int in_smem = smg <= 220 * 1024;
+        const size_t sm = in_smem ? smg : sizeof(double) * (size_t)n;
         if (sm > 48 * 1024) TCK(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_gauss_jordan<<<1, 1024, sm, c.s>>>(n, c.cA.p, c.cinv.p, reinterpret_cast<int*>(c.rho.p + 3 * kMaxLevels)), note_launch();
+        k_gauss_jordan<<<1, 1024, sm, c.s>>>(n, c.cA.p, c.cinv.p, reinterpret_cast<int*>(c.rho.p + 3 * kMaxLevels),
+                                             in_smem), note_launch();
         TCK(cudaGetLastError());
     }
     return 0;
@@ -690,14 +799,18 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
             k_cheb_upd<T><<<grid_for(n, 256), 256, 0, c.s>>>(n, v.t[l].p, v.r[l].p, dcur, x, v.dinv[l].p, rho, cr[k], cq[k]), note_launch();
         } else {
             const int nrows = D.nnode;
-            if (D.bs == 3) {
-                constexpr int G = 32;
+            if (l == 0) {
                 cudaEvent_t e0;
-                if (l == 0) prof_begin(c, PS_CHEB0, &e0);
+                prof_begin(c, PS_CHEB0, &e0);
+                k_sell_cheb<T><<<(nrows + 255) / 256, 256, 0, c.s>>>(nrows, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, dcur,
+                                                                     dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr[k],
+                                                                     cq[k]), note_launch();
+                prof_end(c, PS_CHEB0, e0);
+            } else if (D.bs == 3) {
+                constexpr int G = 32;
                 k_bsr_cheb<T, 3, G><<<(nrows * G + 255) / 256, 256, 0, c.s>>>(nrows, D.A.rp.p, D.A.ci.p, v.A[l].p, dcur,
                                                                             dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr[k],
                                                                             cq[k]), note_launch();
-                if (l == 0) prof_end(c, PS_CHEB0, e0);
             } else {
                 constexpr int G = 32;
                 k_bsr_cheb<T, 6, G><<<(nrows * G + 255) / 256, 256, 0, c.s>>>(nrows, D.A.rp.p, D.A.ci.p, v.A[l].p, dcur,

@@ -64,6 +64,11 @@ struct AmgDevLevel {
     DevPattern A, P, AP, R;
     DBuf<int> diagpos;          // slot of the diagonal block in each A row
     DBuf<int> ptpos, rperm;
+    // level 0 only: sliced-ELLPACK (32-row slices) copy of A for the smoother;
+    // block k of row 32s+l is entry sell_ptr[s] + 32k + l
+    int nslices = 0;
+    long sell_blocks = 0;
+    DBuf<int> sell_ptr, sell_ci;
     DevPattern Ptp;             // tentative prolongator: one block per aggregated node
     DBuf<double> Pt64c;         // its bs x 6 blocks (compact, FP64)
     DBuf<float> Pt32c;          // (FP32 copy for the mixed form)
@@ -76,6 +81,7 @@ struct AmgVals {
     DBuf<T> dinv[kMaxLevels];
     DBuf<T> x[kMaxLevels], b[kMaxLevels], r[kMaxLevels], d[kMaxLevels], d2[kMaxLevels], t[kMaxLevels];
     DBuf<T> pv[kMaxLevels], pw[kMaxLevels];   // power-iteration vectors (warm start)
+    DBuf<T> A0s;                // level-0 operator in the sliced-ELLPACK layout
     bool allocated = false;
 };
 
@@ -129,7 +135,8 @@ struct Ctx {
     DBuf<double> V;             // Krylov basis (restart+1) x ndof
     DBuf<double> Z64;           // preconditioned directions (FP64 form)
     DBuf<float> Z32;            // (mixed form)
-    DBuf<double> w, wtmp;
+    DBuf<double> w, wtmp;       // wtmp: device Arnoldi state + per-iteration outputs
+    std::vector<cudaEvent_t> gm_ev;  // one per Arnoldi step (pipelined residual checks)
     DBuf<double> red;           // reduction partials
     DBuf<double> dsc;           // device scalars
     PinnedScalars hsc;          // pinned host mirror for readbacks

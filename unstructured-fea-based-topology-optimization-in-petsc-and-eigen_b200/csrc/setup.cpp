@@ -382,6 +382,32 @@ int build_amg_host(Ctx& c) {
         for (int i = 0; i < H.nnode; i++)
             if (dp[i] < 0) { set_error("AMG level %d row %d has no diagonal block", l, i); return TOPO_ERR_MESH; }
         TRET(D.diagpos.upload(dp, s));
+        if (l == 0) {
+            // sliced ELLPACK: slice width = longest row of the 32-row slice,
+            // padding blocks point at the row itself with zero values
+            D.nslices = (H.nnode + 31) / 32;
+            std::vector<int> sp(D.nslices + 1, 0), sci;
+            for (int sl = 0; sl < D.nslices; sl++) {
+                int w = 0;
+                for (int r = 32 * sl; r < std::min(H.nnode, 32 * sl + 32); r++) w = std::max(w, H.A.rp[r + 1] - H.A.rp[r]);
+                sp[sl + 1] = sp[sl] + 32 * w;
+            }
+            sci.assign(sp[D.nslices], 0);
+            for (int sl = 0; sl < D.nslices; sl++) {
+                int w = (sp[sl + 1] - sp[sl]) / 32;
+                for (int ln = 0; ln < 32; ln++) {
+                    int r = 32 * sl + ln;
+                    for (int k = 0; k < w; k++) {
+                        int col = r < H.nnode ? r : 0;
+                        if (r < H.nnode && k < H.A.rp[r + 1] - H.A.rp[r]) col = H.A.ci[H.A.rp[r] + k];
+                        sci[sp[sl] + 32 * k + ln] = col;
+                    }
+                }
+            }
+            D.sell_blocks = sp[D.nslices];
+            TRET(D.sell_ptr.upload(sp, s));
+            TRET(D.sell_ci.upload(sci, s));
+        }
         if (l + 1 < c.nlev) {
             TRET(D.P.upload(H.P, s));
             TRET(D.AP.upload(H.AP, s));

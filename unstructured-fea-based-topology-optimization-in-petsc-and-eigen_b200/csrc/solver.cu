@@ -133,31 +133,97 @@ static int precond_apply(Ctx& c, const double* v, int j) {
     return amg_vcycle64(c, v, c.Z64.p + (size_t)j * n);
 }
 
+// ----------------------------------------------------------------- device-side Arnoldi bookkeeping
+// Layout of the per-cycle state (doubles): H (m+1) x m row-major, then cs[m],
+// sn[m], g[m+1], y[m].
+struct GmLayout {
+    int m;
+    __host__ __device__ int H(int i, int j) const { return i * m + j; }
+    __host__ __device__ int cs(int j) const { return (m + 1) * m + j; }
+    __host__ __device__ int sn(int j) const { return (m + 1) * m + m + j; }
+    __host__ __device__ int g(int j) const { return (m + 1) * m + 2 * m + j; }
+    __host__ __device__ int y(int j) const { return (m + 1) * m + 3 * m + 1 + j; }
+    __host__ __device__ int size() const { return (m + 1) * m + 4 * m + 1; }
+};
+
+// cycle start: beta = sqrt(||r||^2), g = (beta, 0, ...); beta also to out[0]
+__global__ void k_gm_start(GmLayout L, double* __restrict__ st, const double* __restrict__ r2,
+                           double* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double beta = sqrt(*r2);
+    for (int j = 0; j <= L.m; j++) st[L.g(j)] = 0.0;
+    st[L.g(0)] = beta;
+    out[0] = beta;
+}
+// column j of the Hessenberg matrix (h[0..j] and h[j+1] = ||w||) is rotated
+// by the previous Givens rotations, a new rotation zeroes h[j+1,j], and the
+// residual estimate |g[j+1]| goes to out[0] (out[1] = ||w||)
+__global__ void k_gm_givens(GmLayout L, int j, const double* __restrict__ hcol, double* __restrict__ st,
+                            double* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int i = 0; i <= j + 1; i++) st[L.H(i, j)] = hcol[i];
+    for (int i = 0; i < j; i++) {
+        const double c = st[L.cs(i)], s = st[L.sn(i)];
+        const double t1 = st[L.H(i, j)], t2 = st[L.H(i + 1, j)];
+        st[L.H(i, j)] = c * t1 + s * t2;
+        st[L.H(i + 1, j)] = -s * t1 + c * t2;
+    }
+    const double hjj = st[L.H(j, j)], hj1 = st[L.H(j + 1, j)];
+    const double den = sqrt(hjj * hjj + hj1 * hj1);
+    double c = 1.0, s = 0.0;
+    if (den != 0.0) { c = hjj / den; s = hj1 / den; }
+    st[L.cs(j)] = c;
+    st[L.sn(j)] = s;
+    st[L.H(j, j)] = c * hjj + s * hj1;
+    st[L.H(j + 1, j)] = 0.0;
+    const double gj = st[L.g(j)];
+    st[L.g(j + 1)] = -s * gj;
+    st[L.g(j)] = c * gj;
+    out[0] = fabs(-s * gj);
+    out[1] = hcol[j + 1];
+}
+// y = R^-1 g for the kd completed columns
+__global__ void k_gm_solve(GmLayout L, int kd, double* __restrict__ st) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int i = kd - 1; i >= 0; i--) {
+        double s = st[L.g(i)];
+        for (int k = i + 1; k < kd; k++) s -= st[L.H(i, k)] * st[L.y(k)];
+        st[L.y(i)] = s / st[L.H(i, i)];
+    }
+}
+
 // FGMRES(restart) on K(Ee64) u = b, x in/out.  Converged when the Arnoldi
 // residual estimate |g_{j+1}| <= max(rtol ||b||, 1e-50) (KSPConvergedDefault
-// with a nonzero initial guess: rnorm0 = ||b||).
+// with a nonzero initial guess: rnorm0 = ||b||).  The Hessenberg
+// bookkeeping lives on the device and iteration j+1 is queued before the
+// host reads iteration j's residual, so the GPU never waits for the host;
+// the one speculative iteration of a converged cycle writes only column
+// j+1 state and is discarded.
 static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status) {
     const long n = c.ndof;
     const int m = std::max(1, std::min(c.p.fem_restart, 30));
     const int maxit = c.p.fem_maxit;
+    const GmLayout GL{m};
     if (!c.V.p) {
         TRET(c.V.alloc((size_t)(m + 1) * n));
-        if (c.p.precision == TOPO_PREC_MIXED) TRET(c.Z32.alloc((size_t)m * n));
-        else TRET(c.Z64.alloc((size_t)m * n));
         TRET(c.w.alloc(n));
-        TRET(c.wtmp.alloc(64));
+        TRET(c.wtmp.alloc(GL.size() + 64));
     }
     if (c.p.precision == TOPO_PREC_MIXED && !c.Z32.p) TRET(c.Z32.alloc((size_t)m * n));
     if (c.p.precision != TOPO_PREC_MIXED && !c.Z64.p) TRET(c.Z64.alloc((size_t)m * n));
     if ((long)c.red.n < kRedBlocks * 40L) TRET(c.red.alloc(std::max<long>(kRedBlocks * 40L, 4096)));
-    double* hs = c.hsc.h;   // pinned: [0..m+1] column, [64] misc
-    double* gm = c.dsc.p + DS_GM;
-    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), yv(m);
-    // ||b||
+    if (c.gm_ev.empty()) {
+        c.gm_ev.resize(31);
+        for (auto& e : c.gm_ev) TCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    double* hs = c.hsc.h;           // pinned: [2j, 2j+1] = (residual, ||w||) of iteration j
+    double* gm = c.dsc.p + DS_GM;   // Hessenberg column scratch
+    double* st = c.wtmp.p;          // device Arnoldi state
+    double* out = st + GL.size();   // per-launch outputs (2 doubles per iteration)
     TRET(dev_dot(c, b, b, n, gm));
-    TCK(cudaMemcpyAsync(hs, gm, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    TCK(cudaMemcpyAsync(hs + 100, gm, sizeof(double), cudaMemcpyDeviceToHost, c.s));
     TCK(cudaStreamSynchronize(c.s));
-    const double bnorm = std::sqrt(hs[0]);
+    const double bnorm = std::sqrt(hs[100]);
     const double ttol = std::max(c.p.fem_rtol * bnorm, 1e-50);
     int its = 0;
     bool conv = false;
@@ -165,61 +231,48 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
         // v0 = (b - K x) / beta
         TRET(kmatvec64r(c, x, c.w.p, b));
         TRET(dev_dot(c, c.w.p, c.w.p, n, gm));
-        TCK(cudaMemcpyAsync(hs, gm, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+        k_gm_start<<<1, 32, 0, c.s>>>(GL, st, gm, out + 62), note_launch();
+        TCK(cudaMemcpyAsync(hs + 101, out + 62, sizeof(double), cudaMemcpyDeviceToHost, c.s));
         TCK(cudaStreamSynchronize(c.s));
-        const double beta = std::sqrt(hs[0]);
+        const double beta = hs[101];
         if (!std::isfinite(beta)) { set_error("FGMRES residual is not finite"); return TOPO_ERR_NAN; }
         if (beta <= ttol) { conv = true; break; }
-        hs[70] = beta;
-        TCK(cudaMemcpyAsync(c.wtmp.p, hs + 70, sizeof(double), cudaMemcpyHostToDevice, c.s));
-        k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, c.wtmp.p, c.V.p, 1), note_launch();
-        std::fill(g.begin(), g.end(), 0.0);
-        g[0] = beta;
-        int kdone = 0;
-        for (int j = 0; j < m && its < maxit; j++) {
-            const double* vj = c.V.p + (size_t)j * n;
-            TRET(precond_apply(c, vj, j));
-            if (c.p.precision == TOPO_PREC_MIXED) TRET(kmatvec_f32in(c, c.Ee64.p, c.Z32.p + (size_t)j * n, c.w.p));
-            else TRET(kmatvec(c, c.Ee64.p, c.Z64.p + (size_t)j * n, c.w.p));
-            TRET(mdot(c, j + 1, c.V.p, n, c.w.p, gm));
-            TRET(orth(c, j + 1, c.V.p, n, gm, c.w.p, gm + j + 1));
-            TCK(cudaMemcpyAsync(hs, gm, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, c.s));
-            k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, gm + j + 1, c.V.p + (size_t)(j + 1) * n, 1), note_launch();
-            TCK(cudaStreamSynchronize(c.s));
-            for (int i = 0; i <= j + 1; i++) H[(size_t)i * m + j] = hs[i];
-            const double hn = hs[j + 1];
-            for (int i = 0; i < j; i++) {
-                double t1 = H[(size_t)i * m + j], t2 = H[(size_t)(i + 1) * m + j];
-                H[(size_t)i * m + j] = cs[i] * t1 + sn[i] * t2;
-                H[(size_t)(i + 1) * m + j] = -sn[i] * t1 + cs[i] * t2;
+        k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, out + 62, c.V.p, 1), note_launch();
+        const int jmax = std::min(m, maxit - its);
+        int kdone = jmax;
+        bool stop = false;
+        for (int j = 0; j <= jmax && !stop; j++) {
+            if (j < jmax) {
+                const double* vj = c.V.p + (size_t)j * n;
+                TRET(precond_apply(c, vj, j));
+                if (c.p.precision == TOPO_PREC_MIXED) TRET(kmatvec_f32in(c, c.Ee64.p, c.Z32.p + (size_t)j * n, c.w.p));
+                else TRET(kmatvec(c, c.Ee64.p, c.Z64.p + (size_t)j * n, c.w.p));
+                TRET(mdot(c, j + 1, c.V.p, n, c.w.p, gm));
+                TRET(orth(c, j + 1, c.V.p, n, gm, c.w.p, gm + j + 1));
+                k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, gm + j + 1, c.V.p + (size_t)(j + 1) * n, 1),
+                    note_launch();
+                k_gm_givens<<<1, 32, 0, c.s>>>(GL, j, gm, st, out + 2 * j), note_launch();
+                TCK(cudaMemcpyAsync(hs + 2 * j, out + 2 * j, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+                TCK(cudaEventRecord(c.gm_ev[j], c.s));
             }
-            double hjj = H[(size_t)j * m + j], hj1 = H[(size_t)(j + 1) * m + j];
-            double den = std::sqrt(hjj * hjj + hj1 * hj1);
-            if (den == 0.0) { cs[j] = 1.0; sn[j] = 0.0; }
-            else { cs[j] = hjj / den; sn[j] = hj1 / den; }
-            H[(size_t)j * m + j] = cs[j] * hjj + sn[j] * hj1;
-            H[(size_t)(j + 1) * m + j] = 0.0;
-            g[j + 1] = -sn[j] * g[j];
-            g[j] = cs[j] * g[j];
+            if (j == 0) continue;
+            // check iteration j-1 while iteration j runs
+            TCK(cudaEventSynchronize(c.gm_ev[j - 1]));
             its++;
-            kdone = j + 1;
-            const double res = std::fabs(g[j + 1]);
+            const double res = hs[2 * (j - 1)], hn = hs[2 * (j - 1) + 1];
             if (!std::isfinite(res)) { set_error("FGMRES breakdown (non-finite residual)"); return TOPO_ERR_NAN; }
-            if (res <= ttol || hn == 0.0) { conv = res <= ttol; break; }
+            if (res <= ttol || hn == 0.0) {
+                conv = res <= ttol;
+                kdone = j;
+                stop = true;
+            }
         }
-        for (int i = kdone - 1; i >= 0; i--) {
-            double s = g[i];
-            for (int k = i + 1; k < kdone; k++) s -= H[(size_t)i * m + k] * yv[k];
-            yv[i] = s / H[(size_t)i * m + i];
-        }
-        for (int k = 0; k < kdone; k++) hs[80 + k] = yv[k];
-        TCK(cudaMemcpyAsync(c.wtmp.p, hs + 80, sizeof(double) * kdone, cudaMemcpyHostToDevice, c.s));
+        k_gm_solve<<<1, 32, 0, c.s>>>(GL, kdone, st), note_launch();
         if (c.p.precision == TOPO_PREC_MIXED)
-            k_update<float><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z32.p, n, c.wtmp.p, x), note_launch();
+            k_update<float><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z32.p, n, st + GL.y(0), x), note_launch();
         else
-            k_update<double><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z64.p, n, c.wtmp.p, x), note_launch();
+            k_update<double><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z64.p, n, st + GL.y(0), x), note_launch();
         TCK(cudaGetLastError());
-        TCK(cudaStreamSynchronize(c.s));  // pinned y buffer reused next cycle
     }
     *its_out = its;
     *status = conv ? 0 : 1;
