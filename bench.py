@@ -156,7 +156,7 @@ def run_device(ctx, T, torch, steps, warmup, stream, dist=None, profile=True):
     ctx.opt_init()
     for _ in range(warmup):
         ctx.opt_step()
-    for s in range(4):
+    for s in range(8):
         ctx.profile_read(s)
     if profile:
         ctx.profile(True)
@@ -178,7 +178,7 @@ def run_device(ctx, T, torch, steps, warmup, stream, dist=None, profile=True):
     ms = e0.elapsed_time(e1)
     prof = {}
     if profile:
-        for s, name in enumerate(["kmv", "cheb0", "res0", "filter_kf"]):
+        for s, name in enumerate(["kmv", "cheb0", "res0", "filter_kf", "setup_asm", "setup_rho", "setup_galerkin", "setup_coarse"]):
             n, t = ctx.profile_read(s)
             prof[name] = (n, t)
         ctx.profile(False)
@@ -211,6 +211,34 @@ def run_e2e(ctx, T, torch, steps, warmup, stream, dist=None):
     return e0.elapsed_time(e1), ne * 8, 2 * ne * 8 + 72
 
 
+def run_serving(T, n_jobs, seed=7, rate=4.0, iters=30):
+    """Serving stream: Poisson arrivals (mean `rate` jobs/s, seeded) of hex8 /
+    tet4 cantilever jobs, sizes log-uniform in [20k, 1.2M] elements, volfrac
+    U(0.1, 0.3), filter radius U(1.2, 2.0) h, `iters` design iterations each,
+    mixed precision; HBM-budget admission, up to 8 jobs in flight."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    s = T.Server(hbm_budget_bytes=0, max_active=8)
+    t = 0.0
+    sizes = []
+    for _ in range(n_jobs):
+        t += rng.exponential(1.0 / rate)
+        ne = float(np.exp(rng.uniform(np.log(2e4), np.log(1.2e6))))
+        nen = 8 if rng.uniform() < 0.5 else 4
+        a = max(2, int(round((ne / (2.0 if nen == 8 else 12.0)) ** (1.0 / 3.0))))
+        v, e, f, ld, lv = T.gen_cantilever(2 * a, a, a, nen, seed=int(rng.integers(1, 2 ** 31)))
+        kw = dict(PARAMS, volfrac=float(rng.uniform(0.1, 0.3)), rmin=float(rng.uniform(1.2, 2.0)),
+                  precision=T.PREC_MIXED)
+        s.submit(v, e, f, ld, lv, iterations=iters, arrival_s=t, **kw)
+        sizes.append(e.shape[0])
+    rc = s.run()
+    st = s.stats()
+    s.close()
+    st.update({"jobs": n_jobs, "arrival_rate_per_s": rate, "iterations_per_job": iters,
+               "elements_min": int(min(sizes)), "elements_max": int(max(sizes)), "rc": rc})
+    return st
+
+
 def kmv_bytes(ctx, u_bytes):
     """Algorithmic bytes of one element-operator launch: per element the 8
     connectivity ids, the fixed mask, E_e and the 300 packed FP64 Ke entries;
@@ -236,7 +264,8 @@ def main():
     ap.add_argument("--workload", default="hex8-392k", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
-    ap.add_argument("--serve", action="store_true", help="also run the serving stream (p50/p99)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving stream (p50/p99 latency)")
+    ap.add_argument("--serve-jobs", type=int, default=12)
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="time one precision only (used for short profiling runs)")
     args = ap.parse_args()
@@ -336,6 +365,9 @@ def main():
                 "frac": dom["gbs"] / peak, "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": dom["bytes"], "avg_launch_us": dom["avg_us"]}
 
+    serve = None
+    if not args.no_serve:
+        serve = run_serving(T, args.serve_jobs, seed=7)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         done, dt, cores = cpu_run(wl, args.cpu_steps, 60.0, warmup=1)
@@ -356,7 +388,7 @@ def main():
             "amg_dofs": list(info.amg_dofs)[:info.amg_levels],
             "e2e": {"value": e2e_val, "unit": "design iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "kernels": kern, "clocks": clocks,
-            "cpu_baseline": cpu}
+            "cpu_baseline": cpu, "serve": serve}
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -71,6 +71,8 @@ typedef struct topo_params {
     double filter_rtol, filter_atol, filter_dtol;
     int filter_maxit;
     int verbose;           /* 1: print the reference's per-solve lines */
+    int amg_rho_its;       /* power iterations for rho(D^-1 A) per level and design iteration */
+    double cheb_safety;    /* Chebyshev interval [0.1, 1.1] * cheb_safety * rho */
 } topo_params;
 
 typedef struct topo_solve_info {
@@ -206,15 +208,56 @@ int topo_opt_step_host(topo_ctx* ctx, const double* x_in, double* x_out, double*
 int topo_opt_vector(topo_ctx* ctx, int which, double** ptr_d);
 int topo_solve_info_get(topo_ctx* ctx, topo_solve_info* info);
 
+/* ---------------------------------------------------------------- serving */
+/* Continuous batching of whole optimisation jobs (no counterpart in the
+ * reference, which runs one job per MPI launch, main.cpp:35-137): jobs wait
+ * in a FIFO until their arrival time, a free slot and their estimated HBM
+ * footprint allow admission; each admitted job runs its iterations on its own
+ * context and stream, overlapping on the device with the others, and frees
+ * its slot and memory when done. */
+typedef struct topo_server topo_server;
+typedef struct topo_server_stats {
+    int jobs_submitted, jobs_done, jobs_failed, max_active;
+    long iterations;
+    double p50_iter_ms, p99_iter_ms, mean_iter_ms;  /* per design iteration, all jobs */
+    double makespan_s, jobs_per_hour, iters_per_s;
+    double peak_reserved_bytes;
+    double p50_queue_s, p99_queue_s;                /* arrival -> admission */
+} topo_server_stats;
+/* bytes a job is admitted against (upper estimate of its device footprint) */
+size_t topo_estimate_job_bytes(int nen, int n_nodes, int n_elems, int precision);
+/* hbm_budget_bytes 0 = 85% of the currently free device memory */
+int topo_server_create(size_t hbm_budget_bytes, int max_active, topo_server** out);
+int topo_server_destroy(topo_server* s);
+/* copies the job's mesh and options; arrival_s is relative to topo_server_run's start */
+int topo_server_submit(topo_server* s, const topo_params* p, int nen, int n_nodes, const double* vertex, int n_elems,
+                       const int32_t* element, int n_fixed, const int32_t* fixed_dofs, int n_cases,
+                       const int32_t* case_ptr, const int32_t* load_dofs, const double* load_vals, int iterations,
+                       double arrival_s, int* job_id);
+/* runs every submitted job to completion (real-time arrivals); blocks */
+int topo_server_run(topo_server* s);
+/* per-job results (host arrays sized by the caller; NULL to skip):
+ * iteration latencies (ms) and compliance history, final XPhys */
+int topo_server_job(topo_server* s, int job_id, int* status, int* n_iters, double* iter_ms, double* fx_hist,
+                    double* xphys, double* admit_s, double* finish_s);
+int topo_server_stats_get(topo_server* s, topo_server_stats* st);
+
 /* ---------------------------------------------------------------- instrumentation */
 /* Kernel launches issued by this library in this process (all contexts). */
 long topo_kernel_launches(void);
 /* CUDA-event timing of the hot kernels on the context's stream (no host
  * syncs added): slot 0 element operator K(x)u, 1 level-0 Chebyshev sweep,
- * 2 level-0 residual, 3 Helmholtz-filter operator. */
+ * 2 level-0 residual, 3 Helmholtz-filter operator, 4..7 AMG setup phases
+ * (assembly, spectral estimates, Galerkin products, coarse inverse). */
 int topo_profile_enable(topo_ctx* ctx, int on);
 /* Synchronises, returns launches and summed milliseconds of a slot, resets it. */
 int topo_profile_read(topo_ctx* ctx, int slot, long* launches, double* total_ms);
+/* AMG hierarchy introspection (replaces what PCGAMG exposes through
+ * PCGetCoarseOperators / -pc_gamg_* viewers): after a solve, matrix `which`
+ * (0 A_l, 1 P_l, 2 R_l = P_l^T) of level l as plain BSR on the host, blocks
+ * row-major.  Call with NULL arrays to get the sizes. */
+int topo_amg_level(topo_ctx* ctx, int level, int which, int* nrows, int* ncols, int* bs_r, int* bs_c, long* nnzb,
+                   int32_t* rp, int32_t* ci, double* vals);
 /* Greedy graph aggregation used for the AMG hierarchy (host only): rows
  * (rp, ci; sorted, self included) of an n-node graph; excl[i] != 0 leaves
  * node i out (-1).  Returns the aggregate count, agg[] the membership. */

@@ -1,0 +1,82 @@
+"""Continuous batching: each job's result is the same alone and in the mix,
+late arrivals are admitted while others run, and the HBM budget gates
+admission.  Tolerance: compliance histories within 1e-6 relative and final
+densities within 1e-5 (the kernels' float atomics make concurrent runs
+reproducible to round-off, amplified through the design iterations)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(Emax=1.0, rmin=1.5, fem_rtol=1e-5, ch_tol=0.0)
+
+
+def jobs(T):
+    specs = [((16, 8, 6), 8, 0.12, 1.5), ((20, 10, 6), 8, 0.2, 1.2), ((10, 6, 4), 4, 0.25, 2.0),
+             ((24, 8, 8), 8, 0.1, 1.8)]
+    out = []
+    for dims, nen, vf, rmin in specs:
+        v, e, f, ld, lv = T.gen_cantilever(*dims, nen)
+        out.append((v, e, f, ld, lv, dict(KW, volfrac=vf, rmin=rmin)))
+    return out
+
+
+def run(T, js, max_active, arrivals, iters=8):
+    s = T.Server(hbm_budget_bytes=0, max_active=max_active)
+    for (v, e, f, ld, lv, kw), a in zip(js, arrivals):
+        s.submit(v, e, f, ld, lv, iterations=iters, arrival_s=a, **kw)
+    assert s.run() == 0
+    res = [s.job(i) for i in range(len(js))]
+    st = s.stats()
+    s.close()
+    return res, st
+
+
+def test_alone_equals_mixed(T, cuda):
+    js = jobs(T)
+    alone = [run(T, [j], 1, [0.0])[0][0] for j in js]
+    mixed, st = run(T, js, 4, [0.0, 0.0, 0.05, 0.1])
+    assert st["jobs_done"] == 4 and st["jobs_failed"] == 0
+    assert st["max_active"] >= 2  # the jobs really overlapped
+    for a, m in zip(alone, mixed):
+        assert a["status"] == 0 and m["status"] == 0
+        assert np.max(np.abs(a["fx"] - m["fx"]) / np.abs(a["fx"])) < 1e-6
+        assert np.abs(a["xphys"] - m["xphys"]).max() < 1e-5
+    assert st["p99_iter_ms"] >= st["p50_iter_ms"] > 0
+    assert st["jobs_per_hour"] > 0 and st["iterations"] == 4 * 8
+
+
+def test_memory_budget_gates_admission(T, cuda):
+    js = jobs(T)
+    v, e = js[0][0], js[0][1]
+    est = T.estimate_job_bytes(8, v.shape[0], e.shape[0], T.PREC_FP64)
+    # a budget for about one job at a time forces serial admission
+    s = T.Server(hbm_budget_bytes=int(est * 1.5), max_active=4)
+    for _ in range(3):
+        s.submit(*js[0][:5], iterations=3, **js[0][5])
+    assert s.run() == 0
+    st = s.stats()
+    assert st["max_active"] == 1 and st["jobs_done"] == 3
+    assert st["peak_reserved_bytes"] <= est * 1.5
+    # a job larger than the whole budget is refused at submission
+    with pytest.raises(T.TopoError):
+        s2 = T.Server(hbm_budget_bytes=int(est * 0.5), max_active=1)
+        s2.submit(*js[0][:5], iterations=1, **js[0][5])
+    s.close()
+
+
+def test_footprint_estimate_is_an_upper_bound(T, cuda):
+    """The admission estimate covers what a job really allocates."""
+    v, e, f, ld, lv = T.gen_cantilever(48, 24, 16, 8)
+    for prec in (T.PREC_FP64, T.PREC_MIXED):
+        cuda.cuda.synchronize()
+        free0, _ = cuda.cuda.mem_get_info()
+        ctx = T.Context(v, e, f, ld, lv, precision=prec, **KW)
+        ctx.opt_init()
+        ctx.opt_step()
+        cuda.cuda.synchronize()
+        free1, _ = cuda.cuda.mem_get_info()
+        used = free0 - free1
+        ctx.close()
+        est = T.estimate_job_bytes(8, v.shape[0], e.shape[0], prec)
+        assert used <= est, (prec, used, est)

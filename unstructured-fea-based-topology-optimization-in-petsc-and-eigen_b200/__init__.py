@@ -38,7 +38,7 @@ class Params(C.Structure):
         ("amg_max_levels", C.c_int), ("amg_coarse_max", C.c_int), ("amg_smooth_p", C.c_int),
         ("cheb_degree", C.c_int), ("fine_smoother_matfree", C.c_int),
         ("filter_rtol", C.c_double), ("filter_atol", C.c_double), ("filter_dtol", C.c_double),
-        ("filter_maxit", C.c_int), ("verbose", C.c_int)]
+        ("filter_maxit", C.c_int), ("verbose", C.c_int), ("amg_rho_its", C.c_int), ("cheb_safety", C.c_double)]
 
 
 class SolveInfo(C.Structure):
@@ -99,10 +99,22 @@ _SIGS = {
     "topo_opt_step": ([C.c_void_p, C.POINTER(C.c_int), _dp, _dp, _dp], C.c_int),
     "topo_opt_run": ([C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)], C.c_int),
     "topo_opt_step_host": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _dp], C.c_int),
+    "topo_estimate_job_bytes": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_size_t),
+    "topo_server_create": ([C.c_size_t, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "topo_server_destroy": ([C.c_void_p], C.c_int),
+    "topo_server_submit": ([C.c_void_p, C.POINTER(Params), C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                            C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                            C.POINTER(C.c_int)], C.c_int),
+    "topo_server_run": ([C.c_void_p], C.c_int),
+    "topo_server_job": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)] + [C.c_void_p] * 3 +
+                        [_dp, _dp], C.c_int),
+    "topo_server_stats_get": ([C.c_void_p, C.c_void_p], C.c_int),
     "topo_kernel_launches": ([], C.c_long),
     "topo_profile_enable": ([C.c_void_p, C.c_int], C.c_int),
     "topo_profile_read": ([C.c_void_p, C.c_int, C.POINTER(C.c_long), _dp], C.c_int),
     "topo_graph_aggregate": ([C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "topo_amg_level": ([C.c_void_p, C.c_int, C.c_int] + [C.POINTER(C.c_int)] * 4 + [C.POINTER(C.c_long)] +
+                       [C.c_void_p] * 3, C.c_int),
     "topo_opt_vector": ([C.c_void_p, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "topo_solve_info_get": ([C.c_void_p, C.POINTER(SolveInfo)], C.c_int),
     "topo_gen_cantilever": ([C.c_int] * 4 + [C.c_double, C.c_uint64, C.c_int] + [C.c_void_p] * 5 +
@@ -386,10 +398,12 @@ class Context:
         return ch.value, xo
 
     def mma_state(self):
-        a = [self.zeros(self.ne) for _ in range(4)]
+        """(xo1, xo2, L, U, k) of the MMA history (MMA::Restart order is xo1, xo2, U, L)."""
+        xo1, xo2, L, U = [self.zeros(self.ne) for _ in range(4)]
         k = C.c_int()
-        _check(lib().topo_mma_restart(self.h, *[_dptr(t) for t in a], C.byref(k), 0), "mma_restart")
-        return a + [k.value]
+        _check(lib().topo_mma_restart(self.h, _dptr(xo1), _dptr(xo2), _dptr(U), _dptr(L), C.byref(k), 0),
+               "mma_restart")
+        return [xo1, xo2, L, U, k.value]
 
     def mma_kkt(self, x, dfdx, gx, dgdx, xmin, xmax):
         n2, ni = C.c_double(), C.c_double()
@@ -419,6 +433,22 @@ class Context:
         _check(lib().topo_opt_step_host(self.h, _ptr(x_in), _ptr(x_out), _ptr(xphys_out), C.byref(fx)),
                "opt_step_host")
         return fx.value
+
+    def amg_level(self, level, which):
+        """Level matrix as a scipy BSR/CSR matrix (which: 0 A, 1 P, 2 R)."""
+        import scipy.sparse as sp
+        nr, nc, br, bc, nb = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_long()
+        L = lib()
+        _check(L.topo_amg_level(self.h, level, which, C.byref(nr), C.byref(nc), C.byref(br), C.byref(bc),
+                                C.byref(nb), None, None, None), "amg_level")
+        rp = np.zeros(nr.value + 1, dtype=np.int32)
+        ci = np.zeros(nb.value, dtype=np.int32)
+        vals = np.zeros(nb.value * br.value * bc.value)
+        _check(L.topo_amg_level(self.h, level, which, C.byref(nr), C.byref(nc), C.byref(br), C.byref(bc),
+                                C.byref(nb), _ptr(rp), _ptr(ci), _ptr(vals)), "amg_level")
+        m = sp.bsr_matrix((vals.reshape(-1, br.value, bc.value), ci, rp),
+                          shape=(nr.value * br.value, nc.value * bc.value))
+        return m.tocsr()
 
     def profile(self, on=True):
         _check(lib().topo_profile_enable(self.h, 1 if on else 0), "profile_enable")
@@ -452,6 +482,77 @@ def device_view(ptr, n):
         __cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3}
 
     return torch.as_tensor(_Arr(), device="cuda")
+
+
+# ---------------------------------------------------------------- serving
+class ServerStats(C.Structure):
+    _fields_ = [("jobs_submitted", C.c_int), ("jobs_done", C.c_int), ("jobs_failed", C.c_int),
+                ("max_active", C.c_int), ("iterations", C.c_long), ("p50_iter_ms", C.c_double),
+                ("p99_iter_ms", C.c_double), ("mean_iter_ms", C.c_double), ("makespan_s", C.c_double),
+                ("jobs_per_hour", C.c_double), ("iters_per_s", C.c_double), ("peak_reserved_bytes", C.c_double),
+                ("p50_queue_s", C.c_double), ("p99_queue_s", C.c_double)]
+
+
+def estimate_job_bytes(nen, n_nodes, n_elems, precision=PREC_FP64):
+    return lib().topo_estimate_job_bytes(nen, n_nodes, n_elems, precision)
+
+
+class Server:
+    """Continuous-batching job server (topo_server_*)."""
+
+    def __init__(self, hbm_budget_bytes=0, max_active=8):
+        h = C.c_void_p()
+        _check(lib().topo_server_create(hbm_budget_bytes, max_active, C.byref(h)), "server_create")
+        self.h = h
+        self.jobs = []
+
+    def submit(self, vertex, element, fixed, load_dofs, load_vals, iterations, arrival_s=0.0, case_ptr=None,
+               params=None, **kw):
+        p = params if params is not None else default_params(**kw)
+        vertex = np.ascontiguousarray(vertex, dtype=np.float64).reshape(-1)
+        element = np.ascontiguousarray(element, dtype=np.int32)
+        nen = element.shape[1]
+        fixed = np.ascontiguousarray(fixed, dtype=np.int32)
+        ld = np.ascontiguousarray(load_dofs, dtype=np.int32)
+        lv = np.ascontiguousarray(load_vals, dtype=np.float64)
+        cp = np.ascontiguousarray(case_ptr if case_ptr is not None else [0, ld.size], dtype=np.int32)
+        jid = C.c_int()
+        _check(lib().topo_server_submit(self.h, C.byref(p), nen, vertex.size // 3, _ptr(vertex), element.shape[0],
+                                        _ptr(element.reshape(-1)), fixed.size, _ptr(fixed), cp.size - 1, _ptr(cp),
+                                        _ptr(ld), _ptr(lv), iterations, arrival_s, C.byref(jid)), "server_submit")
+        self.jobs.append((jid.value, element.shape[0], iterations))
+        return jid.value
+
+    def run(self):
+        return _check(lib().topo_server_run(self.h), "server_run")
+
+    def job(self, jid):
+        _, ne, iters = self.jobs[jid]
+        st, n = C.c_int(), C.c_int()
+        lat = np.zeros(iters)
+        fx = np.zeros(iters)
+        xp = np.zeros(ne)
+        a, f = C.c_double(), C.c_double()
+        rc = lib().topo_server_job(self.h, jid, C.byref(st), C.byref(n), _ptr(lat), _ptr(fx), _ptr(xp), C.byref(a),
+                                   C.byref(f))
+        return dict(rc=rc, status=st.value, iter_ms=lat[:n.value], fx=fx[:n.value], xphys=xp, admit_s=a.value,
+                    finish_s=f.value)
+
+    def stats(self):
+        s = ServerStats()
+        _check(lib().topo_server_stats_get(self.h, C.byref(s)), "server_stats")
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().topo_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------- reference-shaped classes

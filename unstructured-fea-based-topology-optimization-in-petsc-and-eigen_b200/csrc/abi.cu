@@ -184,6 +184,7 @@ int opt_init(Ctx& c) {
     c.mma_k = 0;
     for (DBuf<double>* b : {&c.xo1, &c.xo2, &c.L, &c.Uas, &c.RX}) TRET(b->zero(c.s));
     c.beta_proj = c.beta_tmp = c.p.beta0;
+    TRET(amg_reset_warm_start(c));
     TRET(filter_apply(c, c.X.p, c.XF.p, c.p.Xmin));
     TRET(heaviside(c, c.XF.p, c.XP.p, c.p.x0, c.p.beta0, c.p.betamax, c.itr, c.p.Xmin, c.p.proj));
     c.opt_ready = true;
@@ -273,6 +274,8 @@ void topo_params_default(topo_params* p) {
     p->cheb_degree = 2; p->fine_smoother_matfree = 0;
     p->filter_rtol = 1.0e-5; p->filter_atol = 1.0e-50; p->filter_dtol = 1.0e5; p->filter_maxit = 10000;
     p->verbose = 0;
+    p->amg_rho_its = 10;
+    p->cheb_safety = 1.0;
 }
 
 int topo_device_alloc(size_t bytes, void** ptr) {
@@ -732,6 +735,26 @@ int topo_profile_read(topo_ctx* ctx, int slot, long* launches, double* total_ms)
     *total_ms = tot;
     c.prof.rec[slot].clear();
     return 0;
+}
+
+int topo_amg_level(topo_ctx* ctx, int level, int which, int* nrows, int* ncols, int* bs_r, int* bs_c, long* nnzb,
+                   int32_t* rp, int32_t* ci, double* vals) {
+    if (!ctx || !nrows || !ncols || !bs_r || !bs_c || !nnzb) { set_error("null argument"); return TOPO_ERR_ARG; }
+    GUARD_BEGIN
+    std::vector<double> v;
+    std::vector<int> r, cc;
+    int nr = 0, nc = 0, br = 0, bc = 0;
+    TRET(amg_level_copy(ctx->c, level, which, v, r, cc, nr, nc, br, bc));
+    *nrows = nr;
+    *ncols = nc;
+    *bs_r = br;
+    *bs_c = bc;
+    *nnzb = (long)cc.size();
+    if (rp) std::copy(r.begin(), r.end(), rp);
+    if (ci) std::copy(cc.begin(), cc.end(), ci);
+    if (vals) std::copy(v.begin(), v.end(), vals);
+    return 0;
+    GUARD_END
 }
 
 int topo_graph_aggregate(int n, const int32_t* rp, const int32_t* ci, const unsigned char* excl, int32_t* agg) {

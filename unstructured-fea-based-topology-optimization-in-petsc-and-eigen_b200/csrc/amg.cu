@@ -362,6 +362,92 @@ __global__ void k_spgemm(int nrows, const int* __restrict__ Arp, const int* __re
     }
 }
 
+// Same product with all (A block, B block) pairs of a row spread over the
+// lanes: chunks of 32 A blocks, a warp prefix scan of their B-row lengths,
+// then each lane takes pairs p = lane, lane+32, ... and adds its BR x BC
+// product into the shared-memory row with shared atomics.  Balanced for any
+// mix of short rows (A * Pt: one B block per A block) and long ones (R * AP).
+template <class T, int BR, int BK, int BC>
+__global__ void k_spgemm_pairs(int nrows, const int* __restrict__ Arp, const int* __restrict__ Aci,
+                               const T* __restrict__ A, const int* __restrict__ Brp, const int* __restrict__ Bci,
+                               const T* __restrict__ B, const int* __restrict__ Crp, const int* __restrict__ Cci,
+                               T* __restrict__ C, int maxC) {
+    constexpr int BRK = BR * BK, BKC = BK * BC, BRC = BR * BC;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (blockDim.x >> 5) + wib;
+    if (i >= nrows) return;
+    const size_t accb = ((size_t)maxC * BRC * sizeof(T) + 15) & ~(size_t)15;
+    const size_t per = accb + (((size_t)maxC * sizeof(int) + 15) & ~(size_t)15) + 3 * 32 * sizeof(int);
+    unsigned char* base = smem_raw + wib * per;
+    T* acc = reinterpret_cast<T*>(base);
+    int* cci = reinterpret_cast<int*>(base + accb);
+    int* sp = reinterpret_cast<int*>(base + per - 3 * 32 * sizeof(int));
+    int* sb = sp + 32;
+    int* sl = sp + 64;
+    const int c0 = Crp[i], nC = Crp[i + 1] - c0;
+    for (int s = lane; s < nC; s += 32) cci[s] = Cci[c0 + s];
+    for (int q = lane; q < BRC * maxC; q += 32) acc[q] = T(0);
+    const int a0 = Arp[i], nA = Arp[i + 1] - a0;
+    for (int ab = 0; ab < nA; ab += 32) {
+        const int a = ab + lane;
+        int len = 0, kb = 0;
+        if (a < nA) {
+            const int k = Aci[a0 + a];
+            kb = Brp[k];
+            len = Brp[k + 1] - kb;
+        }
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();
+        sp[lane] = incl - len;
+        sb[lane] = kb;
+        sl[lane] = len;
+        __syncwarp();
+        for (int p = lane; p < total; p += 32) {
+            int lo = 0, hi = 31;  // last q with sp[q] <= p (always a non-empty lane)
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (sp[mid] <= p) lo = mid;
+                else hi = mid - 1;
+            }
+            const int q = lo, s = p - sp[q], bq = sb[q], nB = sl[q], aa = ab + q;
+            const int J = Bci[bq + s];
+            int l2 = 0, h2 = nC - 1;
+            while (l2 < h2) {
+                int mid = (l2 + h2) >> 1;
+                if (cci[mid] < J) l2 = mid + 1;
+                else h2 = mid;
+            }
+            T abk[BRK], bbk[BKC];
+#pragma unroll
+            for (int e = 0; e < BRK; e++) abk[e] = A[(size_t)a0 * BRK + e * nA + aa];
+#pragma unroll
+            for (int e = 0; e < BKC; e++) bbk[e] = B[(size_t)bq * BKC + e * nB + s];
+#pragma unroll
+            for (int r = 0; r < BR; r++)
+#pragma unroll
+                for (int cc = 0; cc < BC; cc++) {
+                    T v = T(0);
+#pragma unroll
+                    for (int m = 0; m < BK; m++) v += abk[r * BK + m] * bbk[m * BC + cc];
+                    atomicAdd(&acc[(r * BC + cc) * maxC + l2], v);
+                }
+        }
+        __syncwarp();
+    }
+    __syncwarp();
+    for (int q = lane; q < BRC * nC; q += 32) {
+        const int e = q / nC, s = q - e * nC;
+        C[(size_t)c0 * BRC + q] = acc[e * maxC + s];
+    }
+}
+
 // P = Pt - (4 / (3 rho)) Dinv (A Pt), pattern of A Pt; Pt's block sits at ptpos
 template <class T, int BS>
 __global__ void k_smooth_p(int nnode, const int* __restrict__ rp, const int* __restrict__ ptpos,
@@ -414,22 +500,32 @@ __global__ void k_dot2(long n, const T* __restrict__ v, const T* __restrict__ w,
     block_sum<2>(s, sm);
     if (threadIdx.x == 0) { part[2 * blockIdx.x] = s[0]; part[2 * blockIdx.x + 1] = s[1]; }
 }
+// lam = Rayleigh estimate, scal = 1/||w|| for the next step, cheb_rho =
+// safety * lam (the Chebyshev smoother's spectral bound)
 __global__ void k_power_final(int nb, const double* __restrict__ part, double* __restrict__ lam,
-                              double* __restrict__ scal) {
+                              double* __restrict__ scal, double* __restrict__ cheb_rho, double safety) {
     __shared__ double sm[64];
     double s[2] = {0.0, 0.0};
     for (int i = threadIdx.x; i < nb; i += blockDim.x) { s[0] += part[2 * i]; s[1] += part[2 * i + 1]; }
     block_sum<2>(s, sm);
     if (threadIdx.x == 0) {
         *lam = s[0];
+        *cheb_rho = safety * s[0];
         *scal = s[1] > 0.0 ? 1.0 / sqrt(s[1]) : 1.0;
     }
 }
+// start vector uniform in [-1, 1) from a splitmix64 hash of the index: rich
+// in the high-frequency modes the power iteration must find
 template <class T>
 __global__ void k_power_seed(long n, T* __restrict__ v, double* __restrict__ scal) {
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-        v[i] = T(1.0 + 0.1 * (double)((i * 7919) % 13) / 13.0);
-    if (blockIdx.x == 0 && threadIdx.x == 0) *scal = 1.0 / sqrt((double)n * 1.1);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        unsigned long long z = (unsigned long long)i * 0x9E3779B97F4A7C15ULL + 0x632BE59BD9B4E019ULL;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        z ^= z >> 31;
+        v[i] = T(2.0 * (double)(z >> 11) * (1.0 / 9007199254740992.0) - 1.0);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *scal = 1.0 / sqrt((double)n / 3.0);
 }
 
 // ----------------------------------------------------------------- coarsest level
@@ -589,11 +685,12 @@ template <int BR, int BK, int BC, class T>
 static int spgemm(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp, const T* B, const DevPattern& Cp,
                   T* C) {
     const size_t mc = (size_t)std::max(Cp.maxrow, 1);
-    const size_t per = ((mc * BR * BC * sizeof(T) + 15) & ~(size_t)15) + ((mc * sizeof(int) + 15) & ~(size_t)15);
+    const size_t per = ((mc * BR * BC * sizeof(T) + 15) & ~(size_t)15) + ((mc * sizeof(int) + 15) & ~(size_t)15) +
+                       3 * 32 * sizeof(int);
     int warps = (int)std::min<size_t>(8, std::max<size_t>(1, (200 * 1024) / per));
     const size_t smem = per * warps;
     if (smem > 227 * 1024) { set_error("SpGEMM row too long for shared memory (%d blocks)", Cp.maxrow); return TOPO_ERR_UNSUPPORTED; }
-    auto kern = k_spgemm<T, BR, BK, BC>;
+    auto kern = k_spgemm_pairs<T, BR, BK, BC>;
     TCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = (Cp.nrows + warps - 1) / warps;
     kern<<<grid, warps * 32, smem, c.s>>>(Cp.nrows, Ap.rp.p, Ap.ci.p, A, Bp.rp.p, Bp.ci.p, B, Cp.rp.p, Cp.ci.p, C,
@@ -655,7 +752,8 @@ static int estimate_rho(Ctx& c, int l, int iters) {
         // w = sigma Dinv A v with sigma = 1/||v||; lam = (sigma v).w; sigma' = 1/||w||
         TRET(level_spmv<T>(c, l, v.pv[l].p, v.pw[l].p, (const T*)nullptr, 3, v.dinv[l].p, scal));
         k_dot2<T><<<nb, 256, 0, c.s>>>(D.ndof, v.pv[l].p, v.pw[l].p, scal, c.red.p), note_launch();
-        k_power_final<<<1, 1024, 0, c.s>>>(nb, c.red.p, lam, scal), note_launch();
+        k_power_final<<<1, 1024, 0, c.s>>>(nb, c.red.p, lam, scal, c.rho.p + 2 * kMaxLevels + l,
+                                           c.p.cheb_safety > 0 ? c.p.cheb_safety : 1.0), note_launch();
         std::swap(v.pv[l], v.pw[l]);
     }
     TCK(cudaGetLastError());
@@ -668,7 +766,9 @@ static int numeric(Ctx& c) {
     AmgVals<T>& v = vals<T>(c);
     const T* ke = std::is_same<T, double>::value ? (const T*)c.ke64.p : (const T*)c.ke32.p;
     const T* Ee = std::is_same<T, double>::value ? (const T*)c.Ee64.p : (const T*)c.Ee32.p;
+    cudaEvent_t pe;
     // level-0 assembly
+    prof_begin(c, PS_SETUP_ASM, &pe);
     {
         AmgDevLevel& D = c.dl[0];
         const int wpb = 4;
@@ -692,6 +792,7 @@ static int numeric(Ctx& c) {
                                                                      v.A[0].p, v.A0s.p), note_launch();
         TCK(cudaGetLastError());
     }
+    prof_end(c, PS_SETUP_ASM, pe);
     for (int l = 0; l < c.nlev; l++) {
         AmgDevLevel& D = c.dl[l];
         if (D.bs == 3)
@@ -702,7 +803,10 @@ static int numeric(Ctx& c) {
                                                                            v.dinv[l].p), note_launch();
         TCK(cudaGetLastError());
         if (l == c.nlev - 1) break;
-        TRET(estimate_rho<T>(c, l, l == 0 ? 6 : 10));
+        prof_begin(c, PS_SETUP_RHO, &pe);
+        TRET(estimate_rho<T>(c, l, std::max(1, c.p.amg_rho_its)));
+        prof_end(c, PS_SETUP_RHO, pe);
+        prof_begin(c, PS_SETUP_GAL, &pe);
         AmgDevLevel& N = c.dl[l + 1];
         // T = A Pt ; P = Pt - w Dinv T
         const T* ptv = pt_vals<T>(c, l);
@@ -732,8 +836,10 @@ static int numeric(Ctx& c) {
             TRET((spgemm<6, 6, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p)));
         }
         TCK(cudaGetLastError());
+        prof_end(c, PS_SETUP_GAL, pe);
     }
     // coarsest: dense FP64 inverse
+    prof_begin(c, PS_SETUP_COARSE, &pe);
     {
         const int L = c.nlev - 1;
         AmgDevLevel& D = c.dl[L];
@@ -755,6 +861,7 @@ static int numeric(Ctx& c) {
                                              in_smem), note_launch();
         TCK(cudaGetLastError());
     }
+    prof_end(c, PS_SETUP_COARSE, pe);
     return 0;
 }
 
@@ -778,7 +885,7 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
     const int deg = std::max(1, c.p.cheb_degree);
     double cr[16] = {0}, cq[16] = {0};
     cheb_coeffs(std::min(deg, 16), cr, cq);
-    const double* rho = c.rho.p + l;
+    const double* rho = c.rho.p + 2 * kMaxLevels + l;  // safety-scaled spectral bound
     const bool matfree = (l == 0) && c.p.fine_smoother_matfree;
     if (!zero_init) {
         // r = b - A x
@@ -856,6 +963,68 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
         else TRET((spmv<T, 6, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 2)));
         TRET(smooth<T>(c, l, bl[l], xl[l], false));
     }
+    return 0;
+}
+
+// re-seed the warm-started power iterations (a fresh optimisation run then
+// reproduces the first one's preconditioners)
+template <class T>
+static int reseed(Ctx& c) {
+    AmgVals<T>& v = vals<T>(c);
+    if (!v.allocated) return 0;
+    for (int l = 0; l < c.nlev; l++) {
+        k_power_seed<T><<<grid_for(c.dl[l].ndof, 256), 256, 0, c.s>>>(c.dl[l].ndof, v.pv[l].p, c.rho.p + kMaxLevels + l),
+            note_launch();
+    }
+    TCK(cudaGetLastError());
+    return 0;
+}
+int amg_reset_warm_start(Ctx& c) {
+    TRET(reseed<double>(c));
+    return reseed<float>(c);
+}
+
+// host copy of level l matrix `which` (0 A, 1 P, 2 R) as plain BSR
+template <class T>
+static int level_copy(Ctx& c, int l, int which, std::vector<double>& out, const DevPattern*& pat, int& br, int& bc) {
+    AmgVals<T>& v = vals<T>(c);
+    if (!v.allocated) { set_error("no AMG hierarchy built yet (run a solve first)"); return TOPO_ERR_ARG; }
+    const AmgDevLevel& D = c.dl[l];
+    const T* src;
+    if (which == 0) { pat = &D.A; br = bc = D.bs; src = v.A[l].p; }
+    else if (which == 1) { pat = &D.P; br = D.bs; bc = 6; src = v.P[l].p; }
+    else { pat = &D.R; br = 6; bc = D.bs; src = v.R[l].p; }
+    const long nv = pat->nnzb * br * bc;
+    std::vector<T> raw(nv);
+    std::vector<int> rp(pat->nrows + 1);
+    TCK(cudaMemcpyAsync(raw.data(), src, sizeof(T) * nv, cudaMemcpyDeviceToHost, c.s));
+    TCK(cudaMemcpyAsync(rp.data(), pat->rp.p, sizeof(int) * (pat->nrows + 1), cudaMemcpyDeviceToHost, c.s));
+    TCK(cudaStreamSynchronize(c.s));
+    out.assign(nv, 0.0);
+    const int bb = br * bc;
+    for (int i = 0; i < pat->nrows; i++) {
+        const int r0 = rp[i], nb = rp[i + 1] - r0;
+        for (int s = 0; s < nb; s++)
+            for (int e = 0; e < bb; e++) out[((size_t)r0 + s) * bb + e] = (double)raw[(size_t)r0 * bb + e * nb + s];
+    }
+    return 0;
+}
+
+int amg_level_copy(Ctx& c, int l, int which, std::vector<double>& vals_out, std::vector<int>& rp, std::vector<int>& ci,
+                   int& nrows, int& ncols, int& br, int& bc) {
+    if (l < 0 || l >= c.nlev || which < 0 || which > 2 || (which > 0 && l == c.nlev - 1)) {
+        set_error("no such AMG level matrix");
+        return TOPO_ERR_ARG;
+    }
+    const DevPattern* pat = nullptr;
+    if (c.p.precision == TOPO_PREC_MIXED) TRET(level_copy<float>(c, l, which, vals_out, pat, br, bc));
+    else TRET(level_copy<double>(c, l, which, vals_out, pat, br, bc));
+    nrows = pat->nrows;
+    ncols = pat->ncols;
+    rp.resize(nrows + 1);
+    ci.resize(pat->nnzb);
+    TCK(cudaMemcpy(rp.data(), pat->rp.p, sizeof(int) * (nrows + 1), cudaMemcpyDeviceToHost));
+    TCK(cudaMemcpy(ci.data(), pat->ci.p, sizeof(int) * pat->nnzb, cudaMemcpyDeviceToHost));
     return 0;
 }
 

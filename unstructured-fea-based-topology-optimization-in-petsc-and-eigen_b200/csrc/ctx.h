@@ -169,7 +169,14 @@ struct Ctx {
 };
 
 // profiler slots
-enum ProfSlot { PS_KMV = 0, PS_CHEB0 = 1, PS_RES0 = 2, PS_FILTER = 3, PS_SPGEMM = 4, PS_COUNT = 8 };
+enum ProfSlot {
+    PS_KMV = 0, PS_CHEB0 = 1, PS_RES0 = 2, PS_FILTER = 3,
+    PS_SETUP_ASM = 4,     // level-0 assembly + sliced-ELLPACK copy + diagonals
+    PS_SETUP_RHO = 5,     // power iterations
+    PS_SETUP_GAL = 6,     // smoothing of P + Galerkin products + transposes
+    PS_SETUP_COARSE = 7,  // coarsest dense inverse
+    PS_COUNT = 8
+};
 cudaEvent_t prof_event(Ctx& c);
 inline void prof_begin(Ctx& c, int slot, cudaEvent_t* e0) {
     *e0 = nullptr;
@@ -205,6 +212,9 @@ int von_mises(Ctx& c, const double* xphys, double* vms);
 
 int amg_alloc(Ctx& c);                                             // amg.cu
 int amg_numeric(Ctx& c);
+int amg_reset_warm_start(Ctx& c);
+int amg_level_copy(Ctx& c, int l, int which, std::vector<double>& vals_out, std::vector<int>& rp, std::vector<int>& ci,
+                   int& nrows, int& ncols, int& br, int& bc);
 int amg_vcycle64(Ctx& c, const double* b, double* x);
 int amg_vcycle32(Ctx& c, const double* b64, float* x);
 

@@ -12,10 +12,16 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "ctx.h"
 
 namespace topo {
+
+static std::mutex& coop_mutex() {
+    static std::mutex m;
+    return m;
+}
 
 constexpr int kMmaSlots = 32;  // mma_scal layout: lam[4] mu[4] y[4] z b[4] its err
 enum { MS_LAM = 0, MS_MU = 4, MS_Y = 8, MS_Z = 12, MS_B = 13, MS_ITS = 17, MS_ERR = 18 };
@@ -480,15 +486,20 @@ static int update_m(Ctx& c, double* x, const double* dfdx, const double* gx_dev,
     const double* Lp = c.L.p; const double* Up = c.Uas.p; const double* al = c.alpha.p; const double* be = c.beta.p;
     int nn = n;
     void* args[] = {&nn, &x, &p0, &q0, &pij, &qij, &Lp, &Up, &al, &be, &ms, &kc, &tol, &part1, &part2, &gb};
-    TCK(cudaLaunchCooperativeKernel((void*)k_solvedip<M>, dim3(blocks), dim3(256), args, 0, c.s));
-    note_launch();
-    // barrier status + iteration count
-    TCK(cudaMemcpyAsync(c.hsc.h + 200, ms + MS_ITS, sizeof(double), cudaMemcpyDeviceToHost, c.s));
-    int herr = 0;
-    TCK(cudaMemcpyAsync(&herr, c.bar_err.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
-    TCK(cudaStreamSynchronize(c.s));
+    int* herr = reinterpret_cast<int*>(c.hsc.h + 201);
+    *herr = 0;
+    {
+        // one cooperative grid in flight per process: concurrent jobs (serving)
+        // never hold parts of the device against each other's grid barriers
+        std::lock_guard<std::mutex> lk(coop_mutex());
+        TCK(cudaLaunchCooperativeKernel((void*)k_solvedip<M>, dim3(blocks), dim3(256), args, 0, c.s));
+        note_launch();
+        TCK(cudaMemcpyAsync(c.hsc.h + 200, ms + MS_ITS, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+        TCK(cudaMemcpyAsync(herr, c.bar_err.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+        TCK(cudaStreamSynchronize(c.s));
+    }
     c.info.mma_inner_its = (int)c.hsc.h[200];
-    if (herr) { set_error("MMA dual solve: grid barrier timed out"); return TOPO_ERR_TIMEOUT; }
+    if (*herr) { set_error("MMA dual solve: grid barrier timed out"); return TOPO_ERR_TIMEOUT; }
     return 0;
 }
 

@@ -1,0 +1,287 @@
+// serve.cpp -- continuous-batching job server over independent contexts.
+//
+// Every submitted job (its own mesh, options and iteration count) waits in a
+// FIFO until its arrival time has passed, a slot is free and its estimated
+// HBM footprint fits the budget; it is then admitted: a worker thread builds
+// its context on a stream of its own and runs its design iterations back to
+// back, so the kernels of all admitted jobs overlap on the device.  A job
+// that finishes frees its slot and memory at once and the scheduler admits
+// the next ones: no step barrier couples the jobs.  Each job's state
+// (densities, displacements, filter warm start, MMA history) stays resident
+// in its context from admission to completion.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "ctx.h"
+
+namespace topo {
+void set_error(const char* fmt, ...);
+const char* last_error();
+}  // namespace topo
+
+using namespace topo;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+    int id = 0;
+    topo_params p{};
+    int nen = 8, nn = 0, ne = 0, ncases = 1, iterations = 0;
+    std::vector<double> vertex, load_vals;
+    std::vector<int32_t> element, fixed, case_ptr, load_dofs;
+    double arrival_s = 0.0;
+    size_t est_bytes = 0;
+    // results
+    int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
+    int status = 0;
+    std::string error;
+    double admit_s = 0.0, finish_s = 0.0;
+    std::vector<double> iter_ms, fx_hist;
+    std::vector<double> xphys;
+};
+
+}  // namespace
+
+struct topo_server {
+    size_t budget = 0;
+    int max_active = 1;
+    std::vector<Job> jobs;
+    std::mutex mu;
+    std::condition_variable cv;
+    size_t reserved = 0, peak_reserved = 0;
+    int active = 0, max_seen = 0;
+    double makespan = 0.0;
+    bool ran = false;
+};
+
+extern "C" {
+
+size_t topo_estimate_job_bytes(int nen, int n_nodes, int n_elems, int precision) {
+    // per element: packed Ke in FP64 + FP32, connectivity, masks, element
+    // pair slots, filter matrices, SIMP moduli, design and MMA vectors
+    const double npk = nen == 8 ? 300 : 78, nkf = nen == 8 ? 36 : 10;
+    const double per_elem = npk * 12 + 4.0 * nen + 4 + 2.0 * nen * nen + nkf * 8 + nen * 8 + 12 + 8 + 20 * 8 + 4.0 * nen;
+    // per node: level-0 operator (BSR + sliced ELLPACK), prolongator and
+    // its smoothing temporary, A*P, restriction, Krylov basis, vectors
+    const double s = precision == TOPO_PREC_MIXED ? 4.0 : 8.0;
+    const double deg = nen == 8 ? 27.0 : 24.0;
+    const double per_node = deg * (9 * s + 4) * 2 + 8 * 18 * s * 3 + deg * 18 * s + 31 * 24 + 30 * 3 * s + 16 * 24 + 8 * 3 * s +
+                            7 * 8;
+    const double bytes = n_elems * per_elem + n_nodes * per_node * 1.25 + 96.0 * (1 << 20);
+    return (size_t)bytes;
+}
+
+int topo_server_create(size_t hbm_budget_bytes, int max_active, topo_server** out) {
+    if (!out || max_active < 1) { set_error("bad argument"); return TOPO_ERR_ARG; }
+    try {
+        topo_server* s = new topo_server();
+        if (hbm_budget_bytes == 0) {
+            size_t fr = 0, tot = 0;
+            if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+                cudaGetLastError();
+                delete s;
+                set_error("no CUDA device: this library has no CPU fallback");
+                return TOPO_ERR_CUDA;
+            }
+            hbm_budget_bytes = (size_t)(0.85 * fr);
+        }
+        s->budget = hbm_budget_bytes;
+        s->max_active = max_active;
+        *out = s;
+        return 0;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return TOPO_ERR_OOM;
+    }
+}
+
+int topo_server_destroy(topo_server* s) {
+    delete s;
+    return 0;
+}
+
+int topo_server_submit(topo_server* s, const topo_params* p, int nen, int n_nodes, const double* vertex, int n_elems,
+                       const int32_t* element, int n_fixed, const int32_t* fixed_dofs, int n_cases,
+                       const int32_t* case_ptr, const int32_t* load_dofs, const double* load_vals, int iterations,
+                       double arrival_s, int* job_id) {
+    if (!s || !vertex || !element || !case_ptr || (n_fixed > 0 && !fixed_dofs) || iterations < 1 || n_cases < 1) {
+        set_error("bad argument");
+        return TOPO_ERR_ARG;
+    }
+    if (s->ran) { set_error("the server already ran; create a new one"); return TOPO_ERR_ARG; }
+    try {
+        Job j;
+        j.id = (int)s->jobs.size();
+        if (p) j.p = *p;
+        else topo_params_default(&j.p);
+        j.nen = nen;
+        j.nn = n_nodes;
+        j.ne = n_elems;
+        j.ncases = n_cases;
+        j.iterations = iterations;
+        j.arrival_s = arrival_s;
+        j.vertex.assign(vertex, vertex + 3L * n_nodes);
+        j.element.assign(element, element + (long)n_elems * nen);
+        j.fixed.assign(fixed_dofs, fixed_dofs + n_fixed);
+        j.case_ptr.assign(case_ptr, case_ptr + n_cases + 1);
+        j.load_dofs.assign(load_dofs, load_dofs + case_ptr[n_cases]);
+        j.load_vals.assign(load_vals, load_vals + case_ptr[n_cases]);
+        j.est_bytes = topo_estimate_job_bytes(nen, n_nodes, n_elems, j.p.precision);
+        if (j.est_bytes > s->budget) {
+            set_error("job %d needs about %zu bytes, more than the whole budget %zu", j.id, j.est_bytes, s->budget);
+            return TOPO_ERR_OOM;
+        }
+        if (job_id) *job_id = j.id;
+        s->jobs.push_back(std::move(j));
+        return 0;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return TOPO_ERR_OOM;
+    }
+}
+
+static void run_job(topo_server* s, Job* j, Clock::time_point t0) {
+    topo_ctx* ctx = nullptr;
+    int rc = topo_create(&j->p, j->nen, j->nn, j->vertex.data(), j->ne, j->element.data(), (int)j->fixed.size(),
+                         j->fixed.data(), j->ncases, j->case_ptr.data(), j->load_dofs.data(), j->load_vals.data(),
+                         nullptr, &ctx);
+    if (rc >= 0) rc = topo_opt_init(ctx);
+    for (int it = 0; rc >= 0 && it < j->iterations; it++) {
+        auto a = Clock::now();
+        int itr = 0;
+        double fx = 0.0, gx = 0.0, ch = 0.0;
+        rc = topo_opt_step(ctx, &itr, &fx, &gx, &ch);
+        auto b = Clock::now();
+        j->iter_ms.push_back(std::chrono::duration<double, std::milli>(b - a).count());
+        j->fx_hist.push_back(fx);
+    }
+    if (rc >= 0) {
+        double* xp = nullptr;
+        j->xphys.resize(j->ne);
+        rc = topo_opt_vector(ctx, 1, &xp);
+        if (rc >= 0) rc = topo_memcpy_d2h(j->xphys.data(), xp, sizeof(double) * j->ne, ctx);
+    }
+    if (rc < 0) j->error = topo::last_error();
+    if (ctx) topo_destroy(ctx);
+    std::lock_guard<std::mutex> lk(s->mu);
+    j->status = rc;
+    j->state = rc < 0 ? 3 : 2;
+    j->finish_s = std::chrono::duration<double>(Clock::now() - t0).count();
+    s->reserved -= j->est_bytes;
+    s->active--;
+    s->cv.notify_all();
+}
+
+int topo_server_run(topo_server* s) {
+    if (!s) { set_error("null server"); return TOPO_ERR_ARG; }
+    if (s->ran) { set_error("the server already ran"); return TOPO_ERR_ARG; }
+    s->ran = true;
+    std::vector<int> order(s->jobs.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return s->jobs[a].arrival_s < s->jobs[b].arrival_s; });
+    std::vector<std::thread> workers;
+    const auto t0 = Clock::now();
+    size_t next = 0;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        while (true) {
+            const double now = std::chrono::duration<double>(Clock::now() - t0).count();
+            // FIFO admission: the head of the queue goes first once it has
+            // arrived and fits (slot + estimated footprint)
+            while (next < order.size()) {
+                Job& j = s->jobs[order[next]];
+                if (j.arrival_s > now || s->active >= s->max_active || s->reserved + j.est_bytes > s->budget) break;
+                j.state = 1;
+                j.admit_s = now;
+                s->reserved += j.est_bytes;
+                s->peak_reserved = std::max(s->peak_reserved, s->reserved);
+                s->active++;
+                s->max_seen = std::max(s->max_seen, s->active);
+                workers.emplace_back(run_job, s, &j, t0);
+                next++;
+            }
+            if (next == order.size() && s->active == 0) break;
+            if (next < order.size() && s->jobs[order[next]].arrival_s > now && s->active < s->max_active) {
+                const double wait = s->jobs[order[next]].arrival_s - now;
+                s->cv.wait_for(lk, std::chrono::duration<double>(wait));
+            } else {
+                s->cv.wait_for(lk, std::chrono::milliseconds(50));
+            }
+        }
+    }
+    for (auto& t : workers) t.join();
+    s->makespan = std::chrono::duration<double>(Clock::now() - t0).count();
+    int failed = 0;
+    for (auto& j : s->jobs) failed += j.state == 3;
+    if (failed) {
+        set_error("%d job(s) failed", failed);
+        return TOPO_NOT_CONVERGED;
+    }
+    return 0;
+}
+
+int topo_server_job(topo_server* s, int job_id, int* status, int* n_iters, double* iter_ms, double* fx_hist,
+                    double* xphys, double* admit_s, double* finish_s) {
+    if (!s || job_id < 0 || job_id >= (int)s->jobs.size()) { set_error("no such job"); return TOPO_ERR_ARG; }
+    const Job& j = s->jobs[job_id];
+    if (status) *status = j.status;
+    if (n_iters) *n_iters = (int)j.iter_ms.size();
+    if (iter_ms) std::copy(j.iter_ms.begin(), j.iter_ms.end(), iter_ms);
+    if (fx_hist) std::copy(j.fx_hist.begin(), j.fx_hist.end(), fx_hist);
+    if (xphys && !j.xphys.empty()) std::copy(j.xphys.begin(), j.xphys.end(), xphys);
+    if (admit_s) *admit_s = j.admit_s;
+    if (finish_s) *finish_s = j.finish_s;
+    if (j.state == 3) set_error("%s", j.error.c_str());
+    return j.state == 3 ? j.status : 0;
+}
+
+int topo_server_stats_get(topo_server* s, topo_server_stats* st) {
+    if (!s || !st) { set_error("null argument"); return TOPO_ERR_ARG; }
+    std::vector<double> lat, wait;
+    int done = 0, failed = 0;
+    long iters = 0;
+    for (const auto& j : s->jobs) {
+        done += j.state == 2;
+        failed += j.state == 3;
+        iters += (long)j.iter_ms.size();
+        lat.insert(lat.end(), j.iter_ms.begin(), j.iter_ms.end());
+        if (j.state >= 2) wait.push_back(j.admit_s - j.arrival_s);
+    }
+    auto pct = [](std::vector<double> v, double q) {
+        if (v.empty()) return 0.0;
+        std::sort(v.begin(), v.end());
+        const double pos = q * (v.size() - 1);
+        const size_t lo = (size_t)std::floor(pos), hi = std::min(v.size() - 1, lo + 1);
+        return v[lo] + (pos - lo) * (v[hi] - v[lo]);
+    };
+    st->jobs_submitted = (int)s->jobs.size();
+    st->jobs_done = done;
+    st->jobs_failed = failed;
+    st->max_active = s->max_seen;
+    st->iterations = iters;
+    st->p50_iter_ms = pct(lat, 0.5);
+    st->p99_iter_ms = pct(lat, 0.99);
+    double sum = 0.0;
+    for (double x : lat) sum += x;
+    st->mean_iter_ms = lat.empty() ? 0.0 : sum / lat.size();
+    st->makespan_s = s->makespan;
+    st->jobs_per_hour = s->makespan > 0 ? 3600.0 * done / s->makespan : 0.0;
+    st->iters_per_s = s->makespan > 0 ? iters / s->makespan : 0.0;
+    st->peak_reserved_bytes = (double)s->peak_reserved;
+    st->p50_queue_s = pct(wait, 0.5);
+    st->p99_queue_s = pct(wait, 0.99);
+    return 0;
+}
+
+}  // extern "C"

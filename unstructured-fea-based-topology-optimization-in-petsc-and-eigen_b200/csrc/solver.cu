@@ -17,7 +17,7 @@ namespace topo {
 
 int kmatvec64r(Ctx& c, const double* u, double* y, const double* b);
 
-constexpr int kRedBlocks = 296;  // 2 x 148 SMs
+constexpr int kRedBlocks = 1184;  // 8 x 148 SMs: enough warps in flight for the vector sweeps
 
 // ----------------------------------------------------------------- reductions
 __global__ void k_dot(long n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ part) {
@@ -28,19 +28,20 @@ __global__ void k_dot(long n, const double* __restrict__ a, const double* __rest
     if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
 // out[k] = sum_b part[b*nv + k]; optional sqrt of entry `sqrt_idx`
+// one warp per value (launch with 32 * min(nv, 32) threads; more values loop)
 __global__ void k_final(int nb, int nv, const double* __restrict__ part, double* __restrict__ out, int sqrt_idx) {
-    __shared__ double sm[32];
-    for (int k = 0; k < nv; k++) {
-        double v[1] = {0.0};
-        for (int i = threadIdx.x; i < nb; i += blockDim.x) v[0] += part[(long)i * nv + k];
-        block_sum<1>(v, sm);
-        if (threadIdx.x == 0) out[k] = (k == sqrt_idx) ? sqrt(v[0]) : v[0];
-        __syncthreads();
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int k = threadIdx.x >> 5; k < nv; k += nw) {
+        double v = 0.0;
+        for (int i = lane; i < nb; i += 32) v += part[(long)i * nv + k];
+        v = warp_sum(v);
+        if (lane == 0) out[k] = (k == sqrt_idx) ? sqrt(v) : v;
     }
 }
+static inline int final_threads(int nv) { return 32 * std::max(1, std::min(nv, 32)); }
 
 int finalize_sum(Ctx& c, const double* partials, int nparts, int nv, double* out_dev) {
-    k_final<<<1, 512, 0, c.s>>>(nparts, nv, partials, out_dev, -1), note_launch();
+    k_final<<<1, final_threads(nv), 0, c.s>>>(nparts, nv, partials, out_dev, -1), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -122,7 +123,7 @@ static int orth(Ctx& c, int nv, const double* V, long ld, const double* h, doubl
     if (nv <= 8) k_orth<8><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p), note_launch();
     else if (nv <= 16) k_orth<16><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p), note_launch();
     else k_orth<32><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p), note_launch();
-    k_final<<<1, 512, 0, c.s>>>(kRedBlocks, 1, c.red.p, hn_out, 0), note_launch();
+    k_final<<<1, 32, 0, c.s>>>(kRedBlocks, 1, c.red.p, hn_out, 0), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -396,7 +397,7 @@ int filter_cg(Ctx& c, const double* b, double* x, int* its_out) {
         k_cg_p<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.fz.p, c.fp.p, sc, i == 0), note_launch();
         TRET(filter_kf(c, c.fp.p, c.fw.p));
         k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.red.p), note_launch();
-        k_final<<<1, 512, 0, c.s>>>(kRedBlocks, 1, c.red.p, sc + 4, -1), note_launch();
+        k_final<<<1, 32, 0, c.s>>>(kRedBlocks, 1, c.red.p, sc + 4, -1), note_launch();
         k_cg_step<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.fdiag_inv.p, x, c.fr.p, c.fz.p, sc, c.red.p), note_launch();
         k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 2, c.red.p, sc, 0), note_launch();
         TCK(cudaMemcpyAsync(hs, sc, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
