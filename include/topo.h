@@ -73,6 +73,8 @@ typedef struct topo_params {
     int verbose;           /* 1: print the reference's per-solve lines */
     int amg_rho_its;       /* power iterations for rho(D^-1 A) per level and design iteration */
     double cheb_safety;    /* Chebyshev interval [0.1, 1.1] * cheb_safety * rho */
+    int fem_warm_start;    /* 1: start FGMRES from the previous U instead of 0 (the
+                              reference zeroes U, SolveFem.cpp:333); same stopping rule */
 } topo_params;
 
 typedef struct topo_solve_info {

@@ -38,7 +38,8 @@ class Params(C.Structure):
         ("amg_max_levels", C.c_int), ("amg_coarse_max", C.c_int), ("amg_smooth_p", C.c_int),
         ("cheb_degree", C.c_int), ("fine_smoother_matfree", C.c_int),
         ("filter_rtol", C.c_double), ("filter_atol", C.c_double), ("filter_dtol", C.c_double),
-        ("filter_maxit", C.c_int), ("verbose", C.c_int), ("amg_rho_its", C.c_int), ("cheb_safety", C.c_double)]
+        ("filter_maxit", C.c_int), ("verbose", C.c_int), ("amg_rho_its", C.c_int), ("cheb_safety", C.c_double),
+        ("fem_warm_start", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -261,7 +262,10 @@ class Context:
         self.nen, self.nn, self.ne = nen, vertex.size // 3, element.size // nen
         self.ndof, self.ncases = 3 * self.nn, case_ptr.size - 1
         if stream is None:
-            stream = torch.cuda.current_stream().cuda_stream
+            # torch's current stream; its legacy default stream (handle 0) is
+            # passed as cudaStreamLegacy (1) so that the library's work stays
+            # ordered with torch's instead of getting a stream of its own
+            stream = torch.cuda.current_stream().cuda_stream or 1
         self.stream = stream
         h = C.c_void_p()
         _check(lib().topo_create(C.byref(self.params), nen, self.nn, _ptr(vertex), self.ne, _ptr(element.reshape(-1)),

@@ -182,6 +182,7 @@ int opt_init(Ctx& c) {
     // a fresh optimisation: MMA history, filter warm start and beta state
     // start over as in a new process (MMA.cpp:178-224, PDEFilter.cpp:64-67)
     c.mma_k = 0;
+    c.u_valid = false;
     for (DBuf<double>* b : {&c.xo1, &c.xo2, &c.L, &c.Uas, &c.RX}) TRET(b->zero(c.s));
     c.beta_proj = c.beta_tmp = c.p.beta0;
     TRET(amg_reset_warm_start(c));
@@ -200,7 +201,7 @@ int create(Ctx& c, int nen, int n_nodes, const double* vertex, int n_elems, cons
     for (int i = 0; i < 4; i++) TCK(cudaEventCreate(&c.ev[i]));
     TRET(c.dsc.alloc(DS_COUNT));
     TRET(c.dsc.zero(c.s));
-    TRET(c.hsc.alloc(512));
+    TRET(c.hsc.alloc(1024));
     TRET(build_mesh(c, vertex, element, n_fixed, fixed, n_cases, case_ptr, load_dofs, load_vals));
     TRET(elem_setup(c));
     TRET(sum_device(c, c.vol.p, c.ne, &c.TV));
@@ -276,6 +277,7 @@ void topo_params_default(topo_params* p) {
     p->verbose = 0;
     p->amg_rho_its = 10;
     p->cheb_safety = 1.0;
+    p->fem_warm_start = 0;
 }
 
 int topo_device_alloc(size_t bytes, void** ptr) {
@@ -314,7 +316,7 @@ static int check_params(const topo_params* p) {
         return TOPO_ERR_ARG;
     }
     if (p->m < 1 || p->m > kMaxM) { set_error("m must be in [1,%d]", kMaxM); return TOPO_ERR_ARG; }
-    if (p->fem_restart < 1 || p->fem_restart > 30) { set_error("fem_restart must be in [1,30]"); return TOPO_ERR_ARG; }
+    if (p->fem_restart < 1 || p->fem_restart > 128) { set_error("fem_restart must be in [1,128]"); return TOPO_ERR_ARG; }
     if (p->cheb_degree < 1 || p->cheb_degree > 15) { set_error("cheb_degree must be in [1,15]"); return TOPO_ERR_ARG; }
     if (p->precision != TOPO_PREC_FP64 && p->precision != TOPO_PREC_MIXED) { set_error("bad precision"); return TOPO_ERR_ARG; }
     if (p->amg_coarse_max < 6 || p->amg_coarse_max > 4000) { set_error("amg_coarse_max must be in [6,4000]"); return TOPO_ERR_ARG; }

@@ -156,6 +156,7 @@ struct Ctx {
     int itr = 0;
     double ch = 1.0, beta_proj = 1.0, beta_tmp = 1.0;
     bool opt_ready = false;
+    bool u_valid = false;       // U holds a solution of this optimisation run
 
     topo_solve_info info{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -236,9 +237,9 @@ enum DscSlot {
     DS_FX = 0, DS_GX = 1,          // .. DS_GX + kMaxM - 1
     DS_CH = 8, DS_TMP = 9,
     DS_CG = 16,                    // CG scratch (16..31)
-    DS_GM = 32,                    // FGMRES column (32..127)
-    DS_KKT = 128,
-    DS_COUNT = 160
+    DS_GM = 32,                    // FGMRES column (32..170)
+    DS_KKT = 176,
+    DS_COUNT = 200
 };
 
 }  // namespace topo

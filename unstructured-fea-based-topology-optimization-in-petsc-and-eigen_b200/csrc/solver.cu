@@ -100,7 +100,7 @@ __global__ void k_scale_to(long n, const double* __restrict__ w, const double* _
 template <class TZ>
 __global__ void k_update(long n, int kd, const TZ* __restrict__ Z, long ld, const double* __restrict__ y,
                          double* __restrict__ x) {
-    __shared__ double ys[64];
+    __shared__ double ys[128];
     if (threadIdx.x < kd) ys[threadIdx.x] = y[threadIdx.x];
     __syncthreads();
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -110,19 +110,30 @@ __global__ void k_update(long n, int kd, const TZ* __restrict__ Z, long ld, cons
     }
 }
 
+// classical Gram-Schmidt sweeps in chunks of at most 32 basis vectors
 static int mdot(Ctx& c, int nv, const double* V, long ld, const double* w, double* out) {
     long n = c.ndof;
-    if (nv <= 8) k_mdot<8><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p), note_launch();
-    else if (nv <= 16) k_mdot<16><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p), note_launch();
-    else k_mdot<32><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, w, c.red.p), note_launch();
-    TCK(cudaGetLastError());
-    return finalize_sum(c, c.red.p, kRedBlocks, nv, out);
+    for (int j0 = 0; j0 < nv; j0 += 32) {
+        const int k = std::min(32, nv - j0);
+        const double* Vj = V + (size_t)j0 * ld;
+        if (k <= 8) k_mdot<8><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
+        else if (k <= 16) k_mdot<16><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
+        else k_mdot<32><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
+        TCK(cudaGetLastError());
+        TRET(finalize_sum(c, c.red.p, kRedBlocks, k, out + j0));
+    }
+    return 0;
 }
 static int orth(Ctx& c, int nv, const double* V, long ld, const double* h, double* w, double* hn_out) {
     long n = c.ndof;
-    if (nv <= 8) k_orth<8><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p), note_launch();
-    else if (nv <= 16) k_orth<16><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p), note_launch();
-    else k_orth<32><<<kRedBlocks, 256, 0, c.s>>>(n, nv, V, ld, h, w, c.red.p), note_launch();
+    for (int j0 = 0; j0 < nv; j0 += 32) {
+        const int k = std::min(32, nv - j0);
+        const double* Vj = V + (size_t)j0 * ld;
+        if (k <= 8) k_orth<8><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
+        else if (k <= 16) k_orth<16><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
+        else k_orth<32><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
+    }
+    // the last sweep's partials hold ||w||^2 of the fully orthogonalised w
     k_final<<<1, 32, 0, c.s>>>(kRedBlocks, 1, c.red.p, hn_out, 0), note_launch();
     TCK(cudaGetLastError());
     return 0;
@@ -202,29 +213,33 @@ __global__ void k_gm_solve(GmLayout L, int kd, double* __restrict__ st) {
 // j+1 state and is discarded.
 static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status) {
     const long n = c.ndof;
-    const int m = std::max(1, std::min(c.p.fem_restart, 30));
+    const int m = std::max(1, std::min(c.p.fem_restart, 128));
     const int maxit = c.p.fem_maxit;
     const GmLayout GL{m};
-    if (!c.V.p) {
+    if (!c.V.p || (long)c.V.n < (long)(m + 1) * n) {
         TRET(c.V.alloc((size_t)(m + 1) * n));
         TRET(c.w.alloc(n));
-        TRET(c.wtmp.alloc(GL.size() + 64));
+        TRET(c.wtmp.alloc(GL.size() + 2 * m + 8));
+        c.Z32.reset();
+        c.Z64.reset();
     }
     if (c.p.precision == TOPO_PREC_MIXED && !c.Z32.p) TRET(c.Z32.alloc((size_t)m * n));
     if (c.p.precision != TOPO_PREC_MIXED && !c.Z64.p) TRET(c.Z64.alloc((size_t)m * n));
     if ((long)c.red.n < kRedBlocks * 40L) TRET(c.red.alloc(std::max<long>(kRedBlocks * 40L, 4096)));
-    if (c.gm_ev.empty()) {
-        c.gm_ev.resize(31);
-        for (auto& e : c.gm_ev) TCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    while ((int)c.gm_ev.size() < m + 1) {
+        cudaEvent_t e;
+        TCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c.gm_ev.push_back(e);
     }
-    double* hs = c.hsc.h;           // pinned: [2j, 2j+1] = (residual, ||w||) of iteration j
+    double* hs = c.hsc.h + 512;     // pinned: [2j, 2j+1] = (residual, ||w||) of iteration j; [300], [301] norms
     double* gm = c.dsc.p + DS_GM;   // Hessenberg column scratch
     double* st = c.wtmp.p;          // device Arnoldi state
-    double* out = st + GL.size();   // per-launch outputs (2 doubles per iteration)
+    double* out = st + GL.size();   // per-launch outputs (2 doubles per iteration, then beta)
+    double* out_beta = out + 2 * m + 2;
     TRET(dev_dot(c, b, b, n, gm));
-    TCK(cudaMemcpyAsync(hs + 100, gm, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    TCK(cudaMemcpyAsync(hs + 300, gm, sizeof(double), cudaMemcpyDeviceToHost, c.s));
     TCK(cudaStreamSynchronize(c.s));
-    const double bnorm = std::sqrt(hs[100]);
+    const double bnorm = std::sqrt(hs[300]);
     const double ttol = std::max(c.p.fem_rtol * bnorm, 1e-50);
     int its = 0;
     bool conv = false;
@@ -232,13 +247,13 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
         // v0 = (b - K x) / beta
         TRET(kmatvec64r(c, x, c.w.p, b));
         TRET(dev_dot(c, c.w.p, c.w.p, n, gm));
-        k_gm_start<<<1, 32, 0, c.s>>>(GL, st, gm, out + 62), note_launch();
-        TCK(cudaMemcpyAsync(hs + 101, out + 62, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+        k_gm_start<<<1, 32, 0, c.s>>>(GL, st, gm, out_beta), note_launch();
+        TCK(cudaMemcpyAsync(hs + 301, out_beta, sizeof(double), cudaMemcpyDeviceToHost, c.s));
         TCK(cudaStreamSynchronize(c.s));
-        const double beta = hs[101];
+        const double beta = hs[301];
         if (!std::isfinite(beta)) { set_error("FGMRES residual is not finite"); return TOPO_ERR_NAN; }
         if (beta <= ttol) { conv = true; break; }
-        k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, out + 62, c.V.p, 1), note_launch();
+        k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, out_beta, c.V.p, 1), note_launch();
         const int jmax = std::min(m, maxit - its);
         int kdone = jmax;
         bool stop = false;
@@ -291,7 +306,10 @@ int fem_solve(Ctx& c, const double* xphys, double* u) {
     for (int k = 0; k < c.ncases; k++) {
         double* uk = u + (size_t)k * n;
         const double* fk = c.F.p + (size_t)k * n;
-        TCK(cudaMemsetAsync(uk, 0, sizeof(double) * n, c.s));
+        // AssembleFem zeroes U (SolveFem.cpp:333); the optional warm start keeps
+        // the previous solution of this context as the initial guess
+        if (!(c.p.fem_warm_start && c.u_valid && uk == c.U.p + (size_t)k * n))
+            TCK(cudaMemsetAsync(uk, 0, sizeof(double) * n, c.s));
         int its = 0, st = 0;
         TRET(fgmres(c, fk, uk, &its, &st));
         its_total += its;
@@ -307,6 +325,7 @@ int fem_solve(Ctx& c, const double* xphys, double* u) {
         rel_worst = std::max(rel_worst, rel);
         if (c.p.verbose) printf("Norm of error %e, Iterations %d\n", rel, its);
     }
+    c.u_valid = (u == c.U.p);
     c.info.fem_its = its_total;
     c.info.fem_relres = rel_worst;
     c.info.fem_status = worst;
