@@ -152,6 +152,28 @@ int topo_fem_displacement(topo_ctx* ctx, double* u_d);
  * stress Emax*D*B*u relaxed by sqrt(x); uses the last displacement. */
 int topo_fem_von_mises(topo_ctx* ctx, const double* xphys_d, double* vms_d);
 
+/* No counterpart in the reference.  The compliance and sensitivity reduction
+ * of ComputeObjectiveAndSensitivities for a displacement the caller already
+ * has, for callers that cannot allocate device memory when they need it
+ * (stream-ordered pipelines that must not synchronise the device, hosts that
+ * allocate only through their own pool, drivers that forbid allocation after
+ * start-up).  It allocates nothing: the caller passes every input and output
+ * (device pointers) and the only scratch is a fixed array inside the library
+ * (about 130 KB per GPU, held until the process exits).
+ *   element_d  n_elems*nen node ids;  ke_d  n_elems * npk packed upper
+ *   triangle (row-major, i <= j) of each E = 1 element matrix, npk = 300
+ *   (hex8) or 78 (tet4), DOF order [x0..,y0..,z0..];  u_d  3*n_nodes.
+ *   Outputs dfdx_d, dgdx_d (n_elems) and fx_gx_d[0] = fx,
+ *   fx_gx_d[1] = sum x vol / TV - volfrac, written in stream order.
+ * Limit: n_elems <= 1,048,576 (larger meshes are rejected with TOPO_ERR_ARG).
+ * The first call on a device looks up the scratch array's device address;
+ * make that first call before capturing a stream into a CUDA graph.  All
+ * calls share the scratch: calls whose work overlaps on the GPU race. */
+int topo_fem_sensitivities_noalloc(int nen, int n_elems, const int32_t* element_d, const double* ke_d,
+                                   const double* xphys_d, const double* vol_d, const double* u_d, double Emin,
+                                   double Emax, double penal, double total_volume, double volfrac, double* dfdx_d,
+                                   double* dgdx_d, double* fx_gx_d, void* stream);
+
 /* ---------------------------------------------------------------- PDEFilter */
 /* PDEFilter::Filter (PDEFilter.cpp:142-165): xf = clamp(TFX' KF^-1 TF x, Xmin, 1);
  * the CG warm-starts from the previous solve's RX (PDEFilter.cpp:127). */

@@ -100,6 +100,8 @@ _SIGS = {
     "topo_opt_step": ([C.c_void_p, C.POINTER(C.c_int), _dp, _dp, _dp], C.c_int),
     "topo_opt_run": ([C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)], C.c_int),
     "topo_opt_step_host": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _dp], C.c_int),
+    "topo_fem_sensitivities_noalloc": ([C.c_int, C.c_int] + [C.c_void_p] * 5 + [C.c_double] * 5 +
+                                       [C.c_void_p] * 4, C.c_int),
     "topo_estimate_job_bytes": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_size_t),
     "topo_server_create": ([C.c_size_t, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "topo_server_destroy": ([C.c_void_p], C.c_int),
