@@ -212,6 +212,49 @@ def run_e2e(ctx, T, torch, steps, warmup, stream, dist=None):
     return e0.elapsed_time(e1), ne * 8, 2 * ne * 8 + 72
 
 
+def run_multiload(T, torch, steps, warmup, stream, forms=("block_mixed", "block_fp64", "one_by_one_mixed")):
+    """The batched multi-load configuration: hex8 100 x 50 x 50 (250,000
+    elements, 788,103 DOF) with k = 8 unit point loads at seeded random nodes
+    of the x = L face (random directions), compliance summed over the cases.
+    The block form (one lockstep FGMRES over the 8 cases, tensor-core block
+    operator, block V-cycle) against solving the cases one by one, both
+    mixed precision, plus the block form in FP64."""
+    import numpy as np
+    nx, ny, nz, k = 100, 50, 50, 8
+    v, e, f, _, _ = T.gen_cantilever(nx, ny, nz, 8)
+    ld, lv = T.gen_multiload(nx, ny, nz, k)
+    cp = np.arange(0, 3 * k + 1, 3, dtype=np.int32)
+    out = {"workload": f"hex8 {nx}x{ny}x{nz} ({e.shape[0]} elements), k={k} load cases", "steps": steps,
+           "warmup": warmup}
+    for name, kw in (("block_mixed", dict(fem_block=1, precision=T.PREC_MIXED)),
+                     ("block_fp64", dict(fem_block=1, precision=T.PREC_FP64)),
+                     ("one_by_one_mixed", dict(fem_block=0, precision=T.PREC_MIXED))):
+        if name not in forms:
+            continue
+        ctx = T.Context(v, e, f, ld, lv, case_ptr=cp, **dict(PARAMS, **kw))
+        ms, launches, prof, its = run_device(ctx, T, torch, steps, warmup, stream, None, profile=(name == "block_mixed"))
+        rec = {"value": steps / (ms / 1e3), "ms_per_step": ms / steps, "fgmres_its": its, "gpu_launches": launches}
+        if name == "block_mixed":
+            n_kmv, t_kmv = prof.get("kmv", (0, 0.0))
+            if n_kmv:
+                ne, nn, kb = e.shape[0], v.shape[0], 8
+                b = ne * (300 * 8 + 4 + 32 + 16 + 4 + 8) + nn * 3 * kb * 8 * 2
+                fl = ne * 2.0 * 24 * 24 * kb
+                avg = t_kmv / n_kmv * 1e-3
+                peak, kind = peaks()
+                rec["block_operator"] = {"kernel": "k_blk_kmv<8,8> (DMMA m8n8k4 FP64, TMA bulk Ke staging)",
+                                         "launches": n_kmv, "avg_us": avg * 1e6, "algorithmic_bytes": b,
+                                         "gbs": b / avg / 1e9, "frac_hbm": b / avg / 1e9 / peak,
+                                         "tflops_fp64": fl / avg / 1e12, "peak_kind": kind}
+        out[name] = rec
+        ctx.close()
+    if "block_mixed" in out and "one_by_one_mixed" in out:
+        out["block_over_one_by_one"] = out["block_mixed"]["value"] / out["one_by_one_mixed"]["value"]
+    if "block_mixed" in out and "block_fp64" in out:
+        out["mixed_over_fp64_block"] = out["block_mixed"]["value"] / out["block_fp64"]["value"]
+    return out
+
+
 def run_serving(T, n_jobs, seed=7, rate=4.0, iters=30):
     """Serving stream: Poisson arrivals (mean `rate` jobs/s, seeded) of hex8 /
     tet4 cantilever jobs, sizes log-uniform in [20k, 1.2M] elements, volfrac
@@ -267,8 +310,11 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving stream (p50/p99 latency)")
     ap.add_argument("--serve-jobs", type=int, default=12)
-    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
-                    help="time one precision only (used for short profiling runs)")
+    ap.add_argument("--only", choices=["mixed", "fp64", "multiload"], default=None,
+                    help="time one form only (used for short profiling runs)")
+    ap.add_argument("--no-multiload", action="store_true", help="skip the k=8 multi-load configuration")
+    ap.add_argument("--multiload-steps", type=int, default=6)
+    ap.add_argument("--multiload-forms", default="block_mixed,block_fp64,one_by_one_mixed")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", "0"))
@@ -307,6 +353,12 @@ def main():
         dist = dist_mod
     T = _pkg()
     stream = torch.cuda.current_stream()
+    if args.only == "multiload":
+        if rank == 0:
+            print(json.dumps({"only": "multiload",
+                              **run_multiload(T, torch, args.multiload_steps, min(args.warmup, 3), stream,
+                                              args.multiload_forms.split(","))}), flush=True)
+        return
     v, e, f, ld, lv = T.gen_cantilever(wl["nx"], wl["ny"], wl["nz"], wl["nen"])
     t0 = time.perf_counter()
     ctx = T.Context(v, e, f, ld, lv, precision=T.PREC_MIXED, **PARAMS)
@@ -376,6 +428,9 @@ def main():
                 "frac": dom["gbs"] / peak, "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": dom["bytes"], "avg_launch_us": dom["avg_us"]}
 
+    multi = None
+    if not args.no_multiload and rank == 0 and world == 1:
+        multi = run_multiload(T, torch, args.multiload_steps, 3, stream)
     serve = None
     if not args.no_serve:
         serve = run_serving(T, args.serve_jobs, seed=7)
@@ -406,7 +461,7 @@ def main():
             "amg_dofs": list(info.amg_dofs)[:info.amg_levels],
             "e2e": {"value": e2e_val, "unit": "design iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "kernels": kern, "clocks": clocks,
-            "cpu_baseline": cpu, "serve": serve}
+            "cpu_baseline": cpu, "multiload": multi, "serve": serve}
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -75,6 +75,8 @@ typedef struct topo_params {
     double cheb_safety;    /* Chebyshev interval [0.1, 1.1] * cheb_safety * rho */
     int fem_warm_start;    /* 1: start FGMRES from the previous U instead of 0 (the
                               reference zeroes U, SolveFem.cpp:333); same stopping rule */
+    int fem_block;         /* n_cases > 1: 1 (default) solves all load cases at once with the
+                              block operator and block V-cycle, 0 solves them one by one */
 } topo_params;
 
 typedef struct topo_solve_info {
@@ -137,6 +139,10 @@ int topo_fem_element_matrix(topo_ctx* ctx, int e, double* ke);
 /* y = K(xphys) u with Dirichlet rows/columns as identity
  * (AssembleFem + MatZeroRowsColumns + MatMult, SolveFem.cpp:267-337). */
 int topo_fem_apply(topo_ctx* ctx, const double* xphys_d, const double* u_d, double* y_d);
+/* The same for all n_cases load cases at once through the block operator
+ * (tensor-core Ke [u_1..u_k] per element): u_d, y_d are [n_cases][3*n_nodes].
+ * No counterpart in the reference (its load cases are solved one by one). */
+int topo_fem_apply_block(topo_ctx* ctx, const double* xphys_d, const double* u_d, double* y_d);
 /* SolveFem::ComputeObjectiveAndSensitivities (SolveFem.h:39-40,
  * SolveFem.cpp:159-265): solves K U = F, then fx = sum E_e u_e'Ke u_e,
  * dfdx, gx[0] = sum x vol / TV - volfrac, dgdx[0] = vol / TV.

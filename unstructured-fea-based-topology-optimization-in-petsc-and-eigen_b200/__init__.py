@@ -39,7 +39,8 @@ class Params(C.Structure):
         ("cheb_degree", C.c_int), ("fine_smoother_matfree", C.c_int),
         ("filter_rtol", C.c_double), ("filter_atol", C.c_double), ("filter_dtol", C.c_double),
         ("filter_maxit", C.c_int), ("verbose", C.c_int), ("amg_rho_its", C.c_int), ("cheb_safety", C.c_double),
-        ("fem_warm_start", C.c_int)]
+        ("fem_warm_start", C.c_int),
+        ("fem_block", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -76,6 +77,7 @@ _SIGS = {
     "topo_fem_volumes": ([C.c_void_p, C.c_void_p, _dp], C.c_int),
     "topo_fem_element_matrix": ([C.c_void_p, C.c_int, C.c_void_p], C.c_int),
     "topo_fem_apply": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "topo_fem_apply_block": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "topo_fem_obj_sens": ([C.c_void_p, C.c_void_p, _dp, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "topo_fem_solve": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "topo_fem_displacement": ([C.c_void_p, C.c_void_p], C.c_int),
@@ -324,6 +326,12 @@ class Context:
     def fem_apply(self, xphys, u):
         y = self.zeros(self.ndof)
         _check(lib().topo_fem_apply(self.h, _dptr(xphys), _dptr(u), _dptr(y)), "fem_apply")
+        return y
+
+    def fem_apply_block(self, xphys, u):
+        """K(xphys) applied to every load case at once; u is [n_cases][ndof]."""
+        y = self.zeros(self.ncases * self.ndof)
+        _check(lib().topo_fem_apply_block(self.h, _dptr(xphys), _dptr(u), _dptr(y)), "fem_apply_block")
         return y
 
     def fem_obj_sens(self, xphys):

@@ -278,6 +278,7 @@ void topo_params_default(topo_params* p) {
     p->amg_rho_its = 10;
     p->cheb_safety = 1.0;
     p->fem_warm_start = 0;
+    p->fem_block = 1;
 }
 
 int topo_device_alloc(size_t bytes, void** ptr) {
@@ -463,6 +464,25 @@ int topo_fem_apply(topo_ctx* ctx, const double* xphys_d, const double* u_d, doub
     TRET(compute_moduli(c, xphys_d));
     TRET(kmatvec(c, c.Ee64.p, u_d, y_d));
     TCK(cudaStreamSynchronize(c.s));
+    return 0;
+    GUARD_END
+}
+
+int topo_fem_apply_block(topo_ctx* ctx, const double* xphys_d, const double* u_d, double* y_d) {
+    if (!ctx || !xphys_d || !u_d || !y_d) { set_error("null argument"); return TOPO_ERR_ARG; }
+    GUARD_BEGIN
+    Ctx& c = ctx->c;
+    TRET(compute_moduli(c, xphys_d));
+    TRET(blk_setup(c));
+    const size_t nf = (size_t)c.ndof * c.blk.kb;
+    DBuf<double> ub, yb;
+    TRET(ub.alloc(nf));
+    TRET(yb.alloc(nf));
+    TRET(blk_interleave(c, u_d, ub.p));
+    TRET(blk_apply(c, ub.p, yb.p, nullptr, 1.0));
+    TRET(blk_deinterleave(c, yb.p, y_d));
+    TCK(cudaStreamSynchronize(c.s));
+    TRET(blk_check_error(c));
     return 0;
     GUARD_END
 }

@@ -866,7 +866,7 @@ static int numeric(Ctx& c) {
 }
 
 // Chebyshev recurrence numbers for sigma = theta/delta = 1.2
-static void cheb_coeffs(int deg, double* cr, double* cq) {
+void cheb_coeffs(int deg, double* cr, double* cq) {
     const double sigma = 1.2;
     double rho_prev = 1.0 / sigma;
     for (int k = 1; k < deg; k++) {

@@ -85,6 +85,39 @@ struct AmgVals {
     bool allocated = false;
 };
 
+// block (KB right-hand sides) work vectors of the V-cycle
+template <class T>
+struct AmgBlkVecs {
+    DBuf<T> x[kMaxLevels], b[kMaxLevels], r[kMaxLevels], d[kMaxLevels], d2[kMaxLevels], t[kMaxLevels];
+    int kb = 0, nlev = 0;
+};
+
+// k-load block operator and solver state (block.cu, block_solve.cu)
+struct BlockState {
+    bool ready = false;
+    int kb = 0;                 // case width of block vectors (4, 8 or 16)
+    int nchunks = 0, nphases = 0, max_nodes = 0, max_phases = 0, node_cap = 0;
+    DBuf<int> ch_ph, ph_sl, ch_np, ch_nodes;  // chunk -> phases, phase -> slots, chunk -> nodes
+    DBuf<int> sl_elem, sl_gn;   // slot -> element, slot -> global nodes
+    DBuf<uint16_t> sl_lc;       // slot -> chunk-local nodes
+    DBuf<uint32_t> sl_mask;     // slot -> fixed local DOFs
+    DBuf<double> keb;           // slot -> packed Ke (E = 1)
+    DBuf<double> Es;            // slot -> SIMP modulus of the current design
+    int es_gen = -1;            // moduli generation Es was gathered from
+    DBuf<int> err;              // set when a bounded wait expired
+    // block FGMRES
+    DBuf<double> F, U;          // loads and solutions, [dof][KB]
+    DBuf<double> V, w, Z64;     // basis (m+1 block vectors), work, FP64 directions
+    DBuf<float> Z32;            // FP32 directions (mixed form)
+    DBuf<double> st;            // per-case Arnoldi states + scratch
+    DBuf<int> ik;               // per-case active flags and column counts
+    PinnedScalars hs;           // host mirror of the per-iteration outputs
+    bool u_valid = false;       // U holds this run's previous block solution
+    bool u_fresh = false;       // U belongs to the last displacement solve
+    AmgBlkVecs<float> bv32;     // V-cycle work vectors, [dof][KB] per level
+    AmgBlkVecs<double> bv64;
+};
+
 struct Ctx {
     topo_params p{};
     cudaStream_t s = nullptr;
@@ -129,6 +162,7 @@ struct Ctx {
 
     // ---- displacement solve
     DBuf<double> Ee64;          // SIMP moduli of the current xphys
+    int moduli_gen = 0;         // bumped whenever Ee64/Ee32 are recomputed
     DBuf<float> Ee32;
     DBuf<double> U;             // [ncases][ndof]
     DBuf<double> uku;           // per-element u'Ke u summed over cases
@@ -157,6 +191,8 @@ struct Ctx {
     double ch = 1.0, beta_proj = 1.0, beta_tmp = 1.0;
     bool opt_ready = false;
     bool u_valid = false;       // U holds a solution of this optimisation run
+
+    BlockState blk;
 
     topo_solve_info info{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -211,6 +247,15 @@ int filter_kf(Ctx& c, const double* r, double* y);
 int filter_tfxT(Ctx& c, const double* rx, double* xf, bool clamp, double xmin);
 int von_mises(Ctx& c, const double* xphys, double* vms);
 
+int blk_width(int ncases);                                         // block.cu
+int blk_setup(Ctx& c);
+int blk_apply(Ctx& c, const double* u, double* y, const double* b, double alpha);
+int blk_apply_f32in(Ctx& c, const float* u, double* y, const double* b, double alpha);
+int blk_uku(Ctx& c, const double* u, double* uku);
+int blk_interleave(Ctx& c, const double* src, double* dst);
+int blk_deinterleave(Ctx& c, const double* src, double* dst);
+int blk_check_error(Ctx& c);
+
 int amg_alloc(Ctx& c);                                             // amg.cu
 int amg_numeric(Ctx& c);
 int amg_reset_warm_start(Ctx& c);
@@ -220,6 +265,7 @@ int amg_vcycle64(Ctx& c, const double* b, double* x);
 int amg_vcycle32(Ctx& c, const double* b64, float* x);
 
 int fem_solve(Ctx& c, const double* xphys, double* u);             // solver.cu
+int fem_solve_block(Ctx& c, const double* xphys, double* u);       // block_solve.cu
 int filter_cg(Ctx& c, const double* b, double* x, int* its);
 int dev_dot(Ctx& c, const double* a, const double* b, long n, double* out_dev);
 int finalize_sum(Ctx& c, const double* partials, int nparts, int nv, double* out_dev);

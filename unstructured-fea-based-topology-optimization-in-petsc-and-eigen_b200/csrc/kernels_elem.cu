@@ -285,6 +285,7 @@ int compute_moduli(Ctx& c, const double* xphys) {
     if (!c.Ee64.p) { TRET(c.Ee64.alloc(npad)); TRET(c.Ee32.alloc(npad)); }
     k_moduli<<<grid_for(npad, 256, 1 << 20), 256, 0, c.s>>>(c.ne, npad, xphys, c.p.Emin, c.p.Emax, c.p.penal, c.Ee64.p,
                                                            c.Ee32.p), note_launch();
+    c.moduli_gen++;
     TCK(cudaGetLastError());
     return 0;
 }
@@ -540,7 +541,11 @@ int fem_sensitivities(Ctx& c, const double* xphys, double* dfdx, double* dgdx) {
     int block = 256, nb = (c.ne + block - 1) / block;
     if ((long)c.red.n < 2L * nb) TRET(c.red.alloc(std::max<long>(2L * nb, 4096)));
     if (!c.uku.p) TRET(c.uku.alloc(c.ne));
-    for (int cs = 0; cs < c.ncases; cs++) {
+    // the block solve leaves all cases in one case-interleaved vector: one
+    // tensor-core pass gives the uKu sum over the cases
+    const bool blk = c.ncases > 1 && c.p.fem_block && c.blk.u_fresh;
+    if (blk) TRET(blk_uku(c, c.blk.U.p, c.uku.p));
+    for (int cs = 0; cs < c.ncases && !blk; cs++) {
         const double* Uc = c.U.p + (size_t)cs * c.ndof;
         if (c.nen == 8) k_uku<8><<<(c.ne + 127) / 128, 128, 0, c.s>>>(c.ne, c.ndof, c.conn.p, c.ke64.p, Uc, c.uku.p, cs > 0), note_launch();
         else k_uku<4><<<(c.ne + 127) / 128, 128, 0, c.s>>>(c.ne, c.ndof, c.conn.p, c.ke64.p, Uc, c.uku.p, cs > 0), note_launch();

@@ -60,7 +60,10 @@ __global__ void __launch_bounds__(256) k_mdot(long n, int nv, const double* __re
     double acc[NV];
 #pragma unroll
     for (int j = 0; j < NV; j++) acc[j] = 0.0;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    // each block sweeps one contiguous stretch of every basis vector
+    const long len = ((n + gridDim.x - 1) / gridDim.x + 255) / 256 * 256;
+    const long i1 = min(n, (blockIdx.x + 1) * len);
+    for (long i = blockIdx.x * len + threadIdx.x; i < i1; i += blockDim.x) {
         const double wi = w[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
@@ -80,7 +83,9 @@ __global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __re
     if (threadIdx.x < nv) hs[threadIdx.x] = h[threadIdx.x];
     __syncthreads();
     double v[1] = {0.0};
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const long len = ((n + gridDim.x - 1) / gridDim.x + 255) / 256 * 256;
+    const long i1 = min(n, (blockIdx.x + 1) * len);
+    for (long i = blockIdx.x * len + threadIdx.x; i < i1; i += blockDim.x) {
         double wi = w[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
@@ -298,6 +303,8 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
 // SolveFem::ComputeFem (SolveFem.cpp:91-157): moduli, AMG numeric setup,
 // U = 0, FGMRES, then the true relative residual.
 int fem_solve(Ctx& c, const double* xphys, double* u) {
+    if (c.ncases > 1 && c.p.fem_block) return fem_solve_block(c, xphys, u);
+    c.blk.u_valid = c.blk.u_fresh = false;
     TRET(compute_moduli(c, xphys));
     TRET(amg_numeric(c));
     const long n = c.ndof;
