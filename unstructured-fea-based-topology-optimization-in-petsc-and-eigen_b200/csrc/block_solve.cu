@@ -403,8 +403,7 @@ static int precond_blk(Ctx& c, const double* v, int j) {
 // ----------------------------------------------------------------- block Krylov kernels
 // Per-case reductions over a block vector of n*KB entries: a thread keeps
 // one case (its stride is a multiple of KB), lanes of equal case combine by
-// xor shuffles of offsets >= KB, warps through shared memory.  Each block
-// sweeps one contiguous stretch of every vector.
+// xor shuffles of offsets >= KB, warps through shared memory.
 template <int KB>
 __device__ __forceinline__ double case_warp_sum(double v) {
 #pragma unroll
@@ -420,9 +419,7 @@ __global__ void __launch_bounds__(256) k_mdot_blk(long nf, int nv, const double*
     double acc[NV];
 #pragma unroll
     for (int j = 0; j < NV; j++) acc[j] = 0.0;
-    const long len = ((nf + gridDim.x - 1) / gridDim.x + 255) / 256 * 256;
-    const long i1 = min(nf, (blockIdx.x + 1) * len);
-    for (long i = blockIdx.x * len + threadIdx.x; i < i1; i += blockDim.x) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nf; i += (long)gridDim.x * blockDim.x) {
         const double wi = w[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
@@ -452,9 +449,7 @@ __global__ void __launch_bounds__(256) k_orth_blk(long nf, int nv, const double*
     __syncthreads();
     const int cs = threadIdx.x % KB;
     double nrm = 0.0;
-    const long len = ((nf + gridDim.x - 1) / gridDim.x + 255) / 256 * 256;
-    const long i1 = min(nf, (blockIdx.x + 1) * len);
-    for (long i = blockIdx.x * len + threadIdx.x; i < i1; i += blockDim.x) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nf; i += (long)gridDim.x * blockDim.x) {
         double wi = w[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)

@@ -60,10 +60,7 @@ __global__ void __launch_bounds__(256) k_mdot(long n, int nv, const double* __re
     double acc[NV];
 #pragma unroll
     for (int j = 0; j < NV; j++) acc[j] = 0.0;
-    // each block sweeps one contiguous stretch of every basis vector
-    const long len = ((n + gridDim.x - 1) / gridDim.x + 255) / 256 * 256;
-    const long i1 = min(n, (blockIdx.x + 1) * len);
-    for (long i = blockIdx.x * len + threadIdx.x; i < i1; i += blockDim.x) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         const double wi = w[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
@@ -83,9 +80,7 @@ __global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __re
     if (threadIdx.x < nv) hs[threadIdx.x] = h[threadIdx.x];
     __syncthreads();
     double v[1] = {0.0};
-    const long len = ((n + gridDim.x - 1) / gridDim.x + 255) / 256 * 256;
-    const long i1 = min(n, (blockIdx.x + 1) * len);
-    for (long i = blockIdx.x * len + threadIdx.x; i < i1; i += blockDim.x) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         double wi = w[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
