@@ -77,6 +77,8 @@ typedef struct topo_params {
                               reference zeroes U, SolveFem.cpp:333); same stopping rule */
     int fem_block;         /* n_cases > 1: 1 (default) solves all load cases at once with the
                               block operator and block V-cycle, 0 solves them one by one */
+    int fem_graphs;        /* 1 (default): replay each FGMRES Arnoldi step from a CUDA graph
+                              captured in an earlier solve with the same buffers */
 } topo_params;
 
 typedef struct topo_solve_info {

@@ -97,3 +97,17 @@ def test_host_buffer_step_matches_device_step(T, cuda, mesh):
     assert rel(xp, a.opt_tensor(1).cpu().numpy()) < 1e-9
     a.close()
     b.close()
+
+
+def test_graph_replayed_steps_match_direct_launches(T, cuda, mesh):
+    """Arnoldi steps replayed from captured CUDA graphs (from the second
+    solve on) give the same design trajectory as launching every kernel."""
+    v, e, f, ld, lv = mesh
+    h = {}
+    for g in (1, 0):
+        ctx = T.Context(v, e, f, ld, lv, precision=T.PREC_MIXED, fem_graphs=g, **KW)
+        ctx.opt_init()
+        h[g] = ctx.opt_run(8)
+        ctx.close()
+    assert rel(h[1][:, 0], h[0][:, 0]) < 1e-6
+    assert np.abs(h[1][:, 1] - h[0][:, 1]).max() < 1e-8

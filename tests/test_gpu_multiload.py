@@ -115,3 +115,16 @@ def test_block_design_loop(T, cuda):
         ctx.close()
     assert rel(hist[0][:, 0], hist[1][:, 0]) < 1e-4
     assert np.abs(hist[0][:, 1] - hist[1][:, 1]).max() < 1e-4
+
+
+def test_block_graph_replay_matches_direct(T, cuda):
+    """The block FGMRES steps replayed from CUDA graphs reproduce the directly
+    launched design trajectory."""
+    v, e, f, ld, lv, cp = mesh(T, 8, 8)
+    hist = []
+    for g in (1, 0):
+        ctx = T.Context(v, e, f, ld, lv, case_ptr=cp, fem_graphs=g, precision=T.PREC_MIXED, ch_tol=0.0, **KW)
+        ctx.opt_init()
+        hist.append(ctx.opt_run(6))
+        ctx.close()
+    assert rel(hist[0][:, 0], hist[1][:, 0]) < 1e-6

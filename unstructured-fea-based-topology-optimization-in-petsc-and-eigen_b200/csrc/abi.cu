@@ -279,6 +279,7 @@ void topo_params_default(topo_params* p) {
     p->cheb_safety = 1.0;
     p->fem_warm_start = 0;
     p->fem_block = 1;
+    p->fem_graphs = 1;
 }
 
 int topo_device_alloc(size_t bytes, void** ptr) {

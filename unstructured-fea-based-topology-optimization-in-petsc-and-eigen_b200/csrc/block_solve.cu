@@ -650,6 +650,34 @@ static int norms_blk(Ctx& c, const double* w, double* out) {
     return 0;
 }
 
+// Arnoldi step j for all cases (see the single-load step in solver.cu)
+struct BlkStepArgs {
+    int j;
+    long nf;
+    GmL GL;
+    double *hcol, *st, *ttol_d, *out, *hs;
+    int *act, *kd;
+};
+template <int KB>
+static int arnoldi_step_blk(Ctx& c, void* p) {
+    const BlkStepArgs& a = *static_cast<const BlkStepArgs*>(p);
+    BlockState& B = c.blk;
+    const int j = a.j;
+    const long nf = a.nf;
+    const double* vj = B.V.p + (size_t)j * nf;
+    TRET(precond_blk(c, vj, j));
+    if (c.p.precision == TOPO_PREC_MIXED) TRET(blk_apply_f32in(c, B.Z32.p + (size_t)j * nf, B.w.p, nullptr, 1.0));
+    else TRET(blk_apply(c, B.Z64.p + (size_t)j * nf, B.w.p, nullptr, 1.0));
+    TRET(mdot_blk<KB>(c, j + 1, B.V.p, nf, B.w.p, a.hcol));
+    TRET(orth_blk<KB>(c, j + 1, B.V.p, nf, a.hcol, B.w.p, a.hcol + (size_t)(j + 1) * KB));
+    k_scale_blk<KB><<<grid_for(nf, 256), 256, 0, c.s>>>(nf, B.w.p, a.hcol + (size_t)(j + 1) * KB, a.act,
+                                                      B.V.p + (size_t)(j + 1) * nf), note_launch();
+    k_gm_givens_blk<<<1, 32, 0, c.s>>>(a.GL, KB, j, a.hcol, a.st, a.ttol_d, a.act, a.kd, a.out + 2 * j), note_launch();
+    TCK(cudaMemcpyAsync(a.hs + 2 * j, a.out + 2 * j, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    TCK(cudaGetLastError());
+    return 0;
+}
+
 template <int KB>
 static int fgmres_blk(Ctx& c, const double* b, double* x, int* its_out, int* status) {
     BlockState& B = c.blk;
@@ -685,6 +713,28 @@ static int fgmres_blk(Ctx& c, const double* b, double* x, int* its_out, int* sta
     int* act = B.ik.p;
     int* kd = B.ik.p + KB;
     double* hs = B.hs.h;
+    // the V-cycle work vectors and the slot moduli exist before any capture
+    // (a captured step must not depend on host-side state that changes)
+    if (mixed) TRET(alloc_bvecs<float>(c));
+    else TRET(alloc_bvecs<double>(c));
+    TRET(blk_setup(c));
+    // buffers and options the Arnoldi-step graphs depend on
+    uint64_t sig = 0x2b1c0ffeeull;
+    for (uint64_t v : {(uint64_t)(uintptr_t)B.V.p, (uint64_t)(uintptr_t)B.Z32.p, (uint64_t)(uintptr_t)B.Z64.p,
+                       (uint64_t)(uintptr_t)B.w.p, (uint64_t)(uintptr_t)B.st.p, (uint64_t)(uintptr_t)B.ik.p,
+                       (uint64_t)(uintptr_t)B.hs.h, (uint64_t)(uintptr_t)c.red.p, (uint64_t)(uintptr_t)B.Es.p,
+                       (uint64_t)(uintptr_t)B.bv32.x[0].p, (uint64_t)(uintptr_t)B.bv64.x[0].p,
+                       (uint64_t)(uintptr_t)c.v32.A0s.p, (uint64_t)(uintptr_t)c.v64.A0s.p,
+                       (uint64_t)(uintptr_t)c.cinv.p, (uint64_t)(uintptr_t)c.rho.p, (uint64_t)c.p.precision,
+                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)KB, (uint64_t)nf})
+        sig = sig_mix(sig, v);
+    StepGraphs& G = B.graphs;
+    if (G.sig != sig) {
+        G.drop();
+        G.sig = sig;
+    }
+    const bool capture_ok = c.p.fem_graphs && G.seen == sig;
+    G.seen = sig;
     // ||b_c|| -> stopping thresholds max(rtol ||b_c||, 1e-50)
     TRET(norms_blk<KB>(c, b, beta_d));
     TCK(cudaMemcpyAsync(hs, beta_d, KB * sizeof(double), cudaMemcpyDeviceToHost, c.s));
@@ -711,16 +761,8 @@ static int fgmres_blk(Ctx& c, const double* b, double* x, int* its_out, int* sta
         bool stop = false;
         for (int j = 0; j <= jmax && !stop; j++) {
             if (j < jmax) {
-                const double* vj = B.V.p + (size_t)j * nf;
-                TRET(precond_blk(c, vj, j));
-                if (mixed) TRET(blk_apply_f32in(c, B.Z32.p + (size_t)j * nf, B.w.p, nullptr, 1.0));
-                else TRET(blk_apply(c, B.Z64.p + (size_t)j * nf, B.w.p, nullptr, 1.0));
-                TRET(mdot_blk<KB>(c, j + 1, B.V.p, nf, B.w.p, hcol));
-                TRET(orth_blk<KB>(c, j + 1, B.V.p, nf, hcol, B.w.p, hcol + (size_t)(j + 1) * KB));
-                k_scale_blk<KB><<<grid_for(nf, 256), 256, 0, c.s>>>(nf, B.w.p, hcol + (size_t)(j + 1) * KB, act,
-                                                                  B.V.p + (size_t)(j + 1) * nf), note_launch();
-                k_gm_givens_blk<<<1, 32, 0, c.s>>>(GL, KB, j, hcol, st, ttol_d, act, kd, out + 2 * j), note_launch();
-                TCK(cudaMemcpyAsync(hs + 2 * j, out + 2 * j, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+                BlkStepArgs sa{j, nf, GL, hcol, st, ttol_d, out, hs, act, kd};
+                TRET(step_graph_run(c, G, j, capture_ok, arnoldi_step_blk<KB>, &sa));
                 TCK(cudaEventRecord(c.gm_ev[j], c.s));
             }
             if (j == 0) continue;

@@ -85,6 +85,31 @@ struct AmgVals {
     bool allocated = false;
 };
 
+// CUDA graphs of the Arnoldi steps of one FGMRES form: step j (V-cycle,
+// operator, Gram-Schmidt, Givens, residual read-back) is captured once and
+// replayed in every later solve with the same buffers.  `sig` identifies the
+// buffers and options the graphs were captured with; any change drops them.
+struct StepGraphs {
+    std::vector<cudaGraphExec_t> exec;
+    std::vector<long> launches;      // kernels per replay (for the launch counter)
+    uint64_t sig = 0;
+    uint64_t seen = 0;               // signature of the previous solve (capture from the second on)
+    cudaStream_t cap = nullptr;      // private capture stream (the context's may be the legacy one)
+    bool disabled = false;           // capture failed once: direct launches from then on
+    void drop() {
+        for (auto e : exec)
+            if (e) cudaGraphExecDestroy(e);
+        exec.clear();
+        launches.clear();
+    }
+    ~StepGraphs() {
+        drop();
+        if (cap) cudaStreamDestroy(cap);
+    }
+};
+int step_graph_run(struct Ctx& c, StepGraphs& G, int j, bool capture_ok, int (*body)(struct Ctx&, void*), void* arg);
+uint64_t sig_mix(uint64_t h, uint64_t v);
+
 // block (KB right-hand sides) work vectors of the V-cycle
 template <class T>
 struct AmgBlkVecs {
@@ -116,6 +141,7 @@ struct BlockState {
     bool u_fresh = false;       // U belongs to the last displacement solve
     AmgBlkVecs<float> bv32;     // V-cycle work vectors, [dof][KB] per level
     AmgBlkVecs<double> bv64;
+    StepGraphs graphs;          // captured Arnoldi steps of the block FGMRES
 };
 
 struct Ctx {
@@ -171,6 +197,7 @@ struct Ctx {
     DBuf<float> Z32;            // (mixed form)
     DBuf<double> w, wtmp;       // wtmp: device Arnoldi state + per-iteration outputs
     std::vector<cudaEvent_t> gm_ev;  // one per Arnoldi step (pipelined residual checks)
+    StepGraphs graphs;          // captured Arnoldi steps of the single-load FGMRES
     DBuf<double> red;           // reduction partials
     DBuf<double> dsc;           // device scalars
     PinnedScalars hsc;          // pinned host mirror for readbacks
