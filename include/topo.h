@@ -79,6 +79,7 @@ typedef struct topo_params {
                               block operator and block V-cycle, 0 solves them one by one */
     int fem_graphs;        /* 1 (default): replay each FGMRES Arnoldi step from a CUDA graph
                               captured in an earlier solve with the same buffers */
+    int cheb_degree_post;  /* post-smoothing Chebyshev degree (0: same as cheb_degree) */
 } topo_params;
 
 typedef struct topo_solve_info {

@@ -41,7 +41,8 @@ class Params(C.Structure):
         ("filter_maxit", C.c_int), ("verbose", C.c_int), ("amg_rho_its", C.c_int), ("cheb_safety", C.c_double),
         ("fem_warm_start", C.c_int),
         ("fem_block", C.c_int),
-        ("fem_graphs", C.c_int)]
+        ("fem_graphs", C.c_int),
+        ("cheb_degree_post", C.c_int)]
 
 
 class SolveInfo(C.Structure):

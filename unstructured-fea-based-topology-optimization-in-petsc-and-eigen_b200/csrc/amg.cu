@@ -882,7 +882,8 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
     AmgVals<T>& v = vals<T>(c);
     AmgDevLevel& D = c.dl[l];
     const long n = D.ndof;
-    const int deg = std::max(1, c.p.cheb_degree);
+    // pre-smoothing (zero initial guess) and post-smoothing degrees
+    const int deg = std::max(1, (!zero_init && c.p.cheb_degree_post > 0) ? c.p.cheb_degree_post : c.p.cheb_degree);
     double cr[16] = {0}, cq[16] = {0};
     cheb_coeffs(std::min(deg, 16), cr, cq);
     const double* rho = c.rho.p + 2 * kMaxLevels + l;  // safety-scaled spectral bound
@@ -940,6 +941,7 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
     for (int l = 0; l <= L; l++) { bl[l] = v.b[l].p; xl[l] = v.x[l].p; }
     bl[0] = b0;
     xl[0] = x0;
+    cudaEvent_t ecoarse = nullptr;
     for (int l = 0; l < L; l++) {
         AmgDevLevel& D = c.dl[l];
         TRET(smooth<T>(c, l, bl[l], xl[l], true));
@@ -951,6 +953,7 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
         }
         if (D.bs == 3) TRET((spmv<T, 6, 3>(c, D.R, v.R[l].p, v.t[l].p, v.b[l + 1].p, nullptr, 0)));
         else TRET((spmv<T, 6, 6>(c, D.R, v.R[l].p, v.t[l].p, v.b[l + 1].p, nullptr, 0)));
+        if (l == 0) prof_begin(c, PS_VC_COARSE, &ecoarse);
     }
     {
         const int n = c.dl[L].ndof;
@@ -959,6 +962,7 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
     }
     for (int l = L - 1; l >= 0; l--) {
         AmgDevLevel& D = c.dl[l];
+        if (l == 0) prof_end(c, PS_VC_COARSE, ecoarse);
         if (D.bs == 3) TRET((spmv<T, 3, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 2)));
         else TRET((spmv<T, 6, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 2)));
         TRET(smooth<T>(c, l, bl[l], xl[l], false));

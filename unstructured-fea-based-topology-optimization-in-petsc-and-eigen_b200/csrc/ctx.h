@@ -228,7 +228,7 @@ struct Ctx {
     struct Prof {
         bool on = false;
         std::vector<cudaEvent_t> pool;                 // free events
-        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rec[8];
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rec[12];
     } prof;
 };
 
@@ -239,7 +239,11 @@ enum ProfSlot {
     PS_SETUP_RHO = 5,     // power iterations
     PS_SETUP_GAL = 6,     // smoothing of P + Galerkin products + transposes
     PS_SETUP_COARSE = 7,  // coarsest dense inverse
-    PS_COUNT = 8
+    PS_VCYCLE = 8,        // whole preconditioner application
+    PS_VC_COARSE = 9,     // V-cycle below level 0 (from the level-0 restriction to the prolongation)
+    PS_ORTH = 10,         // Gram-Schmidt sweeps of one Arnoldi step
+    PS_SOLVE = 11,        // whole displacement solve (setup excluded)
+    PS_COUNT = 12
 };
 cudaEvent_t prof_event(Ctx& c);
 inline void prof_begin(Ctx& c, int slot, cudaEvent_t* e0) {

@@ -141,8 +141,12 @@ static int orth(Ctx& c, int nv, const double* V, long ld, const double* h, doubl
 
 static int precond_apply(Ctx& c, const double* v, int j) {
     const long n = c.ndof;
-    if (c.p.precision == TOPO_PREC_MIXED) return amg_vcycle32(c, v, c.Z32.p + (size_t)j * n);
-    return amg_vcycle64(c, v, c.Z64.p + (size_t)j * n);
+    cudaEvent_t e0;
+    prof_begin(c, PS_VCYCLE, &e0);
+    if (c.p.precision == TOPO_PREC_MIXED) TRET(amg_vcycle32(c, v, c.Z32.p + (size_t)j * n));
+    else TRET(amg_vcycle64(c, v, c.Z64.p + (size_t)j * n));
+    prof_end(c, PS_VCYCLE, e0);
+    return 0;
 }
 
 // ----------------------------------------------------------------- captured Arnoldi steps
@@ -271,8 +275,11 @@ static int arnoldi_step(Ctx& c, void* p) {
     TRET(precond_apply(c, vj, j));
     if (c.p.precision == TOPO_PREC_MIXED) TRET(kmatvec_f32in(c, c.Ee64.p, c.Z32.p + (size_t)j * n, c.w.p));
     else TRET(kmatvec(c, c.Ee64.p, c.Z64.p + (size_t)j * n, c.w.p));
+    cudaEvent_t e0;
+    prof_begin(c, PS_ORTH, &e0);
     TRET(mdot(c, j + 1, c.V.p, n, c.w.p, a.gm));
     TRET(orth(c, j + 1, c.V.p, n, a.gm, c.w.p, a.gm + j + 1));
+    prof_end(c, PS_ORTH, e0);
     k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, a.gm + j + 1, c.V.p + (size_t)(j + 1) * n, 1),
         note_launch();
     k_gm_givens<<<1, 32, 0, c.s>>>(a.GL, j, a.gm, a.st, a.out + 2 * j), note_launch();
@@ -320,7 +327,7 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
                        (uint64_t)(uintptr_t)c.dsc.p, (uint64_t)(uintptr_t)c.hsc.h, (uint64_t)(uintptr_t)c.Ee64.p,
                        (uint64_t)(uintptr_t)c.v32.A0s.p, (uint64_t)(uintptr_t)c.v64.A0s.p,
                        (uint64_t)(uintptr_t)c.cinv.p, (uint64_t)(uintptr_t)c.rho.p, (uint64_t)c.p.precision,
-                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.fine_smoother_matfree,
+                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.fine_smoother_matfree,
                        (uint64_t)n})
         sig = sig_mix(sig, v);
     StepGraphs& G = c.graphs;
@@ -337,6 +344,8 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
     const double ttol = std::max(c.p.fem_rtol * bnorm, 1e-50);
     int its = 0;
     bool conv = false;
+    cudaEvent_t esolve;
+    prof_begin(c, PS_SOLVE, &esolve);
     while (!conv && its < maxit) {
         // v0 = (b - K x) / beta
         TRET(kmatvec64r(c, x, c.w.p, b));
@@ -376,6 +385,7 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
             k_update<double><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z64.p, n, st + GL.y(0), x), note_launch();
         TCK(cudaGetLastError());
     }
+    prof_end(c, PS_SOLVE, esolve);
     *its_out = its;
     *status = conv ? 0 : 1;
     return 0;
