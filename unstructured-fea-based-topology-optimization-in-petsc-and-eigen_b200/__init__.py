@@ -42,7 +42,8 @@ class Params(C.Structure):
         ("fem_warm_start", C.c_int),
         ("fem_block", C.c_int),
         ("fem_graphs", C.c_int),
-        ("cheb_degree_post", C.c_int)]
+        ("cheb_degree_post", C.c_int),
+        ("amg_half_fine", C.c_int)]
 
 
 class SolveInfo(C.Structure):

@@ -281,6 +281,7 @@ void topo_params_default(topo_params* p) {
     p->fem_block = 1;
     p->fem_graphs = 1;
     p->cheb_degree_post = 0;
+    p->amg_half_fine = 0;
 }
 
 int topo_device_alloc(size_t bytes, void** ptr) {

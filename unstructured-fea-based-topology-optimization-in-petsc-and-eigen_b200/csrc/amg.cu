@@ -13,6 +13,7 @@
 //
 // BSR values are slot-interleaved (see ctx.h) so that the lanes of a warp
 // walking the blocks of one row read every block entry as a coalesced run.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -130,6 +131,7 @@ __global__ void k_bsr_spmv(int nrows, const int* __restrict__ rp, const int* __r
         if (mode == 0) y[o] = v;
         else if (mode == 1) y[o] = b[o] - v;
         else if (mode == 2) y[o] += v;
+        else if (mode == 4) y[o] += dinv[o] * v;  // row-scaled prolongation into hat variables
         else y[o] = T(*scal) * dinv[o] * v;
     }
 }
@@ -196,8 +198,7 @@ __global__ void k_bsr_to_sell(int nrows, int nslices, const int* __restrict__ rp
     if (i < nrows) { r0 = rp[i]; nb = rp[i + 1] - r0; }
     for (int k = 0; k < w; k++)
 #pragma unroll
-        for (int e = 0; e < 9; e++)
-            S[((size_t)(base + k) * 9 + e) * 32 + lane] = k < nb ? A[(size_t)r0 * 9 + e * nb + k] : T(0);
+        for (int e = 0; e < 9; e++) S[sell_idx<T>(base + k, e, lane)] = k < nb ? A[(size_t)r0 * 9 + e * nb + k] : T(0);
 }
 
 // mode 0: y = A x; 1: y = b - A x; 3: y = sigma Dinv A x
@@ -210,17 +211,18 @@ __global__ void __launch_bounds__(256) k_sell_spmv(int nrows, const int* __restr
     if (i >= nrows) return;
     const int s = i >> 5, lane = i & 31;
     const int b0 = sp[s], w = (sp[s + 1] - b0) >> 5;
-    const T* a = S + (size_t)(b0 >> 5) * 288 + lane;
+    const size_t sb = (size_t)(b0 >> 5);
     const int* cp = sci + b0 + lane;
     T a0 = T(0), a1 = T(0), a2 = T(0);
 #pragma unroll 3
     for (int k = 0; k < w; k++) {
         const int j = __ldg(cp + 32 * k);
         const T x0 = x[3L * j], x1 = x[3L * j + 1], x2 = x[3L * j + 2];
-        const T* ak = a + (size_t)k * 288;
-        a0 += __ldg(ak) * x0 + __ldg(ak + 32) * x1 + __ldg(ak + 64) * x2;
-        a1 += __ldg(ak + 96) * x0 + __ldg(ak + 128) * x1 + __ldg(ak + 160) * x2;
-        a2 += __ldg(ak + 192) * x0 + __ldg(ak + 224) * x1 + __ldg(ak + 256) * x2;
+        T av[9];
+        sell_load9<T>(S, sb + k, lane, av);
+        a0 += av[0] * x0 + av[1] * x1 + av[2] * x2;
+        a1 += av[3] * x0 + av[4] * x1 + av[5] * x2;
+        a2 += av[6] * x0 + av[7] * x1 + av[8] * x2;
     }
     const long o = 3L * i;
     if (mode == 0) { y[o] = a0; y[o + 1] = a1; y[o + 2] = a2; }
@@ -242,17 +244,18 @@ __global__ void __launch_bounds__(256) k_sell_cheb(int nrows, const int* __restr
     if (i >= nrows) return;
     const int s = i >> 5, lane = i & 31;
     const int b0 = sp[s], w = (sp[s + 1] - b0) >> 5;
-    const T* a = S + (size_t)(b0 >> 5) * 288 + lane;
+    const size_t sb = (size_t)(b0 >> 5);
     const int* cp = sci + b0 + lane;
     T t[3] = {T(0), T(0), T(0)};
 #pragma unroll 3
     for (int k = 0; k < w; k++) {
         const int j = __ldg(cp + 32 * k);
         const T x0 = dold[3L * j], x1 = dold[3L * j + 1], x2 = dold[3L * j + 2];
-        const T* ak = a + (size_t)k * 288;
-        t[0] += __ldg(ak) * x0 + __ldg(ak + 32) * x1 + __ldg(ak + 64) * x2;
-        t[1] += __ldg(ak + 96) * x0 + __ldg(ak + 128) * x1 + __ldg(ak + 160) * x2;
-        t[2] += __ldg(ak + 192) * x0 + __ldg(ak + 224) * x1 + __ldg(ak + 256) * x2;
+        T av[9];
+        sell_load9<T>(S, sb + k, lane, av);
+        t[0] += av[0] * x0 + av[1] * x1 + av[2] * x2;
+        t[1] += av[3] * x0 + av[4] * x1 + av[5] * x2;
+        t[2] += av[6] * x0 + av[7] * x1 + av[8] * x2;
     }
     const double delta = 0.5 * (*rho);
     const T c2 = T(cq / delta), c1 = T(cr);
@@ -265,6 +268,120 @@ __global__ void __launch_bounds__(256) k_sell_cheb(int nrows, const int* __restr
         dnew[o] = dn;
         x[o] += dn;
     }
+}
+
+// ----------------------------------------------------------------- level 0 in FP16, diagonally scaled
+// Mixed form: the level-0 smoother works on A^ = D^-1/2 A D^-1/2 (unit
+// diagonal, |a^_ij| <= 1 for the SPD stiffness matrix) stored as FP16 in the
+// sliced-ELLPACK layout, with hat variables x^ = D^1/2 x, b^ = D^-1/2 b,
+// r^ = D^-1/2 r.  Chebyshev-Jacobi on A is Chebyshev on A^ with the identity
+// there, so no diagonal is read; the matrix stream is 9 x 2 + 4 bytes per
+// block instead of 9 x 4 + 4.  Arithmetic stays FP32.
+__global__ void k_sell_half_build(int nrows, int nslices, const int* __restrict__ rp, const int* __restrict__ ci,
+                                  const int* __restrict__ sp, const float* __restrict__ A,
+                                  const float* __restrict__ dinv, __half* __restrict__ S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = i >> 5, lane = i & 31;
+    if (s >= nslices) return;
+    const int base = sp[s] >> 5, w = (sp[s + 1] - sp[s]) >> 5;
+    int r0 = 0, nb = 0;
+    if (i < nrows) { r0 = rp[i]; nb = rp[i + 1] - r0; }
+    float si[3] = {0.f, 0.f, 0.f};
+    if (i < nrows)
+        for (int q = 0; q < 3; q++) si[q] = sqrtf(fabsf(dinv[3L * i + q]));
+    for (int k = 0; k < w; k++) {
+        const int j = k < nb ? ci[r0 + k] : 0;
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            float v = 0.f;
+            if (k < nb) v = A[(size_t)r0 * 9 + e * nb + k] * si[e / 3] * sqrtf(fabsf(dinv[3L * j + e % 3]));
+            S[sell_idx<__half>(base + k, e, lane)] = __float2half_rn(v);
+        }
+    }
+}
+// s = D^1/2, sinv = D^-1/2 per DOF
+__global__ void k_hat_scales(long n, const float* __restrict__ dinv, float* __restrict__ s, float* __restrict__ sinv) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const float d = fabsf(dinv[i]);
+        sinv[i] = sqrtf(d);
+        s[i] = d > 0.f ? 1.f / sqrtf(d) : 1.f;
+    }
+}
+// MODE 1: y = b - A^ x          2: Chebyshev step t = A^ d; r -= t; d' = c1 d + c2 r; xo += d'
+// MODE 3: y = sigma A^ x        4: y = s (b - A^ x)  (unscaled residual for the restriction)
+template <int MODE>
+__global__ void __launch_bounds__(256) k_sell_hat(int nrows, const int* __restrict__ sp, const int* __restrict__ sci,
+                                                  const __half* __restrict__ S, const float* __restrict__ x,
+                                                  float* __restrict__ y, const float* __restrict__ b,
+                                                  float* __restrict__ r, float* __restrict__ xo,
+                                                  const float* __restrict__ sc, const double* __restrict__ rho,
+                                                  double cr, double cq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrows) return;
+    const int s = i >> 5, lane = i & 31;
+    const int b0 = sp[s], w = (sp[s + 1] - b0) >> 5;
+    const size_t sb = (size_t)(b0 >> 5);
+    const int* cp = sci + b0 + lane;
+    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+#pragma unroll 3
+    for (int k = 0; k < w; k++) {
+        const int j = __ldg(cp + 32 * k);
+        const float x0 = x[3L * j], x1 = x[3L * j + 1], x2 = x[3L * j + 2];
+        float av[9];
+        sell_load9<__half>(S, sb + k, lane, av);
+        t0 += av[0] * x0 + av[1] * x1 + av[2] * x2;
+        t1 += av[3] * x0 + av[4] * x1 + av[5] * x2;
+        t2 += av[6] * x0 + av[7] * x1 + av[8] * x2;
+    }
+    const float t[3] = {t0, t1, t2};
+    const long o = 3L * i;
+    if (MODE == 1) {
+#pragma unroll
+        for (int q = 0; q < 3; q++) y[o + q] = b[o + q] - t[q];
+    } else if (MODE == 3) {
+        const float sg = (float)(*rho);
+#pragma unroll
+        for (int q = 0; q < 3; q++) y[o + q] = sg * t[q];
+    } else if (MODE == 4) {
+#pragma unroll
+        for (int q = 0; q < 3; q++) y[o + q] = sc[o + q] * (b[o + q] - t[q]);
+    } else {
+        const double delta = 0.5 * (*rho);
+        const float c2 = (float)(cq / delta), c1 = (float)cr;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const float rn = r[o + q] - t[q];
+            const float dn = c1 * x[o + q] + c2 * rn;
+            r[o + q] = rn;
+            y[o + q] = dn;
+            xo[o + q] += dn;
+        }
+    }
+}
+// first Chebyshev step on the hat variables (identity preconditioner)
+__global__ void k_cheb_first_hat(long n, const float* __restrict__ b, float* __restrict__ r, float* __restrict__ d,
+                                 float* __restrict__ x, const double* __restrict__ rho, int zero_init) {
+    const float it = (float)(1.0 / (0.6 * (*rho)));
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        if (zero_init) {
+            const float bi = b[i];
+            r[i] = bi;
+            d[i] = bi * it;
+            x[i] = bi * it;
+        } else {
+            const float di = r[i] * it;
+            d[i] = di;
+            x[i] += di;
+        }
+    }
+}
+// b^ = D^-1/2 v (FP64 in, FP32 out) and x = D^-1/2 x^ in place
+__global__ void k_to_hat(long n, const double* __restrict__ v, const float* __restrict__ sinv, float* __restrict__ b) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        b[i] = (float)(v[i] * (double)sinv[i]);
+}
+__global__ void k_from_hat(long n, const float* __restrict__ sinv, float* __restrict__ x) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) x[i] *= sinv[i];
 }
 
 // first Chebyshev step.  zero_init: r = b, d = Dinv b / theta, x = d.
@@ -721,10 +838,45 @@ static int spmv(Ctx& c, const DevPattern& Ap, const T* A, const T* x, T* y, cons
     return 0;
 }
 
+// level 0 of the mixed form runs on the FP16 scaled operator (single load case)
+static bool use_half0(const Ctx& c) {
+    return c.p.precision == TOPO_PREC_MIXED && c.p.amg_half_fine && !c.p.fine_smoother_matfree &&
+           !(c.ncases > 1 && c.p.fem_block);
+}
+template <class T>
+static bool half_level(const Ctx& c, int l) {
+    return l == 0 && std::is_same<T, float>::value && use_half0(c) && c.h0.valid;
+}
+// hat-variable level-0 products (see k_sell_hat)
+template <int MODE>
+static int sell_hat(Ctx& c, const float* x, float* y, const float* b, float* r, float* xo, const float* sc,
+                    const double* rho, double cr = 0.0, double cq = 0.0) {
+    const AmgDevLevel& D = c.dl[0];
+    k_sell_hat<MODE><<<(D.nnode + 255) / 256, 256, 0, c.s>>>(D.nnode, D.sell_ptr.p, D.sell_ci.p,
+                                                             reinterpret_cast<const __half*>(c.h0.S.p), x, y, b, r, xo,
+                                                             sc, rho, cr, cq), note_launch();
+    TCK(cudaGetLastError());
+    return 0;
+}
+
 template <class T>
 static int level_spmv(Ctx& c, int l, const T* x, T* y, const T* b, int mode, const T* dinv = nullptr,
                       const double* scal = nullptr) {
     AmgVals<T>& v = vals<T>(c);
+    if (half_level<T>(c, l) && (mode == 1 || mode == 3)) {
+        // mode 1: r^ = b^ - A^ x^; mode 3: w = sigma A^ v (power iteration)
+        const float* xf = reinterpret_cast<const float*>(x);
+        float* yf = reinterpret_cast<float*>(y);
+        cudaEvent_t e0;
+        if (mode == 1) {
+            prof_begin(c, PS_RES0, &e0);
+            TRET(sell_hat<1>(c, xf, yf, reinterpret_cast<const float*>(b), nullptr, nullptr, nullptr, nullptr));
+            prof_end(c, PS_RES0, e0);
+        } else {
+            TRET(sell_hat<3>(c, xf, yf, nullptr, nullptr, nullptr, nullptr, scal));
+        }
+        return 0;
+    }
     if (l == 0 && mode != 2) {
         const AmgDevLevel& D = c.dl[0];
         cudaEvent_t e0;
@@ -786,11 +938,15 @@ static int numeric(Ctx& c) {
                                               c.dof_fixed.p, v.A[0].p, c.maxdeg), note_launch();
         }
         TCK(cudaGetLastError());
-        // sliced-ELLPACK copy of the level-0 operator for the smoother
+        // sliced-ELLPACK copy of the level-0 operator for the smoother (the
+        // mixed single-load form uses the FP16 scaled copy built below)
         AmgDevLevel& D0 = c.dl[0];
-        k_bsr_to_sell<T><<<D0.nslices * 32 / 256 + 1, 256, 0, c.s>>>(D0.nnode, D0.nslices, D0.A.rp.p, D0.sell_ptr.p,
-                                                                     v.A[0].p, v.A0s.p), note_launch();
-        TCK(cudaGetLastError());
+        c.h0.valid = false;
+        if (!(std::is_same<T, float>::value && use_half0(c))) {
+            k_bsr_to_sell<T><<<D0.nslices * 32 / 256 + 1, 256, 0, c.s>>>(D0.nnode, D0.nslices, D0.A.rp.p,
+                                                                         D0.sell_ptr.p, v.A[0].p, v.A0s.p), note_launch();
+            TCK(cudaGetLastError());
+        }
     }
     prof_end(c, PS_SETUP_ASM, pe);
     for (int l = 0; l < c.nlev; l++) {
@@ -802,6 +958,23 @@ static int numeric(Ctx& c) {
             k_diag_inv<T, 6><<<grid_for(D.nnode, 256, 1 << 20), 256, 0, c.s>>>(D.nnode, D.A.rp.p, D.diagpos.p, v.A[l].p,
                                                                            v.dinv[l].p), note_launch();
         TCK(cudaGetLastError());
+        if (l == 0 && std::is_same<T, float>::value && use_half0(c)) {
+            prof_begin(c, PS_SETUP_ASM, &pe);
+            Half0& H = c.h0;
+            if (!H.S.p) {
+                TRET(H.S.alloc((size_t)D.sell_blocks * 9));
+                TRET(H.s.alloc(D.ndof));
+                TRET(H.sinv.alloc(D.ndof));
+            }
+            k_sell_half_build<<<D.nslices * 32 / 256 + 1, 256, 0, c.s>>>(
+                D.nnode, D.nslices, D.A.rp.p, D.A.ci.p, D.sell_ptr.p, reinterpret_cast<const float*>(v.A[0].p),
+                reinterpret_cast<const float*>(v.dinv[0].p), reinterpret_cast<__half*>(H.S.p)), note_launch();
+            k_hat_scales<<<grid_for(D.ndof, 256), 256, 0, c.s>>>(D.ndof, reinterpret_cast<const float*>(v.dinv[0].p),
+                                                                  H.s.p, H.sinv.p), note_launch();
+            TCK(cudaGetLastError());
+            H.valid = true;
+            prof_end(c, PS_SETUP_ASM, pe);
+        }
         if (l == c.nlev - 1) break;
         prof_begin(c, PS_SETUP_RHO, &pe);
         TRET(estimate_rho<T>(c, l, std::max(1, c.p.amg_rho_its)));
@@ -887,6 +1060,25 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
     double cr[16] = {0}, cq[16] = {0};
     cheb_coeffs(std::min(deg, 16), cr, cq);
     const double* rho = c.rho.p + 2 * kMaxLevels + l;  // safety-scaled spectral bound
+    if (half_level<T>(c, l)) {
+        // Chebyshev on A^ in hat variables: no diagonal
+        float* xf = reinterpret_cast<float*>(x);
+        const float* bf = reinterpret_cast<const float*>(b);
+        float* r = reinterpret_cast<float*>(v.r[0].p);
+        float* dc = reinterpret_cast<float*>(v.d[0].p);
+        float* dn = reinterpret_cast<float*>(v.d2[0].p);
+        if (!zero_init) TRET(level_spmv<T>(c, 0, x, v.r[0].p, b, 1));
+        k_cheb_first_hat<<<grid_for(n, 256), 256, 0, c.s>>>(n, bf, r, dc, xf, rho, zero_init ? 1 : 0), note_launch();
+        for (int k = 1; k < deg && k < 16; k++) {
+            cudaEvent_t e0;
+            prof_begin(c, PS_CHEB0, &e0);
+            TRET(sell_hat<2>(c, dc, dn, nullptr, r, xf, nullptr, rho, cr[k], cq[k]));
+            prof_end(c, PS_CHEB0, e0);
+            std::swap(dc, dn);
+        }
+        TCK(cudaGetLastError());
+        return 0;
+    }
     const bool matfree = (l == 0) && c.p.fine_smoother_matfree;
     if (!zero_init) {
         // r = b - A x
@@ -945,7 +1137,14 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
     for (int l = 0; l < L; l++) {
         AmgDevLevel& D = c.dl[l];
         TRET(smooth<T>(c, l, bl[l], xl[l], true));
-        if (l == 0 && c.p.fine_smoother_matfree) {
+        if (half_level<T>(c, l)) {
+            // unscaled residual t = D^1/2 (b^ - A^ x^) for the restriction
+            cudaEvent_t e0;
+            prof_begin(c, PS_RES0, &e0);
+            TRET(sell_hat<4>(c, reinterpret_cast<const float*>(xl[0]), reinterpret_cast<float*>(v.t[0].p),
+                             reinterpret_cast<const float*>(bl[0]), nullptr, nullptr, c.h0.s.p, nullptr));
+            prof_end(c, PS_RES0, e0);
+        } else if (l == 0 && c.p.fine_smoother_matfree) {
             if (std::is_same<T, float>::value) TRET(kmatvec32(c, (const float*)xl[0], (float*)v.t[0].p, (const float*)bl[0]));
             else TRET(kmatvec64r(c, (const double*)xl[0], (double*)v.t[0].p, (const double*)bl[0]));
         } else {
@@ -963,9 +1162,16 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
     for (int l = L - 1; l >= 0; l--) {
         AmgDevLevel& D = c.dl[l];
         if (l == 0) prof_end(c, PS_VC_COARSE, ecoarse);
-        if (D.bs == 3) TRET((spmv<T, 3, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 2)));
+        if (half_level<T>(c, l))  // x^ += D^1/2 P e
+            TRET((spmv<T, 3, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 4, reinterpret_cast<const T*>(c.h0.s.p))));
+        else if (D.bs == 3) TRET((spmv<T, 3, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 2)));
         else TRET((spmv<T, 6, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 2)));
         TRET(smooth<T>(c, l, bl[l], xl[l], false));
+    }
+    if (half_level<T>(c, 0)) {
+        const long n0 = c.dl[0].ndof;
+        k_from_hat<<<grid_for(n0, 256), 256, 0, c.s>>>(n0, c.h0.sinv.p, reinterpret_cast<float*>(x0)), note_launch();
+        TCK(cudaGetLastError());
     }
     return 0;
 }
@@ -1043,7 +1249,10 @@ int amg_vcycle64(Ctx& c, const double* b, double* x) { return vcycle<double>(c, 
 int amg_vcycle32(Ctx& c, const double* b64, float* x) {
     AmgVals<float>& v = c.v32;
     const long n = c.dl[0].ndof;
-    k_convert<double, float><<<grid_for(n, 256), 256, 0, c.s>>>(n, b64, v.b[0].p), note_launch();
+    if (half_level<float>(c, 0))
+        k_to_hat<<<grid_for(n, 256), 256, 0, c.s>>>(n, b64, c.h0.sinv.p, v.b[0].p), note_launch();
+    else
+        k_convert<double, float><<<grid_for(n, 256), 256, 0, c.s>>>(n, b64, v.b[0].p), note_launch();
     TCK(cudaGetLastError());
     // level-0 rhs lives in v.b[0]; the smoother keeps b intact
     return vcycle<float>(c, v.b[0].p, x);

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(256) k_sell_blk(int nrows, const int* __restri
     if (i >= nrows) return;
     const int s = i >> 5, lane = i & 31;
     const int b0 = sp[s], w = (sp[s + 1] - b0) >> 5;
-    const T* a = S + (size_t)(b0 >> 5) * 288 + lane;
+    const size_t sb = (size_t)(b0 >> 5);
     const int* cp = sci + b0 + lane;
     const int c0 = g * CPT;
     T acc[3][CPT];
@@ -63,10 +63,8 @@ __global__ void __launch_bounds__(256) k_sell_blk(int nrows, const int* __restri
             const uint4 t = __ldg(reinterpret_cast<const uint4*>(x + (3L * j + d) * KB + c0));
             memcpy(xv[d], &t, 16);
         }
-        const T* ak = a + (size_t)k * 288;
         T av[9];
-#pragma unroll
-        for (int e = 0; e < 9; e++) av[e] = __ldg(ak + 32 * e);
+        sell_load9<T>(S, sb + k, lane, av);
 #pragma unroll
         for (int q = 0; q < 3; q++)
 #pragma unroll

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <cstring>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -190,6 +191,36 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& b) {
     }
     __syncthreads();
     return s_ok != 0;
+}
+
+// ----------------------------------------------------------------- level-0 sliced ELLPACK values
+// One slot of a 32-row slice holds 9 values per row (a 3x3 block) in 288
+// elements: the first G*VPL entries of all 32 rows as 16-byte vectors
+// (VPL = 16/sizeof(T) entries per row and vector, G vectors), then the
+// remaining entries row-interleaved.  A warp reads a slot with G 16-byte
+// loads and 9 - G*VPL scalar loads per lane (float: 2 + 1, double: 4 + 1,
+// half: 1 + 1) instead of 9 scalar loads.
+template <class T>
+__host__ __device__ __forceinline__ size_t sell_idx(size_t slot, int e, int lane) {
+    constexpr int VPL = 16 / (int)sizeof(T), G = 9 / VPL;
+    const size_t base = slot * 288;
+    if (e < G * VPL) return base + (size_t)(e / VPL) * 32 * VPL + (size_t)lane * VPL + (e % VPL);
+    return base + (size_t)G * 32 * VPL + (size_t)(e - G * VPL) * 32 + lane;
+}
+template <class T, class TV>
+__device__ __forceinline__ void sell_load9(const T* __restrict__ S, size_t slot, int lane, TV (&av)[9]) {
+    constexpr int VPL = 16 / (int)sizeof(T), G = 9 / VPL;
+    const T* p = S + slot * 288;
+    T raw[9];
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        const uint4 t = __ldg(reinterpret_cast<const uint4*>(p + g * 32 * VPL + lane * VPL));
+        memcpy(raw + g * VPL, &t, 16);
+    }
+#pragma unroll
+    for (int r = 0; r < 9 - G * VPL; r++) raw[G * VPL + r] = p[G * 32 * VPL + r * 32 + lane];
+#pragma unroll
+    for (int e = 0; e < 9; e++) av[e] = (TV)raw[e];
 }
 
 #endif  // __CUDACC__

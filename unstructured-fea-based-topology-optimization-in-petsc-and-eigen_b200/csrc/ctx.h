@@ -85,6 +85,13 @@ struct AmgVals {
     bool allocated = false;
 };
 
+// mixed form, level 0 in FP16 on the diagonally scaled operator (amg.cu)
+struct Half0 {
+    DBuf<uint16_t> S;           // D^-1/2 A D^-1/2 as FP16, sliced-ELLPACK layout
+    DBuf<float> s, sinv;        // D^1/2, D^-1/2 per DOF
+    bool valid = false;         // built for the current design iteration
+};
+
 // CUDA graphs of the Arnoldi steps of one FGMRES form: step j (V-cycle,
 // operator, Gram-Schmidt, Givens, residual read-back) is captured once and
 // replayed in every later solve with the same buffers.  `sig` identifies the
@@ -183,6 +190,7 @@ struct Ctx {
     DBuf<double> cA;            // coarsest dense matrix scratch
     AmgVals<double> v64;
     AmgVals<float> v32;
+    Half0 h0;
     DBuf<double> rho;           // [kMaxLevels] spectral estimates of D^-1 A
     bool amg_ready = false;
 
