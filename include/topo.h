@@ -80,6 +80,9 @@ typedef struct topo_params {
     int fem_graphs;        /* 1 (default): replay each FGMRES Arnoldi step from a CUDA graph
                               captured in an earlier solve with the same buffers */
     int cheb_degree_post;  /* post-smoothing Chebyshev degree (0: same as cheb_degree) */
+    int cheb_degree_coarse; /* Chebyshev degree below the finest level (0: as the finest; default 4:
+                               the coarse levels are small and latency-bound, and stronger
+                               smoothing there cuts FGMRES iterations by about a quarter) */
     int amg_half_fine;     /* mixed form: 1 keeps the level-0 smoother's matrix as FP16
                               D^-1/2 A D^-1/2 (FP32 arithmetic); 0 (default) keeps it FP32 */
 } topo_params;

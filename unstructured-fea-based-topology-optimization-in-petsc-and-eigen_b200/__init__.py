@@ -43,6 +43,7 @@ class Params(C.Structure):
         ("fem_block", C.c_int),
         ("fem_graphs", C.c_int),
         ("cheb_degree_post", C.c_int),
+        ("cheb_degree_coarse", C.c_int),
         ("amg_half_fine", C.c_int)]
 
 

@@ -1056,7 +1056,9 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
     AmgDevLevel& D = c.dl[l];
     const long n = D.ndof;
     // pre-smoothing (zero initial guess) and post-smoothing degrees
-    const int deg = std::max(1, (!zero_init && c.p.cheb_degree_post > 0) ? c.p.cheb_degree_post : c.p.cheb_degree);
+    int deg = (!zero_init && c.p.cheb_degree_post > 0) ? c.p.cheb_degree_post : c.p.cheb_degree;
+    if (l > 0 && c.p.cheb_degree_coarse > 0) deg = c.p.cheb_degree_coarse;  // levels below the finest
+    deg = std::max(1, deg);
     double cr[16] = {0}, cq[16] = {0};
     cheb_coeffs(std::min(deg, 16), cr, cq);
     const double* rho = c.rho.p + 2 * kMaxLevels + l;  // safety-scaled spectral bound

@@ -319,7 +319,9 @@ static int smooth_blk(Ctx& c, int l, const T* b, T* x, bool zero_init) {
     AmgBlkVecs<T>& w = bvecs<T>(c);
     const AmgDevLevel& D = c.dl[l];
     const long n = D.ndof;
-    const int deg = std::max(1, std::min((!zero_init && c.p.cheb_degree_post > 0) ? c.p.cheb_degree_post : c.p.cheb_degree, 16));
+    int deg = (!zero_init && c.p.cheb_degree_post > 0) ? c.p.cheb_degree_post : c.p.cheb_degree;
+    if (l > 0 && c.p.cheb_degree_coarse > 0) deg = c.p.cheb_degree_coarse;
+    deg = std::max(1, std::min(deg, 16));
     double cr[16] = {0}, cq[16] = {0};
     cheb_coeffs(deg, cr, cq);
     const double* rho = c.rho.p + 2 * kMaxLevels + l;
@@ -724,7 +726,7 @@ static int fgmres_blk(Ctx& c, const double* b, double* x, int* its_out, int* sta
                        (uint64_t)(uintptr_t)B.bv32.x[0].p, (uint64_t)(uintptr_t)B.bv64.x[0].p,
                        (uint64_t)(uintptr_t)c.v32.A0s.p, (uint64_t)(uintptr_t)c.v64.A0s.p,
                        (uint64_t)(uintptr_t)c.cinv.p, (uint64_t)(uintptr_t)c.rho.p, (uint64_t)c.p.precision,
-                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)KB, (uint64_t)nf})
+                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)KB, (uint64_t)nf})
         sig = sig_mix(sig, v);
     StepGraphs& G = B.graphs;
     if (G.sig != sig) {
