@@ -565,6 +565,53 @@ __global__ void k_spgemm_pairs(int nrows, const int* __restrict__ Arp, const int
     }
 }
 
+// The same product from its plan (output-stationary): G lanes per C row, a
+// lane owns one C block at a time and sums its contributing (A block,
+// B block) pairs in registers: no shared memory, no atomics, no searches,
+// and the C block's entries are written as coalesced runs.
+template <class T, int BR, int BK, int BC, int G>
+__global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __restrict__ Arp, const int* __restrict__ Aci,
+                                                     const T* __restrict__ A, const int* __restrict__ Brp,
+                                                     const T* __restrict__ B, const int* __restrict__ Crp,
+                                                     T* __restrict__ C, const int* __restrict__ pptr,
+                                                     const uint32_t* __restrict__ pr) {
+    constexpr int BRK = BR * BK, BKC = BK * BC, BRC = BR * BC;
+    const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int i = (int)(tid / G), gl = (int)(tid % G);
+    if (i >= nrows) return;
+    const int a0 = Arp[i], nA = Arp[i + 1] - a0;
+    const int c0 = Crp[i], nC = Crp[i + 1] - c0;
+    const T* Ar = A + (size_t)a0 * BRK;
+    for (int sl = gl; sl < nC; sl += G) {
+        T acc[BRC];
+#pragma unroll
+        for (int e = 0; e < BRC; e++) acc[e] = T(0);
+        const int p1 = pptr[c0 + sl + 1];
+        for (int p = pptr[c0 + sl]; p < p1; p++) {
+            const uint32_t w = __ldg(pr + p);
+            const int a = (int)(w >> 16), s = (int)(w & 0xffffu);
+            const int k = __ldg(Aci + a0 + a);
+            const int b0 = __ldg(Brp + k), nB = __ldg(Brp + k + 1) - b0;
+            T ab[BRK], bb[BKC];
+#pragma unroll
+            for (int e = 0; e < BRK; e++) ab[e] = __ldg(Ar + (size_t)e * nA + a);
+#pragma unroll
+            for (int e = 0; e < BKC; e++) bb[e] = __ldg(B + (size_t)b0 * BKC + (size_t)e * nB + s);
+#pragma unroll
+            for (int r = 0; r < BR; r++)
+#pragma unroll
+                for (int cc = 0; cc < BC; cc++) {
+                    T v = acc[r * BC + cc];
+#pragma unroll
+                    for (int m = 0; m < BK; m++) v += ab[r * BK + m] * bb[m * BC + cc];
+                    acc[r * BC + cc] = v;
+                }
+        }
+#pragma unroll
+        for (int e = 0; e < BRC; e++) C[(size_t)c0 * BRC + (size_t)e * nC + sl] = acc[e];
+    }
+}
+
 // P = Pt - (4 / (3 rho)) Dinv (A Pt), pattern of A Pt; Pt's block sits at ptpos
 template <class T, int BS>
 __global__ void k_smooth_p(int nnode, const int* __restrict__ rp, const int* __restrict__ ptpos,
@@ -798,6 +845,26 @@ static const T* pt_vals(Ctx& c, int l) {
     return (const T*)c.dl[l].Pt32c.p;
 }
 
+template <int BR, int BK, int BC, class T, int G>
+static void spgemm_plan_g(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp, const T* B,
+                          const DevPattern& Cp, T* C, const ProductPlan& pl) {
+    const long nt = (long)Cp.nrows * G;
+    k_spgemm_plan<T, BR, BK, BC, G><<<(int)((nt + 255) / 256), 256, 0, c.s>>>(Cp.nrows, Ap.rp.p, Ap.ci.p, A, Bp.rp.p, B,
+                                                                             Cp.rp.p, C, pl.ptr.p, pl.pr.p);
+}
+// C = A B from the product's plan
+template <int BR, int BK, int BC, class T>
+static int spgemm_plan(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp, const T* B, const DevPattern& Cp,
+                       T* C, const ProductPlan& pl) {
+    if (pl.avg_row > 24) spgemm_plan_g<BR, BK, BC, T, 32>(c, Ap, A, Bp, B, Cp, C, pl);
+    else if (pl.avg_row > 12) spgemm_plan_g<BR, BK, BC, T, 16>(c, Ap, A, Bp, B, Cp, C, pl);
+    else if (pl.avg_row > 6) spgemm_plan_g<BR, BK, BC, T, 8>(c, Ap, A, Bp, B, Cp, C, pl);
+    else spgemm_plan_g<BR, BK, BC, T, 4>(c, Ap, A, Bp, B, Cp, C, pl);
+    note_launch();
+    TCK(cudaGetLastError());
+    return 0;
+}
+
 template <int BR, int BK, int BC, class T>
 static int spgemm(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp, const T* B, const DevPattern& Cp,
                   T* C) {
@@ -985,28 +1052,28 @@ static int numeric(Ctx& c) {
         const T* ptv = pt_vals<T>(c, l);
         if (D.bs == 3) {
             if (c.p.amg_smooth_p) {
-                TRET((spgemm<3, 3, 6, T>(c, D.A, v.A[l].p, D.Ptp, ptv, D.P, v.T_[l].p)));
+                TRET((spgemm_plan<3, 3, 6, T>(c, D.A, v.A[l].p, D.Ptp, ptv, D.P, v.T_[l].p, D.plan_T)));
                 k_smooth_p<T, 3><<<(D.nnode * 32 + 255) / 256, 256, 0, c.s>>>(
                     D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p), note_launch();
             } else {
                 TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 18, cudaMemcpyDeviceToDevice, c.s));
             }
-            TRET((spgemm<3, 3, 6, T>(c, D.A, v.A[l].p, D.P, v.P[l].p, D.AP, v.AP[l].p)));
+            TRET((spgemm_plan<3, 3, 6, T>(c, D.A, v.A[l].p, D.P, v.P[l].p, D.AP, v.AP[l].p, D.plan_AP)));
             k_transpose<T, 3><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
                                                                              D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();
-            TRET((spgemm<6, 3, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p)));
+            TRET((spgemm_plan<6, 3, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
         } else {
             if (c.p.amg_smooth_p) {
-                TRET((spgemm<6, 6, 6, T>(c, D.A, v.A[l].p, D.Ptp, ptv, D.P, v.T_[l].p)));
+                TRET((spgemm_plan<6, 6, 6, T>(c, D.A, v.A[l].p, D.Ptp, ptv, D.P, v.T_[l].p, D.plan_T)));
                 k_smooth_p<T, 6><<<(D.nnode * 32 + 255) / 256, 256, 0, c.s>>>(
                     D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p), note_launch();
             } else {
                 TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 36, cudaMemcpyDeviceToDevice, c.s));
             }
-            TRET((spgemm<6, 6, 6, T>(c, D.A, v.A[l].p, D.P, v.P[l].p, D.AP, v.AP[l].p)));
+            TRET((spgemm_plan<6, 6, 6, T>(c, D.A, v.A[l].p, D.P, v.P[l].p, D.AP, v.AP[l].p, D.plan_AP)));
             k_transpose<T, 6><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
                                                                              D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();
-            TRET((spgemm<6, 6, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p)));
+            TRET((spgemm_plan<6, 6, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
         }
         TCK(cudaGetLastError());
         prof_end(c, PS_SETUP_GAL, pe);

@@ -59,6 +59,17 @@ struct AmgHostLevel {
     std::vector<int> rperm;     // R block -> P block index
 };
 
+// Output-stationary plan of a fixed-pattern block product C = A B: for every
+// block of C (CSR order) the (A slot, B slot) pairs that contribute, packed
+// as (slot in A's row) << 16 | (slot in B's row).  Built on the host once
+// per mesh.
+struct ProductPlan {
+    DBuf<int> ptr;              // nnzb(C) + 1
+    DBuf<uint32_t> pr;          // pairs
+    int avg_row = 0;            // mean blocks per C row (picks lanes per row)
+};
+int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, ProductPlan& out, cudaStream_t s);
+
 struct AmgDevLevel {
     int bs = 3, nnode = 0, ndof = 0, nagg = 0;
     DevPattern A, P, AP, R;
@@ -69,6 +80,7 @@ struct AmgDevLevel {
     int nslices = 0;
     long sell_blocks = 0;
     DBuf<int> sell_ptr, sell_ci;
+    ProductPlan plan_T, plan_AP, plan_RAP;  // A Pt, A P, R (A P)
     DevPattern Ptp;             // tentative prolongator: one block per aggregated node
     DBuf<double> Pt64c;         // its bs x 6 blocks (compact, FP64)
     DBuf<float> Pt32c;          // (FP32 copy for the mixed form)

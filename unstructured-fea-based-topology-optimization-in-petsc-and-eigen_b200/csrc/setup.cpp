@@ -8,7 +8,9 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <atomic>
 #include <mutex>
+#include <thread>
 
 #include "ctx.h"
 
@@ -35,6 +37,59 @@ long& launch_counter() {
 int cuda_fail(cudaError_t e, const char* file, int line) {
     set_error("CUDA error %s (%s) at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e), file, line);
     return e == cudaErrorMemoryAllocation ? TOPO_ERR_OOM : TOPO_ERR_CUDA;
+}
+
+// ----------------------------------------------------------------- product plans
+int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, ProductPlan& out, cudaStream_t s) {
+    const int n = A.nrows;
+    std::vector<int> ptr((size_t)C.nnzb() + 1, 0);
+    const int nth = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+    auto for_rows = [&](auto&& fn) {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nth; t++)
+            th.emplace_back([&, t]() {
+                std::vector<int> slot(C.ncols, -1);
+                for (int i = (int)((long)n * t / nth); i < (int)((long)n * (t + 1) / nth); i++) fn(i, slot);
+            });
+        for (auto& x : th) x.join();
+    };
+    std::atomic<bool> bad(false);
+    // pass 1: pairs per C block
+    for_rows([&](int i, std::vector<int>& slot) {
+        for (int q = C.rp[i]; q < C.rp[i + 1]; q++) slot[C.ci[q]] = q;
+        const int na = A.rp[i + 1] - A.rp[i];
+        if (na > 65535) bad = true;
+        for (int a = 0; a < na; a++) {
+            const int k = A.ci[A.rp[i] + a];
+            for (int sb = 0; sb < B.rp[k + 1] - B.rp[k]; sb++) {
+                const int q = slot[B.ci[B.rp[k] + sb]];
+                if (q < 0 || sb > 65535) { bad = true; continue; }
+                ptr[q + 1]++;
+            }
+        }
+        for (int q = C.rp[i]; q < C.rp[i + 1]; q++) slot[C.ci[q]] = -1;
+    });
+    if (bad) { set_error("product plan: a row is too long or a pattern is inconsistent"); return TOPO_ERR_UNSUPPORTED; }
+    for (size_t q = 0; q + 1 < ptr.size(); q++) ptr[q + 1] += ptr[q];
+    std::vector<uint32_t> pr((size_t)ptr.back());
+    std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+    // pass 2: the pairs, in (A slot, B slot) order within each C block
+    for_rows([&](int i, std::vector<int>& slot) {
+        for (int q = C.rp[i]; q < C.rp[i + 1]; q++) slot[C.ci[q]] = q;
+        const int na = A.rp[i + 1] - A.rp[i];
+        for (int a = 0; a < na; a++) {
+            const int k = A.ci[A.rp[i] + a];
+            for (int sb = 0; sb < B.rp[k + 1] - B.rp[k]; sb++) {
+                const int q = slot[B.ci[B.rp[k] + sb]];
+                pr[fill[q]++] = ((uint32_t)a << 16) | (uint32_t)sb;
+            }
+        }
+        for (int q = C.rp[i]; q < C.rp[i + 1]; q++) slot[C.ci[q]] = -1;
+    });
+    out.avg_row = C.nrows ? (int)((C.nnzb() + C.nrows - 1) / C.nrows) : 1;
+    TRET(out.ptr.upload(ptr, s));
+    TRET(out.pr.upload(pr, s));
+    return 0;
 }
 
 // ----------------------------------------------------------------- patterns
@@ -433,6 +488,9 @@ int build_amg_host(Ctx& c) {
             TRET(D.Ptp.upload(Ptp, s));
             TRET(D.Pt64c.upload(pv, s));
             TRET(D.Pt32c.upload(pv32, s));
+            TRET(build_plan(H.A, Ptp, H.P, D.plan_T, s));
+            TRET(build_plan(H.A, H.P, H.AP, D.plan_AP, s));
+            TRET(build_plan(H.R, H.AP, c.hl[l + 1].A, D.plan_RAP, s));
         }
     }
     return 0;
