@@ -52,7 +52,9 @@ int dev_dot(Ctx& c, const double* a, const double* b, long n, double* out_dev) {
 }
 
 // ----------------------------------------------------------------- FGMRES kernels
-// h_j = V_j . w for j < nv (classical Gram-Schmidt: one pass over w)
+// h_j = V_j . w for j < nv (classical Gram-Schmidt: one pass over w).
+// Two entries per thread and load (16-byte vectors: the basis rows are
+// 16-byte aligned, ld even), the odd last entry by one thread.
 template <int NV>
 __global__ void __launch_bounds__(256) k_mdot(long n, int nv, const double* __restrict__ V, long ld,
                                               const double* __restrict__ w, double* __restrict__ part) {
@@ -60,12 +62,21 @@ __global__ void __launch_bounds__(256) k_mdot(long n, int nv, const double* __re
     double acc[NV];
 #pragma unroll
     for (int j = 0; j < NV; j++) acc[j] = 0.0;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        const double wi = w[i];
+    const long n2 = n >> 1;
+    const double2* w2 = reinterpret_cast<const double2*>(w);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n2; i += (long)gridDim.x * blockDim.x) {
+        const double2 wi = w2[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
-            if (j < nv) acc[j] += V[j * ld + i] * wi;
+            if (j < nv) {
+                const double2 v = reinterpret_cast<const double2*>(V + j * ld)[i];
+                acc[j] += v.x * wi.x + v.y * wi.y;
+            }
     }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0)
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < nv) acc[j] += V[j * ld + n - 1] * w[n - 1];
     block_sum<NV>(acc, sm);
     if (threadIdx.x == 0)
         for (int j = 0; j < nv; j++) part[(long)blockIdx.x * nv + j] = acc[j];
@@ -80,12 +91,26 @@ __global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __re
     if (threadIdx.x < nv) hs[threadIdx.x] = h[threadIdx.x];
     __syncthreads();
     double v[1] = {0.0};
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        double wi = w[i];
+    const long n2 = n >> 1;
+    double2* w2 = reinterpret_cast<double2*>(w);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n2; i += (long)gridDim.x * blockDim.x) {
+        double2 wi = w2[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
-            if (j < nv) wi -= hs[j] * V[j * ld + i];
-        w[i] = wi;
+            if (j < nv) {
+                const double2 vv = reinterpret_cast<const double2*>(V + j * ld)[i];
+                wi.x -= hs[j] * vv.x;
+                wi.y -= hs[j] * vv.y;
+            }
+        w2[i] = wi;
+        v[0] += wi.x * wi.x + wi.y * wi.y;
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        double wi = w[n - 1];
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < nv) wi -= hs[j] * V[j * ld + n - 1];
+        w[n - 1] = wi;
         v[0] += wi * wi;
     }
     block_sum<1>(v, sm);
@@ -271,16 +296,17 @@ static int arnoldi_step(Ctx& c, void* p) {
     const StepArgs& a = *static_cast<const StepArgs*>(p);
     const int j = a.j;
     const long n = a.n;
-    const double* vj = c.V.p + (size_t)j * n;
+    const long ldv = (n + 31) & ~31L;  // basis rows 256-byte aligned
+    const double* vj = c.V.p + (size_t)j * ldv;
     TRET(precond_apply(c, vj, j));
     if (c.p.precision == TOPO_PREC_MIXED) TRET(kmatvec_f32in(c, c.Ee64.p, c.Z32.p + (size_t)j * n, c.w.p));
     else TRET(kmatvec(c, c.Ee64.p, c.Z64.p + (size_t)j * n, c.w.p));
     cudaEvent_t e0;
     prof_begin(c, PS_ORTH, &e0);
-    TRET(mdot(c, j + 1, c.V.p, n, c.w.p, a.gm));
-    TRET(orth(c, j + 1, c.V.p, n, a.gm, c.w.p, a.gm + j + 1));
+    TRET(mdot(c, j + 1, c.V.p, ldv, c.w.p, a.gm));
+    TRET(orth(c, j + 1, c.V.p, ldv, a.gm, c.w.p, a.gm + j + 1));
     prof_end(c, PS_ORTH, e0);
-    k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, a.gm + j + 1, c.V.p + (size_t)(j + 1) * n, 1),
+    k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, a.gm + j + 1, c.V.p + (size_t)(j + 1) * ldv, 1),
         note_launch();
     k_gm_givens<<<1, 32, 0, c.s>>>(a.GL, j, a.gm, a.st, a.out + 2 * j), note_launch();
     TCK(cudaMemcpyAsync(a.hs + 2 * j, a.out + 2 * j, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
@@ -300,8 +326,9 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
     const int m = std::max(1, std::min(c.p.fem_restart, 128));
     const int maxit = c.p.fem_maxit;
     const GmLayout GL{m};
-    if (!c.V.p || (long)c.V.n < (long)(m + 1) * n) {
-        TRET(c.V.alloc((size_t)(m + 1) * n));
+    const long ldv = (n + 31) & ~31L;  // basis rows 256-byte aligned
+    if (!c.V.p || (long)c.V.n < (long)(m + 1) * ldv) {
+        TRET(c.V.alloc((size_t)(m + 1) * ldv));
         TRET(c.w.alloc(n));
         TRET(c.wtmp.alloc(GL.size() + 2 * m + 8));
         c.Z32.reset();
