@@ -83,6 +83,9 @@ typedef struct topo_params {
     int cheb_degree_coarse; /* Chebyshev degree below the finest level (0: as the finest; default 4:
                                the coarse levels are small and latency-bound, and stronger
                                smoothing there cuts FGMRES iterations by about a quarter) */
+    int amg_coarse_cta;    /* 1: the V-cycle below the first level with <= 8192 DOFs runs in one
+                              thread-block cluster (one launch instead of one per sweep); 0 (default):
+                              per-sweep kernels, which measured faster at 392k under graph replay */
     int amg_half_fine;     /* mixed form: 1 keeps the level-0 smoother's matrix as FP16
                               D^-1/2 A D^-1/2 (FP32 arithmetic); 0 (default) keeps it FP32 */
 } topo_params;

@@ -64,3 +64,20 @@ def test_prolongator_structure(built):
     At = A @ t
     rows_free = np.abs(At) < (1e-9 if prec == 0 else 1e-5) * abs(A).max()
     assert rows_free.mean() > 0.5
+
+
+def test_cluster_coarse_cycle_matches_per_level_kernels(T, cuda):
+    """The lower V-cycle run by one thread-block cluster gives the same solve
+    (same operations, summation order aside) as the per-level kernels."""
+    import numpy as np
+    v, e, f, ld, lv = T.gen_cantilever(40, 20, 10, 8)
+    x = cuda.tensor(np.random.default_rng(4).uniform(0.05, 1.0, e.shape[0]), device="cuda")
+    out = []
+    for cc in (1, 0):
+        ctx = T.Context(v, e, f, ld, lv, Emax=1.0, rmin=1.5, volfrac=0.12, amg_coarse_cta=cc, fem_rtol=1e-8)
+        fx, gx, df, dg, rc = ctx.fem_obj_sens(x)
+        assert rc == 0
+        out.append((fx, ctx.info().fem_its))
+        ctx.close()
+    assert abs(out[0][0] - out[1][0]) <= 1e-10 * abs(out[1][0])
+    assert abs(out[0][1] - out[1][1]) <= 1

@@ -44,6 +44,7 @@ class Params(C.Structure):
         ("fem_graphs", C.c_int),
         ("cheb_degree_post", C.c_int),
         ("cheb_degree_coarse", C.c_int),
+        ("amg_coarse_cta", C.c_int),
         ("amg_half_fine", C.c_int)]
 
 

@@ -792,6 +792,167 @@ __global__ void k_convert(long n, const TI* __restrict__ a, TO* __restrict__ b) 
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = TO(a[i]);
 }
 
+// ----------------------------------------------------------------- coarse levels in one thread-block cluster
+// The levels below l0 (a few thousand DOFs at most) are latency-bound: each
+// of their sweeps is a tiny kernel.  One thread-block cluster (up to 16
+// CTAs on 16 SMs) runs the whole lower part of the V-cycle from the
+// restricted right-hand side at level l0 to the correction at level l0 --
+// Chebyshev smoothing, residuals, restrictions, the dense coarsest solve and
+// the prolongations, the same operations in the same order as the per-level
+// kernels -- with hardware cluster barriers between the steps and every
+// vector in global memory (L2-resident at these sizes).
+template <class T>
+struct CoarseArgs {
+    int l0, L, deg_pre, deg_post;
+    int nrow[kMaxLevels];                 // block rows (nodes) per level
+    const int *Arp[kMaxLevels], *Aci[kMaxLevels], *Rrp[kMaxLevels], *Rci[kMaxLevels], *Prp[kMaxLevels],
+        *Pci[kMaxLevels];
+    const T *A[kMaxLevels], *R[kMaxLevels], *P[kMaxLevels], *dinv[kMaxLevels];
+    T *x[kMaxLevels], *b[kMaxLevels], *r[kMaxLevels], *d[kMaxLevels], *d2[kMaxLevels], *t[kMaxLevels];
+    const double* rho;                    // safety-scaled bounds, one per level
+    const double* cinv;                   // coarsest dense inverse
+    int ncoarse;
+    double cr[16], cq[16];
+};
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ int cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return (int)r;
+}
+__device__ __forceinline__ int cluster_size() {
+    uint32_t n;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(n));
+    return (int)n;
+}
+
+// y = A x / y = b - A x / y += A x (mode 0/1/2) for 6x6 blocks over the cluster
+template <class T>
+__device__ __forceinline__ void cl_bsr66(int g0, int gs, int nrows, const int* __restrict__ rp,
+                                         const int* __restrict__ ci, const T* __restrict__ A, const T* x, T* y,
+                                         const T* b, int mode) {
+    for (int o = g0; o < nrows * 6; o += gs) {
+        const int row = o / 6, q = o - row * 6;
+        const int r0 = rp[row], nb = rp[row + 1] - r0;
+        const T* Ar = A + (size_t)r0 * 36;
+        T s = T(0);
+        for (int sl = 0; sl < nb; sl++) {
+            const int j = ci[r0 + sl];
+#pragma unroll
+            for (int dd = 0; dd < 6; dd++) s += Ar[(size_t)(q * 6 + dd) * nb + sl] * x[6L * j + dd];
+        }
+        if (mode == 0) y[o] = s;
+        else if (mode == 1) y[o] = b[o] - s;
+        else y[o] += s;
+    }
+    cluster_sync_all();
+}
+
+template <class T>
+__device__ void cl_smooth(const CoarseArgs<T>& a, int g0, int gs, int l, bool zero_init) {
+    const int n = a.nrow[l] * 6;
+    const T* dinv = a.dinv[l];
+    T *x = a.x[l], *b = a.b[l], *r = a.r[l];
+    T *dc = a.d[l], *dn = a.d2[l];
+    const double rho = a.rho[l];
+    const int deg = zero_init ? a.deg_pre : a.deg_post;
+    if (!zero_init) cl_bsr66<T>(g0, gs, a.nrow[l], a.Arp[l], a.Aci[l], a.A[l], x, r, b, 1);
+    const T it = T(1.0 / (0.6 * rho));
+    for (int i = g0; i < n; i += gs) {
+        if (zero_init) {
+            const T bi = b[i];
+            r[i] = bi;
+            const T v = dinv[i] * bi * it;
+            dc[i] = v;
+            x[i] = v;
+        } else {
+            const T v = dinv[i] * r[i] * it;
+            dc[i] = v;
+            x[i] += v;
+        }
+    }
+    cluster_sync_all();
+    for (int k = 1; k < deg && k < 16; k++) {
+        cl_bsr66<T>(g0, gs, a.nrow[l], a.Arp[l], a.Aci[l], a.A[l], dc, a.t[l], nullptr, 0);
+        const T c2 = T(a.cq[k] / (0.5 * rho)), c1 = T(a.cr[k]);
+        for (int i = g0; i < n; i += gs) {
+            const T rn = r[i] - a.t[l][i];
+            const T v = c1 * dc[i] + c2 * dinv[i] * rn;
+            r[i] = rn;
+            dn[i] = v;
+            x[i] += v;
+        }
+        cluster_sync_all();
+        T* tmp = dc;
+        dc = dn;
+        dn = tmp;
+    }
+}
+
+// launched as exactly one cluster
+template <class T>
+__global__ void __launch_bounds__(512) k_coarse_cycle(CoarseArgs<T> a) {
+    const int g0 = cluster_rank() * blockDim.x + threadIdx.x, gs = cluster_size() * blockDim.x;
+    for (int l = a.l0; l < a.L; l++) {
+        cl_smooth<T>(a, g0, gs, l, true);
+        cl_bsr66<T>(g0, gs, a.nrow[l], a.Arp[l], a.Aci[l], a.A[l], a.x[l], a.t[l], a.b[l], 1);
+        cl_bsr66<T>(g0, gs, a.nrow[l + 1], a.Rrp[l], a.Rci[l], a.R[l], a.t[l], a.b[l + 1], nullptr, 0);
+    }
+    {
+        const int n = a.ncoarse;
+        const T* bL = a.b[a.L];
+        T* xL = a.x[a.L];
+        for (int i = g0; i < n; i += gs) {
+            double s = 0.0;
+            for (int j = 0; j < n; j++) s += a.cinv[(size_t)i * n + j] * (double)bL[j];
+            xL[i] = T(s);
+        }
+        cluster_sync_all();
+    }
+    for (int l = a.L - 1; l >= a.l0; l--) {
+        cl_bsr66<T>(g0, gs, a.nrow[l], a.Prp[l], a.Pci[l], a.P[l], a.x[l + 1], a.x[l], nullptr, 2);
+        cl_smooth<T>(a, g0, gs, l, false);
+    }
+}
+
+// one cluster of up to 16 CTAs (8 where 16 cannot be co-scheduled)
+template <class T>
+static int launch_coarse_cycle(Ctx& c, const CoarseArgs<T>& a) {
+    auto kern = k_coarse_cycle<T>;
+    static int csize_cache[2] = {0, 0};
+    int& csize = csize_cache[std::is_same<T, double>::value ? 1 : 0];
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    cfg.blockDim = dim3(512, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c.s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    if (csize == 0) {
+        csize = 8;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+            int nclusters = 0;
+            cfg.gridDim = dim3(16, 1, 1);
+            attr[0].val.clusterDim.x = 16;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) == cudaSuccess && nclusters >= 1) csize = 16;
+        }
+        cudaGetLastError();
+    }
+    cfg.gridDim = dim3(csize, 1, 1);
+    attr[0].val.clusterDim.x = csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    TCK(cudaLaunchKernelEx(&cfg, kern, a));
+    note_launch();
+    return 0;
+}
+
 // ----------------------------------------------------------------- host orchestration
 template <class T>
 static AmgVals<T>& vals(Ctx& c);
@@ -1193,6 +1354,14 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
     return 0;
 }
 
+// first level (>= 1) small enough for the one-cluster lower V-cycle, or -1
+static int coarse_cta_level(const Ctx& c) {
+    if (!c.p.amg_coarse_cta) return -1;
+    for (int l = 1; l < c.nlev; l++)
+        if (c.dl[l].bs == 6 && (long)c.dl[l].ndof <= 8192) return l;
+    return -1;
+}
+
 template <class T>
 static int vcycle(Ctx& c, const T* b0, T* x0) {
     AmgVals<T>& v = vals<T>(c);
@@ -1203,7 +1372,10 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
     bl[0] = b0;
     xl[0] = x0;
     cudaEvent_t ecoarse = nullptr;
-    for (int l = 0; l < L; l++) {
+    // levels l0..L run in one CTA (k_coarse_cycle); above them, per-level kernels
+    const int l0 = coarse_cta_level(c);
+    const int ldown = l0 > 0 ? l0 : L;
+    for (int l = 0; l < ldown; l++) {
         AmgDevLevel& D = c.dl[l];
         TRET(smooth<T>(c, l, bl[l], xl[l], true));
         if (half_level<T>(c, l)) {
@@ -1223,12 +1395,46 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
         else TRET((spmv<T, 6, 6>(c, D.R, v.R[l].p, v.t[l].p, v.b[l + 1].p, nullptr, 0)));
         if (l == 0) prof_begin(c, PS_VC_COARSE, &ecoarse);
     }
-    {
+    if (l0 > 0) {
+        CoarseArgs<T> a{};
+        a.l0 = l0;
+        a.L = L;
+        const int dc = c.p.cheb_degree_coarse;
+        a.deg_pre = std::max(1, dc > 0 ? dc : c.p.cheb_degree);
+        a.deg_post = std::max(1, dc > 0 ? dc : (c.p.cheb_degree_post > 0 ? c.p.cheb_degree_post : c.p.cheb_degree));
+        for (int l = l0; l <= L; l++) {
+            AmgDevLevel& D = c.dl[l];
+            a.nrow[l] = D.nnode;
+            a.Arp[l] = D.A.rp.p;
+            a.Aci[l] = D.A.ci.p;
+            a.A[l] = v.A[l].p;
+            a.dinv[l] = v.dinv[l].p;
+            a.x[l] = v.x[l].p;
+            a.b[l] = v.b[l].p;
+            a.r[l] = v.r[l].p;
+            a.d[l] = v.d[l].p;
+            a.d2[l] = v.d2[l].p;
+            a.t[l] = v.t[l].p;
+            if (l < L) {
+                a.Rrp[l] = D.R.rp.p;
+                a.Rci[l] = D.R.ci.p;
+                a.R[l] = v.R[l].p;
+                a.Prp[l] = D.P.rp.p;
+                a.Pci[l] = D.P.ci.p;
+                a.P[l] = v.P[l].p;
+            }
+        }
+        a.rho = c.rho.p + 2 * kMaxLevels;
+        a.cinv = c.cinv.p;
+        a.ncoarse = c.dl[L].ndof;
+        cheb_coeffs(16, a.cr, a.cq);
+        TRET(launch_coarse_cycle<T>(c, a));
+    } else {
         const int n = c.dl[L].ndof;
         k_dense_apply<T><<<(n * 32 + 255) / 256, 256, 0, c.s>>>(n, c.cinv.p, v.b[L].p, v.x[L].p), note_launch();
         TCK(cudaGetLastError());
     }
-    for (int l = L - 1; l >= 0; l--) {
+    for (int l = ldown - 1; l >= 0; l--) {
         AmgDevLevel& D = c.dl[l];
         if (l == 0) prof_end(c, PS_VC_COARSE, ecoarse);
         if (half_level<T>(c, l))  // x^ += D^1/2 P e

@@ -411,25 +411,43 @@ __device__ __forceinline__ double case_warp_sum(double v) {
     return v;
 }
 
-// part[blk][j][case] = sum_i V_j[i] w[i] over this block's entries
+// part[blk][j][case] = sum_i V_j[i] w[i] over this block's entries.  Two
+// consecutive entries (cases c, c+1) per thread and 16-byte load; lanes
+// with the same case pair combine by xor shuffles of offsets >= KB/2.
+template <int KB>
+__device__ __forceinline__ double case2_warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o >= KB / 2; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
 template <int NV, int KB>
 __global__ void __launch_bounds__(256) k_mdot_blk(long nf, int nv, const double* __restrict__ V, long ld,
                                                   const double* __restrict__ w, double* __restrict__ part) {
     __shared__ double sm[8][NV * KB];
-    double acc[NV];
+    double acc[NV][2];
 #pragma unroll
-    for (int j = 0; j < NV; j++) acc[j] = 0.0;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nf; i += (long)gridDim.x * blockDim.x) {
-        const double wi = w[i];
+    for (int j = 0; j < NV; j++) acc[j][0] = acc[j][1] = 0.0;
+    const long n2 = nf >> 1;
+    const double2* w2 = reinterpret_cast<const double2*>(w);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n2; i += (long)gridDim.x * blockDim.x) {
+        const double2 wi = w2[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
-            if (j < nv) acc[j] += V[j * ld + i] * wi;
+            if (j < nv) {
+                const double2 v = reinterpret_cast<const double2*>(V + j * ld)[i];
+                acc[j][0] += v.x * wi.x;
+                acc[j][1] += v.y * wi.y;
+            }
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int c0 = (2 * lane) % KB;
 #pragma unroll
     for (int j = 0; j < NV; j++) {
-        const double s = case_warp_sum<KB>(acc[j]);
-        if (lane < KB && j < nv) sm[wid][j * KB + lane] = s;
+        const double s0 = case2_warp_sum<KB>(acc[j][0]), s1 = case2_warp_sum<KB>(acc[j][1]);
+        if (lane < KB / 2 && j < nv) {
+            sm[wid][j * KB + c0] = s0;
+            sm[wid][j * KB + c0 + 1] = s1;
+        }
     }
     __syncthreads();
     for (int t = threadIdx.x; t < nv * KB; t += blockDim.x) {
@@ -447,19 +465,30 @@ __global__ void __launch_bounds__(256) k_orth_blk(long nf, int nv, const double*
     __shared__ double sm[8][KB];
     for (int t = threadIdx.x; t < nv * KB; t += blockDim.x) hs[t] = h[t];
     __syncthreads();
-    const int cs = threadIdx.x % KB;
-    double nrm = 0.0;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nf; i += (long)gridDim.x * blockDim.x) {
-        double wi = w[i];
+    const int c0 = (2 * threadIdx.x) % KB;
+    double n0 = 0.0, n1 = 0.0;
+    const long n2 = nf >> 1;
+    double2* w2 = reinterpret_cast<double2*>(w);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n2; i += (long)gridDim.x * blockDim.x) {
+        double2 wi = w2[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
-            if (j < nv) wi -= hs[j * KB + cs] * V[j * ld + i];
-        w[i] = wi;
-        nrm += wi * wi;
+            if (j < nv) {
+                const double2 v = reinterpret_cast<const double2*>(V + j * ld)[i];
+                wi.x -= hs[j * KB + c0] * v.x;
+                wi.y -= hs[j * KB + c0 + 1] * v.y;
+            }
+        w2[i] = wi;
+        n0 += wi.x * wi.x;
+        n1 += wi.y * wi.y;
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    nrm = case_warp_sum<KB>(nrm);
-    if (lane < KB) sm[wid][lane] = nrm;
+    n0 = case2_warp_sum<KB>(n0);
+    n1 = case2_warp_sum<KB>(n1);
+    if (lane < KB / 2) {
+        sm[wid][c0] = n0;
+        sm[wid][c0 + 1] = n1;
+    }
     __syncthreads();
     if (threadIdx.x < KB) {
         double s = 0.0;
@@ -609,7 +638,7 @@ constexpr int kRedBlocksB = 1184;
 template <int KB>
 static int mdot_blk(Ctx& c, int nv, const double* V, long ld, const double* w, double* out) {
     const long nf = (long)c.ndof * KB;
-    constexpr int CH = KB >= 16 ? 16 : 32;
+    constexpr int CH = KB >= 16 ? 8 : 16;
     for (int j0 = 0; j0 < nv; j0 += CH) {
         const int k = std::min(CH, nv - j0);
         const double* Vj = V + (size_t)j0 * ld;
@@ -625,7 +654,7 @@ static int mdot_blk(Ctx& c, int nv, const double* V, long ld, const double* w, d
 template <int KB>
 static int orth_blk(Ctx& c, int nv, const double* V, long ld, const double* h, double* w, double* nrm_out) {
     const long nf = (long)c.ndof * KB;
-    constexpr int CH = KB >= 16 ? 16 : 32;
+    constexpr int CH = KB >= 16 ? 8 : 16;
     for (int j0 = 0; j0 < nv; j0 += CH) {
         const int k = std::min(CH, nv - j0);
         const double* Vj = V + (size_t)j0 * ld;

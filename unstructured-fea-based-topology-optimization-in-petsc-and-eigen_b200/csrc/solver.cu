@@ -354,7 +354,7 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
                        (uint64_t)(uintptr_t)c.dsc.p, (uint64_t)(uintptr_t)c.hsc.h, (uint64_t)(uintptr_t)c.Ee64.p,
                        (uint64_t)(uintptr_t)c.v32.A0s.p, (uint64_t)(uintptr_t)c.v64.A0s.p,
                        (uint64_t)(uintptr_t)c.h0.S.p, (uint64_t)c.p.amg_half_fine, (uint64_t)(uintptr_t)c.cinv.p, (uint64_t)(uintptr_t)c.rho.p, (uint64_t)c.p.precision,
-                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.p.fine_smoother_matfree,
+                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.p.amg_coarse_cta, (uint64_t)c.p.fine_smoother_matfree,
                        (uint64_t)n})
         sig = sig_mix(sig, v);
     StepGraphs& G = c.graphs;
