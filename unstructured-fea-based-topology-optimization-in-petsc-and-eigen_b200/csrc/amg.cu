@@ -40,7 +40,8 @@ template <class T, int NEN>
 __global__ void k_assemble_A0(int nn, const int* __restrict__ n2e_ptr, const int* __restrict__ n2e,
                               const uint16_t* __restrict__ bpos, const T* __restrict__ ke, const T* __restrict__ Ee,
                               const int* __restrict__ rp, const int* __restrict__ ci,
-                              const unsigned char* __restrict__ dfix, T* __restrict__ A, int maxdeg) {
+                              const unsigned char* __restrict__ dfix, T* __restrict__ A, int maxdeg,
+                              T* __restrict__ S, const int* __restrict__ sp) {
     constexpr int ND = 3 * NEN, NPK = ND * (ND + 1) / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -74,6 +75,8 @@ __global__ void k_assemble_A0(int nn, const int* __restrict__ n2e_ptr, const int
         const bool rf = dfix[3L * i + cc], cf = dfix[3L * j + d];
         if (rf || cf) v = (rf && j == i && cc == d) ? T(1) : T(0);
         A[(size_t)r0 * 9 + idx] = v;
+        // the smoother's sliced-ELLPACK copy (its padding stays zero)
+        if (S) S[sell_idx<T>((size_t)(sp[i >> 5] >> 5) + slot, ent, i & 31)] = v;
     }
 }
 
@@ -185,22 +188,9 @@ __global__ void k_bsr_cheb(int nrows, const int* __restrict__ rp, const int* __r
 
 // ----------------------------------------------------------------- level-0 sliced ELLPACK
 // One thread per node row; block k of the rows of slice s is entry
-// sp[s] + 32k + lane, its 9 values sit at ((sp[s]/32 + k)*9 + e)*32 + lane, so
-// every value and column-id load of a warp is one contiguous line.
-template <class T>
-__global__ void k_bsr_to_sell(int nrows, int nslices, const int* __restrict__ rp, const int* __restrict__ sp,
-                              const T* __restrict__ A, T* __restrict__ S) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = i >> 5, lane = i & 31;
-    if (s >= nslices) return;
-    const int base = sp[s] >> 5, w = (sp[s + 1] - sp[s]) >> 5;
-    int r0 = 0, nb = 0;
-    if (i < nrows) { r0 = rp[i]; nb = rp[i + 1] - r0; }
-    for (int k = 0; k < w; k++)
-#pragma unroll
-        for (int e = 0; e < 9; e++) S[sell_idx<T>(base + k, e, lane)] = k < nb ? A[(size_t)r0 * 9 + e * nb + k] : T(0);
-}
-
+// sp[s] + 32k + lane (column ids: one contiguous line per warp), its 9
+// values in slot sp[s]/32 + k of the value array (sell_idx: two 16-byte
+// vectors and one scalar per row, each a coalesced run over the warp).
 // mode 0: y = A x; 1: y = b - A x; 3: y = sigma Dinv A x
 template <class T>
 __global__ void __launch_bounds__(256) k_sell_spmv(int nrows, const int* __restrict__ sp, const int* __restrict__ sci,
@@ -421,152 +411,8 @@ __global__ void k_cheb_upd(long n, const T* __restrict__ t, T* __restrict__ r, T
 }
 
 // ----------------------------------------------------------------- fixed-pattern SpGEMM
-// C = A * B, blocks A: BR x BK, B: BK x BC, C: BR x BC.  One warp per C row;
-// the row's column ids and an accumulator live in shared memory; lanes walk
-// the blocks of each B row (distinct columns, so no two lanes of one step
-// touch the same accumulator slot) and find their slot by binary search.
-template <class T, int BR, int BK, int BC>
-__global__ void k_spgemm(int nrows, const int* __restrict__ Arp, const int* __restrict__ Aci, const T* __restrict__ A,
-                         const int* __restrict__ Brp, const int* __restrict__ Bci, const T* __restrict__ B,
-                         const int* __restrict__ Crp, const int* __restrict__ Cci, T* __restrict__ C, int maxC) {
-    constexpr int BRK = BR * BK, BKC = BK * BC, BRC = BR * BC;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * (blockDim.x >> 5) + wib;
-    if (i >= nrows) return;
-    const size_t accb = ((size_t)maxC * BRC * sizeof(T) + 15) & ~(size_t)15;
-    const size_t per = accb + (((size_t)maxC * sizeof(int) + 15) & ~(size_t)15);
-    unsigned char* base = smem_raw + wib * per;
-    T* acc = reinterpret_cast<T*>(base);
-    int* cci = reinterpret_cast<int*>(base + accb);
-    const int c0 = Crp[i], nC = Crp[i + 1] - c0;
-    for (int s = lane; s < nC; s += 32) cci[s] = Cci[c0 + s];
-    for (int q = lane; q < BRC * maxC; q += 32) acc[q] = T(0);
-    __syncwarp();
-    const int a0 = Arp[i], nA = Arp[i + 1] - a0;
-    for (int a = 0; a < nA; a++) {
-        const int k = Aci[a0 + a];
-        T ab[BRK];
-#pragma unroll
-        for (int e = 0; e < BRK; e++) ab[e] = A[(size_t)a0 * BRK + e * nA + a];
-        const int b0 = Brp[k], nB = Brp[k + 1] - b0;
-        for (int s = lane; s < nB; s += 32) {
-            const int J = Bci[b0 + s];
-            int lo = 0, hi = nC - 1;
-            while (lo < hi) {
-                int mid = (lo + hi) >> 1;
-                if (cci[mid] < J) lo = mid + 1;
-                else hi = mid;
-            }
-            T bb[BKC];
-#pragma unroll
-            for (int e = 0; e < BKC; e++) bb[e] = B[(size_t)b0 * BKC + e * nB + s];
-#pragma unroll
-            for (int r = 0; r < BR; r++)
-#pragma unroll
-                for (int cc = 0; cc < BC; cc++) {
-                    T v = T(0);
-#pragma unroll
-                    for (int m = 0; m < BK; m++) v += ab[r * BK + m] * bb[m * BC + cc];
-                    acc[(r * BC + cc) * maxC + lo] += v;
-                }
-        }
-        __syncwarp();
-    }
-    for (int q = lane; q < BRC * nC; q += 32) {
-        const int e = q / nC, s = q - e * nC;
-        C[(size_t)c0 * BRC + q] = acc[e * maxC + s];
-    }
-}
-
-// Same product with all (A block, B block) pairs of a row spread over the
-// lanes: chunks of 32 A blocks, a warp prefix scan of their B-row lengths,
-// then each lane takes pairs p = lane, lane+32, ... and adds its BR x BC
-// product into the shared-memory row with shared atomics.  Balanced for any
-// mix of short rows (A * Pt: one B block per A block) and long ones (R * AP).
-template <class T, int BR, int BK, int BC>
-__global__ void k_spgemm_pairs(int nrows, const int* __restrict__ Arp, const int* __restrict__ Aci,
-                               const T* __restrict__ A, const int* __restrict__ Brp, const int* __restrict__ Bci,
-                               const T* __restrict__ B, const int* __restrict__ Crp, const int* __restrict__ Cci,
-                               T* __restrict__ C, int maxC) {
-    constexpr int BRK = BR * BK, BKC = BK * BC, BRC = BR * BC;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * (blockDim.x >> 5) + wib;
-    if (i >= nrows) return;
-    const size_t accb = ((size_t)maxC * BRC * sizeof(T) + 15) & ~(size_t)15;
-    const size_t per = accb + (((size_t)maxC * sizeof(int) + 15) & ~(size_t)15) + 3 * 32 * sizeof(int);
-    unsigned char* base = smem_raw + wib * per;
-    T* acc = reinterpret_cast<T*>(base);
-    int* cci = reinterpret_cast<int*>(base + accb);
-    int* sp = reinterpret_cast<int*>(base + per - 3 * 32 * sizeof(int));
-    int* sb = sp + 32;
-    int* sl = sp + 64;
-    const int c0 = Crp[i], nC = Crp[i + 1] - c0;
-    for (int s = lane; s < nC; s += 32) cci[s] = Cci[c0 + s];
-    for (int q = lane; q < BRC * maxC; q += 32) acc[q] = T(0);
-    const int a0 = Arp[i], nA = Arp[i + 1] - a0;
-    for (int ab = 0; ab < nA; ab += 32) {
-        const int a = ab + lane;
-        int len = 0, kb = 0;
-        if (a < nA) {
-            const int k = Aci[a0 + a];
-            kb = Brp[k];
-            len = Brp[k + 1] - kb;
-        }
-        int incl = len;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        __syncwarp();
-        sp[lane] = incl - len;
-        sb[lane] = kb;
-        sl[lane] = len;
-        __syncwarp();
-        for (int p = lane; p < total; p += 32) {
-            int lo = 0, hi = 31;  // last q with sp[q] <= p (always a non-empty lane)
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (sp[mid] <= p) lo = mid;
-                else hi = mid - 1;
-            }
-            const int q = lo, s = p - sp[q], bq = sb[q], nB = sl[q], aa = ab + q;
-            const int J = Bci[bq + s];
-            int l2 = 0, h2 = nC - 1;
-            while (l2 < h2) {
-                int mid = (l2 + h2) >> 1;
-                if (cci[mid] < J) l2 = mid + 1;
-                else h2 = mid;
-            }
-            T abk[BRK], bbk[BKC];
-#pragma unroll
-            for (int e = 0; e < BRK; e++) abk[e] = A[(size_t)a0 * BRK + e * nA + aa];
-#pragma unroll
-            for (int e = 0; e < BKC; e++) bbk[e] = B[(size_t)bq * BKC + e * nB + s];
-#pragma unroll
-            for (int r = 0; r < BR; r++)
-#pragma unroll
-                for (int cc = 0; cc < BC; cc++) {
-                    T v = T(0);
-#pragma unroll
-                    for (int m = 0; m < BK; m++) v += abk[r * BK + m] * bbk[m * BC + cc];
-                    atomicAdd(&acc[(r * BC + cc) * maxC + l2], v);
-                }
-        }
-        __syncwarp();
-    }
-    __syncwarp();
-    for (int q = lane; q < BRC * nC; q += 32) {
-        const int e = q / nC, s = q - e * nC;
-        C[(size_t)c0 * BRC + q] = acc[e * maxC + s];
-    }
-}
-
-// The same product from its plan (output-stationary): G lanes per C row, a
-// lane owns one C block at a time and sums its contributing (A block,
+// C = A * B with blocks A: BR x BK, B: BK x BC, C: BR x BC, from the
+// product's plan (output-stationary): G lanes per C row, a lane owns one C block at a time and sums its contributing (A block,
 // B block) pairs in registers: no shared memory, no atomics, no searches,
 // and the C block's entries are written as coalesced runs.
 template <class T, int BR, int BK, int BC, int G>
@@ -978,7 +824,10 @@ static int alloc_vals(Ctx& c) {
         TRET(v.t[l].alloc(D.ndof));
         TRET(v.pv[l].alloc(D.ndof));
         TRET(v.pw[l].alloc(D.ndof));
-        if (l == 0) TRET(v.A0s.alloc((size_t)D.sell_blocks * 9));
+        if (l == 0) {
+            TRET(v.A0s.alloc((size_t)D.sell_blocks * 9));
+            TRET(v.A0s.zero(c.s));  // padding slots are never written
+        }
         if (l + 1 < c.nlev) {
             TRET(v.P[l].alloc((size_t)D.P.nnzb * bs * 6));
             TRET(v.T_[l].alloc((size_t)D.P.nnzb * bs * 6));
@@ -1022,24 +871,6 @@ static int spgemm_plan(Ctx& c, const DevPattern& Ap, const T* A, const DevPatter
     else if (pl.avg_row > 6) spgemm_plan_g<BR, BK, BC, T, 8>(c, Ap, A, Bp, B, Cp, C, pl);
     else spgemm_plan_g<BR, BK, BC, T, 4>(c, Ap, A, Bp, B, Cp, C, pl);
     note_launch();
-    TCK(cudaGetLastError());
-    return 0;
-}
-
-template <int BR, int BK, int BC, class T>
-static int spgemm(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp, const T* B, const DevPattern& Cp,
-                  T* C) {
-    const size_t mc = (size_t)std::max(Cp.maxrow, 1);
-    const size_t per = ((mc * BR * BC * sizeof(T) + 15) & ~(size_t)15) + ((mc * sizeof(int) + 15) & ~(size_t)15) +
-                       3 * 32 * sizeof(int);
-    int warps = (int)std::min<size_t>(8, std::max<size_t>(1, (200 * 1024) / per));
-    const size_t smem = per * warps;
-    if (smem > 227 * 1024) { set_error("SpGEMM row too long for shared memory (%d blocks)", Cp.maxrow); return TOPO_ERR_UNSUPPORTED; }
-    auto kern = k_spgemm_pairs<T, BR, BK, BC>;
-    TCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = (Cp.nrows + warps - 1) / warps;
-    kern<<<grid, warps * 32, smem, c.s>>>(Cp.nrows, Ap.rp.p, Ap.ci.p, A, Bp.rp.p, Bp.ci.p, B, Cp.rp.p, Cp.ci.p, C,
-                                          std::max(Cp.maxrow, 1)), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -1154,27 +985,23 @@ static int numeric(Ctx& c) {
         const int wpb = 4;
         const size_t smem = (size_t)wpb * c.maxdeg * 9 * sizeof(T);
         const int grid = (c.nn + wpb - 1) / wpb;
+        // the sliced-ELLPACK copy of the level-0 operator for the smoother is
+        // written by the same pass (the mixed single-load form with the FP16
+        // scaled copy built below does not need it)
+        c.h0.valid = false;
+        T* sell = (std::is_same<T, float>::value && use_half0(c)) ? nullptr : v.A0s.p;
         if (c.nen == 8) {
             auto k = k_assemble_A0<T, 8>;
             TCK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, ke, Ee, D.A.rp.p, D.A.ci.p,
-                                              c.dof_fixed.p, v.A[0].p, c.maxdeg), note_launch();
+                                              c.dof_fixed.p, v.A[0].p, c.maxdeg, sell, D.sell_ptr.p), note_launch();
         } else {
             auto k = k_assemble_A0<T, 4>;
             TCK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, ke, Ee, D.A.rp.p, D.A.ci.p,
-                                              c.dof_fixed.p, v.A[0].p, c.maxdeg), note_launch();
+                                              c.dof_fixed.p, v.A[0].p, c.maxdeg, sell, D.sell_ptr.p), note_launch();
         }
         TCK(cudaGetLastError());
-        // sliced-ELLPACK copy of the level-0 operator for the smoother (the
-        // mixed single-load form uses the FP16 scaled copy built below)
-        AmgDevLevel& D0 = c.dl[0];
-        c.h0.valid = false;
-        if (!(std::is_same<T, float>::value && use_half0(c))) {
-            k_bsr_to_sell<T><<<D0.nslices * 32 / 256 + 1, 256, 0, c.s>>>(D0.nnode, D0.nslices, D0.A.rp.p,
-                                                                         D0.sell_ptr.p, v.A[0].p, v.A0s.p), note_launch();
-            TCK(cudaGetLastError());
-        }
     }
     prof_end(c, PS_SETUP_ASM, pe);
     for (int l = 0; l < c.nlev; l++) {
