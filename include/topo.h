@@ -83,6 +83,8 @@ typedef struct topo_params {
     int cheb_degree_coarse; /* Chebyshev degree below the finest level (0: as the finest; default 4:
                                the coarse levels are small and latency-bound, and stronger
                                smoothing there cuts FGMRES iterations by about a quarter) */
+    int autotune;          /* 1 (default): time candidate launch shapes of the hot kernels on
+                              this context's own data at its first solve and keep the fastest */
     int amg_coarse_cta;    /* 1: the V-cycle below the first level with <= 8192 DOFs runs in one
                               thread-block cluster (one launch instead of one per sweep); 0 (default):
                               per-sweep kernels, which measured faster at 392k under graph replay */
@@ -100,6 +102,8 @@ typedef struct topo_solve_info {
     int mma_inner_its;     /* dual interior-point steps of the last update */
     double last_fx, last_gx0, last_ch;
     double t_fem_ms, t_filter_ms, t_mma_ms, t_setup_ms; /* stage times (CUDA events) */
+    int tuned[4];          /* launch shapes picked by the autotuner: element-operator block,
+                              level-0 smoother block, reduction grid, block-operator CTAs/SM */
 } topo_solve_info;
 
 /* ---------------------------------------------------------------- basics */

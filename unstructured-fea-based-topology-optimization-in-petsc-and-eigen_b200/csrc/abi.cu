@@ -284,6 +284,7 @@ void topo_params_default(topo_params* p) {
     p->cheb_degree_coarse = 4;
     p->amg_half_fine = 0;
     p->amg_coarse_cta = 0;
+    p->autotune = 1;
 }
 
 int topo_device_alloc(size_t bytes, void** ptr) {

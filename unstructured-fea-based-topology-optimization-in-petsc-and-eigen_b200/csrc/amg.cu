@@ -941,7 +941,8 @@ static int level_spmv(Ctx& c, int l, const T* x, T* y, const T* b, int mode, con
         cudaEvent_t e0;
         const bool rec = mode == 1;
         if (rec) prof_begin(c, PS_RES0, &e0);
-        k_sell_spmv<T><<<(D.nnode + 255) / 256, 256, 0, c.s>>>(D.nnode, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, x, y, b,
+        const int sb = c.tune.sell_block;
+        k_sell_spmv<T><<<(D.nnode + sb - 1) / sb, sb, 0, c.s>>>(D.nnode, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, x, y, b,
                                                                mode, dinv, scal), note_launch();
         if (rec) prof_end(c, PS_RES0, e0);
         TCK(cudaGetLastError());
@@ -1159,7 +1160,8 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
             if (l == 0) {
                 cudaEvent_t e0;
                 prof_begin(c, PS_CHEB0, &e0);
-                k_sell_cheb<T><<<(nrows + 255) / 256, 256, 0, c.s>>>(nrows, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, dcur,
+                k_sell_cheb<T><<<(nrows + c.tune.sell_block - 1) / c.tune.sell_block, c.tune.sell_block, 0, c.s>>>(
+                    nrows, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, dcur,
                                                                      dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr[k],
                                                                      cq[k]), note_launch();
                 prof_end(c, PS_CHEB0, e0);
@@ -1338,6 +1340,18 @@ int amg_level_copy(Ctx& c, int l, int which, std::vector<double>& vals_out, std:
     TCK(cudaMemcpy(rp.data(), pat->rp.p, sizeof(int) * (nrows + 1), cudaMemcpyDeviceToHost));
     TCK(cudaMemcpy(ci.data(), pat->ci.p, sizeof(int) * pat->nnzb, cudaMemcpyDeviceToHost));
     return 0;
+}
+
+// y = A0 x with the level-0 smoother's operator (sliced ELLPACK, current
+// precision); -1 when the FP16 scaled copy replaces it.  Used to time launch
+// shapes.
+int amg_level0_apply(Ctx& c, const void* x, void* y) {
+    if (c.p.precision == TOPO_PREC_MIXED) {
+        if (half_level<float>(c, 0) || !c.v32.allocated) return -1;
+        return level_spmv<float>(c, 0, static_cast<const float*>(x), static_cast<float*>(y), nullptr, 0);
+    }
+    if (!c.v64.allocated) return -1;
+    return level_spmv<double>(c, 0, static_cast<const double*>(x), static_cast<double*>(y), nullptr, 0);
 }
 
 int amg_numeric(Ctx& c) {

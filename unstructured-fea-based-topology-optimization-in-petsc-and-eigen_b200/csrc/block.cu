@@ -536,7 +536,8 @@ static int launch_blk(Ctx& c, const TU* u, double* y, double alpha, double* uku)
     int dev = 0, nsm = 148;
     TCK(cudaGetDevice(&dev));
     TCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const int grid = std::max(1, std::min(B.nchunks, std::max(1, occ) * nsm));
+    const int per_sm = c.tune.blk_ctas > 0 ? std::min(std::max(1, occ), c.tune.blk_ctas) : std::max(1, occ);
+    const int grid = std::max(1, std::min(B.nchunks, per_sm * nsm));
     BlkArgs a{B.nchunks, B.ch_ph.p, B.ph_sl.p, B.ch_np.p, B.ch_nodes.p, B.sl_elem.p, B.sl_gn.p, B.sl_lc.p,
               B.sl_mask.p, B.keb.p, B.Es.p, B.max_nodes, B.err.p};
     kern<<<grid, kWarps * 32, smem, c.s>>>(a, u, y, alpha, uku), note_launch();

@@ -679,6 +679,45 @@ static int norms_blk(Ctx& c, const double* w, double* out) {
     return 0;
 }
 
+// Autotuning of the block operator's CTAs per SM (1 or the occupancy
+// limit), timed on this context's operator at its first block solve.
+int autotune_block(Ctx& c) {
+    BlockState& B = c.blk;
+    if (!c.p.autotune || c.tune.block_done || !B.V.p) return 0;
+    c.tune.block_done = true;
+    const long nf = (long)c.ndof * B.kb;
+    double* u = B.V.p;
+    double* y = B.V.p + nf;
+    TCK(cudaMemsetAsync(u, 0, sizeof(double) * 2 * nf, c.s));
+    const bool prof = c.prof.on;
+    c.prof.on = false;
+    cudaEvent_t e0, e1;
+    TCK(cudaEventCreate(&e0));
+    TCK(cudaEventCreate(&e1));
+    double best = 1e30;
+    int pick = 0;
+    for (int ctas : {1, 0}) {
+        c.tune.blk_ctas = ctas;
+        double t = 1e30;
+        for (int rep = 0; rep < 3; rep++) {
+            TCK(cudaEventRecord(e0, c.s));
+            TRET(blk_apply(c, u, y, nullptr, 1.0));
+            TCK(cudaEventRecord(e1, c.s));
+            TCK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            TCK(cudaEventElapsedTime(&ms, e0, e1));
+            t = std::min(t, (double)ms);
+        }
+        if (t < best) { best = t; pick = ctas; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c.tune.blk_ctas = pick;
+    c.prof.on = prof;
+    c.info.tuned[3] = pick;
+    return 0;
+}
+
 // Arnoldi step j for all cases (see the single-load step in solver.cu)
 struct BlkStepArgs {
     int j;
@@ -742,6 +781,8 @@ static int fgmres_blk(Ctx& c, const double* b, double* x, int* its_out, int* sta
     int* act = B.ik.p;
     int* kd = B.ik.p + KB;
     double* hs = B.hs.h;
+    TRET(blk_setup(c));
+    TRET(autotune_block(c));
     // the V-cycle work vectors and the slot moduli exist before any capture
     // (a captured step must not depend on host-side state that changes)
     if (mixed) TRET(alloc_bvecs<float>(c));
@@ -755,7 +796,7 @@ static int fgmres_blk(Ctx& c, const double* b, double* x, int* its_out, int* sta
                        (uint64_t)(uintptr_t)B.bv32.x[0].p, (uint64_t)(uintptr_t)B.bv64.x[0].p,
                        (uint64_t)(uintptr_t)c.v32.A0s.p, (uint64_t)(uintptr_t)c.v64.A0s.p,
                        (uint64_t)(uintptr_t)c.cinv.p, (uint64_t)(uintptr_t)c.rho.p, (uint64_t)c.p.precision,
-                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)KB, (uint64_t)nf})
+                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.tune.blk_ctas, (uint64_t)KB, (uint64_t)nf})
         sig = sig_mix(sig, v);
     StepGraphs& G = B.graphs;
     if (G.sig != sig) {

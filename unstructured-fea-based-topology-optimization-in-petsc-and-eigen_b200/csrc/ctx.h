@@ -241,6 +241,15 @@ struct Ctx {
 
     BlockState blk;
 
+    // launch shapes (autotuned at the first solve, see autotune.cu)
+    struct Tune {
+        int kmv_block = 128;        // k_kmv threads per block
+        int sell_block = 256;       // level-0 sliced-ELLPACK kernels
+        int red_blocks = 1184;      // grid of the vector reductions / Gram-Schmidt sweeps
+        int blk_ctas = 0;           // block operator CTAs per SM (0: occupancy limit)
+        bool single_done = false, block_done = false;
+    } tune;
+
     topo_solve_info info{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
@@ -309,12 +318,15 @@ int blk_check_error(Ctx& c);
 
 int amg_alloc(Ctx& c);                                             // amg.cu
 int amg_numeric(Ctx& c);
+int amg_level0_apply(Ctx& c, const void* x, void* y);
 int amg_reset_warm_start(Ctx& c);
 int amg_level_copy(Ctx& c, int l, int which, std::vector<double>& vals_out, std::vector<int>& rp, std::vector<int>& ci,
                    int& nrows, int& ncols, int& br, int& bc);
 int amg_vcycle64(Ctx& c, const double* b, double* x);
 int amg_vcycle32(Ctx& c, const double* b64, float* x);
 
+int autotune_single(Ctx& c);                                       // autotune.cu
+int autotune_block(Ctx& c);
 int fem_solve(Ctx& c, const double* xphys, double* u);             // solver.cu
 int fem_solve_block(Ctx& c, const double* xphys, double* u);       // block_solve.cu
 int filter_cg(Ctx& c, const double* b, double* x, int* its);

@@ -398,7 +398,7 @@ __global__ void k_fix_rows(int nf, const int* __restrict__ fixed, const TU* __re
 
 template <class TK, class TU, class TY>
 static int launch_kmv(Ctx& c, const TK* ke, const TK* Ee, const TU* u, TY* y, TK alpha) {
-    int block = 128, grid = c.ntiles * 32 / block + 1;
+    const int block = c.tune.kmv_block, grid = c.ntiles * 32 / block + 1;
     if (c.nen == 8)
         k_kmv<8, TK, TU, TY><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, y, alpha), note_launch();
     else

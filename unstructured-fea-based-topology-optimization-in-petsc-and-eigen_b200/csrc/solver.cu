@@ -18,6 +18,7 @@ namespace topo {
 int kmatvec64r(Ctx& c, const double* u, double* y, const double* b);
 
 constexpr int kRedBlocks = 1184;  // 8 x 148 SMs: enough warps in flight for the vector sweeps
+constexpr int kRedMax = 4736;     // largest reduction grid the autotuner tries
 
 // ----------------------------------------------------------------- reductions
 __global__ void k_dot(long n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ part) {
@@ -141,11 +142,12 @@ static int mdot(Ctx& c, int nv, const double* V, long ld, const double* w, doubl
     for (int j0 = 0; j0 < nv; j0 += 32) {
         const int k = std::min(32, nv - j0);
         const double* Vj = V + (size_t)j0 * ld;
-        if (k <= 8) k_mdot<8><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
-        else if (k <= 16) k_mdot<16><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
-        else k_mdot<32><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
+        const int g = c.tune.red_blocks;
+        if (k <= 8) k_mdot<8><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
+        else if (k <= 16) k_mdot<16><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
+        else k_mdot<32><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
         TCK(cudaGetLastError());
-        TRET(finalize_sum(c, c.red.p, kRedBlocks, k, out + j0));
+        TRET(finalize_sum(c, c.red.p, g, k, out + j0));
     }
     return 0;
 }
@@ -154,12 +156,12 @@ static int orth(Ctx& c, int nv, const double* V, long ld, const double* h, doubl
     for (int j0 = 0; j0 < nv; j0 += 32) {
         const int k = std::min(32, nv - j0);
         const double* Vj = V + (size_t)j0 * ld;
-        if (k <= 8) k_orth<8><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
-        else if (k <= 16) k_orth<16><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
-        else k_orth<32><<<kRedBlocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
+        if (k <= 8) k_orth<8><<<c.tune.red_blocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
+        else if (k <= 16) k_orth<16><<<c.tune.red_blocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
+        else k_orth<32><<<c.tune.red_blocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
     }
     // the last sweep's partials hold ||w||^2 of the fully orthogonalised w
-    k_final<<<1, 32, 0, c.s>>>(kRedBlocks, 1, c.red.p, hn_out, 0), note_launch();
+    k_final<<<1, 32, 0, c.s>>>(c.tune.red_blocks, 1, c.red.p, hn_out, 0), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -171,6 +173,76 @@ static int precond_apply(Ctx& c, const double* v, int j) {
     if (c.p.precision == TOPO_PREC_MIXED) TRET(amg_vcycle32(c, v, c.Z32.p + (size_t)j * n));
     else TRET(amg_vcycle64(c, v, c.Z64.p + (size_t)j * n));
     prof_end(c, PS_VCYCLE, e0);
+    return 0;
+}
+
+// ----------------------------------------------------------------- launch-shape autotuning
+// Each candidate shape of a hot kernel is timed (best of 3, CUDA events) on
+// this context's own operator and vectors at its first solve; the fastest is
+// kept for the context's lifetime.  The timed launches write scratch rows of
+// the Krylov basis only.
+template <class F>
+static int time_best(Ctx& c, F&& fn, double* ms) {
+    cudaEvent_t e0, e1;
+    TCK(cudaEventCreate(&e0));
+    TCK(cudaEventCreate(&e1));
+    double best = 1e30;
+    for (int rep = 0; rep < 3; rep++) {
+        TCK(cudaEventRecord(e0, c.s));
+        const int rc = fn();
+        TCK(cudaEventRecord(e1, c.s));
+        TCK(cudaEventSynchronize(e1));
+        float t = 0.f;
+        TCK(cudaEventElapsedTime(&t, e0, e1));
+        if (rc < 0) { best = 1e30; break; }
+        best = std::min(best, (double)t);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = best;
+    return 0;
+}
+
+int autotune_single(Ctx& c) {
+    if (!c.p.autotune || c.tune.single_done || !c.V.p) return 0;
+    c.tune.single_done = true;
+    const long n = c.ndof;
+    const long ldv = (n + 31) & ~31L;
+    double* u = c.V.p;
+    double* y = c.V.p + ldv;
+    TCK(cudaMemsetAsync(u, 0, sizeof(double) * 2 * ldv, c.s));
+    const bool prof = c.prof.on;
+    c.prof.on = false;
+    double best = 1e30, t = 0.0;
+    int pick = c.tune.kmv_block;
+    for (int b : {64, 128}) {
+        c.tune.kmv_block = b;
+        TRET(time_best(c, [&]() { return kmatvec(c, c.Ee64.p, u, y, 1); }, &t));
+        if (t < best) { best = t; pick = b; }
+    }
+    c.tune.kmv_block = pick;
+    best = 1e30;
+    pick = c.tune.sell_block;
+    for (int b : {128, 256}) {
+        c.tune.sell_block = b;
+        TRET(time_best(c, [&]() { return amg_level0_apply(c, u, y); }, &t));
+        if (t < best) { best = t; pick = b; }
+    }
+    c.tune.sell_block = pick;
+    if (c.V.n >= (size_t)17 * ldv) {
+        best = 1e30;
+        pick = c.tune.red_blocks;
+        for (int g : {592, 1184, 2368, 4736}) {
+            c.tune.red_blocks = g;
+            TRET(time_best(c, [&]() { return mdot(c, 16, c.V.p, ldv, y, c.dsc.p + DS_GM); }, &t));
+            if (t < best) { best = t; pick = g; }
+        }
+        c.tune.red_blocks = pick;
+    }
+    c.prof.on = prof;
+    c.info.tuned[0] = c.tune.kmv_block;
+    c.info.tuned[1] = c.tune.sell_block;
+    c.info.tuned[2] = c.tune.red_blocks;
     return 0;
 }
 
@@ -336,12 +408,13 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
     }
     if (c.p.precision == TOPO_PREC_MIXED && !c.Z32.p) TRET(c.Z32.alloc((size_t)m * n));
     if (c.p.precision != TOPO_PREC_MIXED && !c.Z64.p) TRET(c.Z64.alloc((size_t)m * n));
-    if ((long)c.red.n < kRedBlocks * 40L) TRET(c.red.alloc(std::max<long>(kRedBlocks * 40L, 4096)));
+    if ((long)c.red.n < kRedMax * 40L) TRET(c.red.alloc(std::max<long>(kRedMax * 40L, 4096)));
     while ((int)c.gm_ev.size() < m + 1) {
         cudaEvent_t e;
         TCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         c.gm_ev.push_back(e);
     }
+    TRET(autotune_single(c));
     double* hs = c.hsc.h + 512;     // pinned: [2j, 2j+1] = (residual, ||w||) of iteration j; [300], [301] norms
     double* gm = c.dsc.p + DS_GM;   // Hessenberg column scratch
     double* st = c.wtmp.p;          // device Arnoldi state
@@ -355,6 +428,7 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
                        (uint64_t)(uintptr_t)c.v32.A0s.p, (uint64_t)(uintptr_t)c.v64.A0s.p,
                        (uint64_t)(uintptr_t)c.h0.S.p, (uint64_t)c.p.amg_half_fine, (uint64_t)(uintptr_t)c.cinv.p, (uint64_t)(uintptr_t)c.rho.p, (uint64_t)c.p.precision,
                        (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.p.amg_coarse_cta, (uint64_t)c.p.fine_smoother_matfree,
+                       (uint64_t)c.tune.kmv_block, (uint64_t)c.tune.sell_block, (uint64_t)c.tune.red_blocks,
                        (uint64_t)n})
         sig = sig_mix(sig, v);
     StepGraphs& G = c.graphs;
