@@ -115,3 +115,19 @@ def test_graph_replayed_steps_match_direct_launches(T, cuda, mesh):
         ctx.close()
     assert rel(h[1][:, 0], h[0][:, 0]) < 1e-6
     assert np.abs(h[1][:, 1] - h[0][:, 1]).max() < 1e-8
+
+
+def test_tet4_trajectory(T, O, cuda):
+    """Twenty design iterations on a tet4 mesh (6 tets per hex) against the
+    oracle; the same final-design bar as hex8."""
+    v, e, f, ld, lv = T.gen_cantilever(8, 4, 4, 4)
+    ctx = T.Context(v, e, f, ld, lv, **KW)
+    ctx.opt_init()
+    hist = ctx.opt_run(20)
+    orc = O.Oracle(v, e, f, ld, lv, **{k: x for k, x in KW.items() if k != "ch_tol"})
+    ohist, _ = orc.run(20, ch_tol=0.0)
+    relf = np.abs(hist[:, 0] - ohist[:, 0]) / np.abs(ohist[:, 0])
+    assert relf[-1] < 1e-3 and relf.max() < 5e-3, relf
+    assert np.abs(hist[:, 1] - ohist[:, 1]).max() < 1e-3
+    ctx.close()
+    orc.close()
