@@ -415,25 +415,29 @@ __global__ void k_cheb_upd(long n, const T* __restrict__ t, T* __restrict__ r, T
 // product's plan (output-stationary): G lanes per C row, a lane owns one C block at a time and sums its contributing (A block,
 // B block) pairs in registers: no shared memory, no atomics, no searches,
 // and the C block's entries are written as coalesced runs.
-template <class T, int BR, int BK, int BC, int G>
+template <class T, int BR, int BK, int BC, int GS, int PS>
 __global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __restrict__ Arp, const int* __restrict__ Aci,
                                                      const T* __restrict__ A, const int* __restrict__ Brp,
                                                      const T* __restrict__ B, const int* __restrict__ Crp,
                                                      T* __restrict__ C, const int* __restrict__ pptr,
                                                      const uint32_t* __restrict__ pr) {
-    constexpr int BRK = BR * BK, BKC = BK * BC, BRC = BR * BC;
+    // GS C blocks of a row at a time, each summed by PS lanes (long pair
+    // lists: shorter dependent-load chains), combined by xor shuffles
+    constexpr int BRK = BR * BK, BKC = BK * BC, BRC = BR * BC, G = GS * PS;
     const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    const int i = (int)(tid / G), gl = (int)(tid % G);
+    const int i = (int)(tid / G), gl = (int)(tid % G), gs = gl / PS, ps = gl % PS;
     if (i >= nrows) return;
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned gmask = PS >= 32 ? 0xffffffffu : (((1u << PS) - 1u) << (lane & ~(unsigned)(PS - 1)));
     const int a0 = Arp[i], nA = Arp[i + 1] - a0;
     const int c0 = Crp[i], nC = Crp[i + 1] - c0;
     const T* Ar = A + (size_t)a0 * BRK;
-    for (int sl = gl; sl < nC; sl += G) {
+    for (int sl = gs; sl < nC; sl += GS) {
         T acc[BRC];
 #pragma unroll
         for (int e = 0; e < BRC; e++) acc[e] = T(0);
         const int p1 = pptr[c0 + sl + 1];
-        for (int p = pptr[c0 + sl]; p < p1; p++) {
+        for (int p = pptr[c0 + sl] + ps; p < p1; p += PS) {
             const uint32_t w = __ldg(pr + p);
             const int a = (int)(w >> 16), s = (int)(w & 0xffffu);
             const int k = __ldg(Aci + a0 + a);
@@ -453,8 +457,15 @@ __global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __res
                     acc[r * BC + cc] = v;
                 }
         }
+        if (PS > 1) {
 #pragma unroll
-        for (int e = 0; e < BRC; e++) C[(size_t)c0 * BRC + (size_t)e * nC + sl] = acc[e];
+            for (int e = 0; e < BRC; e++)
+#pragma unroll
+                for (int o = PS / 2; o > 0; o >>= 1) acc[e] += __shfl_xor_sync(gmask, acc[e], o);
+        }
+        if (ps == 0)
+#pragma unroll
+            for (int e = 0; e < BRC; e++) C[(size_t)c0 * BRC + (size_t)e * nC + sl] = acc[e];
     }
 }
 
@@ -855,21 +866,29 @@ static const T* pt_vals(Ctx& c, int l) {
     return (const T*)c.dl[l].Pt32c.p;
 }
 
-template <int BR, int BK, int BC, class T, int G>
+template <int BR, int BK, int BC, class T, int GS, int PS>
 static void spgemm_plan_g(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp, const T* B,
                           const DevPattern& Cp, T* C, const ProductPlan& pl) {
-    const long nt = (long)Cp.nrows * G;
-    k_spgemm_plan<T, BR, BK, BC, G><<<(int)((nt + 255) / 256), 256, 0, c.s>>>(Cp.nrows, Ap.rp.p, Ap.ci.p, A, Bp.rp.p, B,
-                                                                             Cp.rp.p, C, pl.ptr.p, pl.pr.p);
+    const long nt = (long)Cp.nrows * GS * PS;
+    k_spgemm_plan<T, BR, BK, BC, GS, PS><<<(int)((nt + 255) / 256), 256, 0, c.s>>>(
+        Cp.nrows, Ap.rp.p, Ap.ci.p, A, Bp.rp.p, B, Cp.rp.p, C, pl.ptr.p, pl.pr.p);
 }
-// C = A B from the product's plan
+// C = A B from the product's plan: lanes per C block by the mean pair count,
+// C blocks per row group by the mean row length (at most 32 lanes per row)
 template <int BR, int BK, int BC, class T>
 static int spgemm_plan(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp, const T* B, const DevPattern& Cp,
                        T* C, const ProductPlan& pl) {
-    if (pl.avg_row > 24) spgemm_plan_g<BR, BK, BC, T, 32>(c, Ap, A, Bp, B, Cp, C, pl);
-    else if (pl.avg_row > 12) spgemm_plan_g<BR, BK, BC, T, 16>(c, Ap, A, Bp, B, Cp, C, pl);
-    else if (pl.avg_row > 6) spgemm_plan_g<BR, BK, BC, T, 8>(c, Ap, A, Bp, B, Cp, C, pl);
-    else spgemm_plan_g<BR, BK, BC, T, 4>(c, Ap, A, Bp, B, Cp, C, pl);
+    if (pl.avg_pairs >= 48) {
+        if (pl.avg_row > 2) spgemm_plan_g<BR, BK, BC, T, 4, 8>(c, Ap, A, Bp, B, Cp, C, pl);
+        else spgemm_plan_g<BR, BK, BC, T, 2, 8>(c, Ap, A, Bp, B, Cp, C, pl);
+    } else if (pl.avg_pairs >= 16) {
+        if (pl.avg_row > 4) spgemm_plan_g<BR, BK, BC, T, 8, 4>(c, Ap, A, Bp, B, Cp, C, pl);
+        else spgemm_plan_g<BR, BK, BC, T, 4, 4>(c, Ap, A, Bp, B, Cp, C, pl);
+    } else {
+        if (pl.avg_row > 12) spgemm_plan_g<BR, BK, BC, T, 16, 1>(c, Ap, A, Bp, B, Cp, C, pl);
+        else if (pl.avg_row > 6) spgemm_plan_g<BR, BK, BC, T, 8, 1>(c, Ap, A, Bp, B, Cp, C, pl);
+        else spgemm_plan_g<BR, BK, BC, T, 4, 1>(c, Ap, A, Bp, B, Cp, C, pl);
+    }
     note_launch();
     TCK(cudaGetLastError());
     return 0;

@@ -67,6 +67,7 @@ struct ProductPlan {
     DBuf<int> ptr;              // nnzb(C) + 1
     DBuf<uint32_t> pr;          // pairs
     int avg_row = 0;            // mean blocks per C row (picks lanes per row)
+    int avg_pairs = 0;          // mean pairs per C block (picks lanes per block)
 };
 int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, ProductPlan& out, cudaStream_t s);
 

@@ -87,6 +87,7 @@ int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, ProductPlan
         for (int q = C.rp[i]; q < C.rp[i + 1]; q++) slot[C.ci[q]] = -1;
     });
     out.avg_row = C.nrows ? (int)((C.nnzb() + C.nrows - 1) / C.nrows) : 1;
+    out.avg_pairs = C.nnzb() ? (int)(pr.size() / (size_t)C.nnzb()) : 1;
     TRET(out.ptr.upload(ptr, s));
     TRET(out.pr.upload(pr, s));
     return 0;
