@@ -497,7 +497,8 @@ def main():
             "amg_setup_ms_per_iter": {k: prof[k][1] / prof_steps for k in
                                       ("setup_asm", "setup_rho", "setup_galerkin", "setup_coarse") if k in prof},
             "amg_dofs": list(info.amg_dofs)[:info.amg_levels],
-            "autotuned": dict(zip(("kmv_block", "sell_block", "reduction_grid"), list(info.tuned)[:3])),
+            "autotuned": dict(zip(("kmv_block", "sell_block", "reduction_grid"), list(info.tuned)[:3]),
+                              amg_lanes_per_row=list(info.tuned_lanes)[1:info.amg_levels - 1]),
             "e2e": {"value": e2e_val, "unit": "design iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "kernels": kern, "clocks": clocks,
             "cpu_baseline": cpu, "multiload": multi, "serve": serve}

@@ -90,6 +90,9 @@ typedef struct topo_params {
                               per-sweep kernels, which measured faster at 392k under graph replay */
     int amg_half_fine;     /* mixed form: 1 keeps the level-0 smoother's matrix as FP16
                               D^-1/2 A D^-1/2 (FP32 arithmetic); 0 (default) keeps it FP32 */
+    int pdl;               /* 1 (default): V-cycle kernels use programmatic dependent launch (each
+                              starts while its predecessor drains and waits on the GPU before it
+                              reads the predecessor's output); 0: plain stream order */
 } topo_params;
 
 typedef struct topo_solve_info {
@@ -104,6 +107,8 @@ typedef struct topo_solve_info {
     double t_fem_ms, t_filter_ms, t_mma_ms, t_setup_ms; /* stage times (CUDA events) */
     int tuned[4];          /* launch shapes picked by the autotuner: element-operator block,
                               level-0 smoother block, reduction grid, block-operator CTAs/SM */
+    int tuned_lanes[8];    /* lanes per block row picked for the smoothing and residual products
+                              of AMG level l >= 1 (0: not tuned) */
 } topo_solve_info;
 
 /* ---------------------------------------------------------------- basics */

@@ -46,7 +46,8 @@ class Params(C.Structure):
         ("cheb_degree_coarse", C.c_int),
         ("autotune", C.c_int),
         ("amg_coarse_cta", C.c_int),
-        ("amg_half_fine", C.c_int)]
+        ("amg_half_fine", C.c_int),
+        ("pdl", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -54,7 +55,8 @@ class SolveInfo(C.Structure):
                 ("filter_its", C.c_int * 4), ("amg_levels", C.c_int), ("amg_dofs", C.c_int * 8),
                 ("mma_inner_its", C.c_int), ("last_fx", C.c_double), ("last_gx0", C.c_double),
                 ("last_ch", C.c_double), ("t_fem_ms", C.c_double), ("t_filter_ms", C.c_double),
-                ("t_mma_ms", C.c_double), ("t_setup_ms", C.c_double), ("tuned", C.c_int * 4)]
+                ("t_mma_ms", C.c_double), ("t_setup_ms", C.c_double), ("tuned", C.c_int * 4),
+                ("tuned_lanes", C.c_int * 8)]
 
 
 class TopoError(RuntimeError):

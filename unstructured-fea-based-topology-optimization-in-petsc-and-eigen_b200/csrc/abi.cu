@@ -285,6 +285,7 @@ void topo_params_default(topo_params* p) {
     p->amg_half_fine = 0;
     p->amg_coarse_cta = 0;
     p->autotune = 1;
+    p->pdl = 1;
 }
 
 int topo_device_alloc(size_t bytes, void** ptr) {

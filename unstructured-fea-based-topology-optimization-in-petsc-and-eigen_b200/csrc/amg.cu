@@ -98,17 +98,31 @@ __global__ void k_diag_inv(int nnode, const int* __restrict__ rp, const int* __r
 // G lanes per block row.  mode 0: y = A x; 1: y = b - A x; 2: y += A x;
 // 3 (power iteration): y = sigma * Dinv A x with sigma = *scal.
 template <class T, int BR, int BC, int G>
-__global__ void k_bsr_spmv(int nrows, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ A,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (BR * BC <= 18 ? 5 : 4) : 2) k_bsr_spmv(int nrows, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ A,
                            const T* __restrict__ x, T* __restrict__ y, const T* __restrict__ b, int mode,
                            const T* __restrict__ dinv, const double* __restrict__ scal) {
+    pdl_trigger();
     const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     const int gl = threadIdx.x % G;
     const bool active = gid < nrows;
+    const long o = (long)BR * gid + gl;
+    int r0 = 0, nb = 0;
+    if (active) {
+        r0 = rp[gid];
+        nb = rp[gid + 1] - r0;
+    }
+    pdl_wait();
+    // the epilogue's own operand, loaded ahead of the row's products
+    T pre = T(0);
+    if (active && gl < BR) {
+        if (mode == 1) pre = b[o];
+        else if (mode == 2) pre = y[o];
+        else if (mode >= 3) pre = dinv[o];
+    }
     T acc[BR];
 #pragma unroll
     for (int r = 0; r < BR; r++) acc[r] = T(0);
     if (active) {
-        const int r0 = rp[gid], nb = rp[gid + 1] - r0;
         const T* Ar = A + (size_t)r0 * BR * BC;
         for (int s = gl; s < nb; s += G) {
             const int j = ci[r0 + s];
@@ -130,12 +144,125 @@ __global__ void k_bsr_spmv(int nrows, const int* __restrict__ rp, const int* __r
 #pragma unroll
         for (int r = 0; r < BR; r++)
             if (r == gl) v = acc[r];
-        const long o = (long)BR * gid + gl;
         if (mode == 0) y[o] = v;
-        else if (mode == 1) y[o] = b[o] - v;
-        else if (mode == 2) y[o] += v;
-        else if (mode == 4) y[o] += dinv[o] * v;  // row-scaled prolongation into hat variables
-        else y[o] = T(*scal) * dinv[o] * v;
+        else if (mode == 1) y[o] = pre - v;
+        else if (mode == 2) y[o] = pre + v;
+        else if (mode == 4) y[o] += pre * v;  // row-scaled prolongation into hat variables
+        else y[o] = T(*scal) * pre * v;
+    }
+}
+
+// ----------------------------------------------------------------- prolongation, one block per lane
+// Packed block-major layout: entry e of block g sits in 16-byte group e / VPL
+// (VPL = 16 / sizeof(T) entries per group), groups of all blocks stored one
+// after another, so lane g of a warp reads its block's group as one 16-byte
+// load and the warp's loads are contiguous; a remainder of fewer than VPL
+// entries (FP32 3x6 blocks: 2) forms one more, narrower group.
+template <class T, int BB>
+__host__ __device__ __forceinline__ size_t pk_off(int e, long g, long npad) {
+    constexpr int VPL = 16 / (int)sizeof(T), NG = BB / VPL, REM = BB - NG * VPL;
+    if (e < NG * VPL) return (size_t)(e / VPL) * npad * VPL + (size_t)g * VPL + (e % VPL);
+    return (size_t)NG * npad * VPL + (size_t)g * REM + (e - NG * VPL);
+}
+
+template <class T, int BB>
+__global__ void k_bsr_pack(int nrows, const int* __restrict__ rp, const T* __restrict__ A, T* __restrict__ Pk,
+                           long npad) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= nrows) return;
+    const int r0 = rp[i], nb = rp[i + 1] - r0;
+    for (int q = lane; q < BB * nb; q += 32) {
+        const int e = q / nb, s = q - e * nb;
+        Pk[pk_off<T, BB>(e, (long)r0 + s, npad)] = A[(size_t)r0 * BB + q];
+    }
+}
+
+// y += P x (mode 2) or y += dinv (P x) (mode 4, hat variables) with P packed:
+// warp w owns rows [wrow[w], wrow[w+1]) -- at most 32 rows whose blocks
+// (at most 32) are blocks rp[wrow[w]] .. of the packed array -- one block per
+// lane.  Each lane finds its row by a binary search over the row starts held
+// one per lane, and a segmented shuffle reduction leaves each row's sum in
+// the row's first lane.  Rows without blocks are skipped (nothing to add).
+template <class T, int BR, int BC>
+__global__ void __launch_bounds__(256) k_bsr_lane(int nw, const int* __restrict__ wrow, const int* __restrict__ rp,
+                                                  const int* __restrict__ ci, const T* __restrict__ Pk, long npad,
+                                                  const T* __restrict__ x, T* __restrict__ y, int mode,
+                                                  const T* __restrict__ dinv) {
+    constexpr int BB = BR * BC, VPL = 16 / (int)sizeof(T), NG = BB / VPL, REM = BB - NG * VPL;
+    static_assert(BC % 2 == 0, "column blocks are read as pairs");
+    pdl_trigger();
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= nw) return;  // uniform per warp
+    const int ra = wrow[w], nr = wrow[w + 1] - ra;
+    const int g0 = rp[ra], nblk = rp[ra + nr] - g0;
+    const int my_start = lane < nr ? rp[ra + lane] - g0 : 64;  // start lane of row ra + lane
+    // row of this lane's block: last row whose start <= lane (an empty row
+    // shares its start with the next row, which the search then picks)
+    int lo = 0, hi = nr - 1;
+#pragma unroll
+    for (int it = 0; it < 5; it++) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int sm = __shfl_sync(0xffffffffu, my_start, mid);
+        if (lo < hi) {
+            if (sm <= lane) lo = mid;
+            else hi = mid - 1;
+        }
+    }
+    const int row = lo;
+    const int seg_start = __shfl_sync(0xffffffffu, my_start, row);
+    const int nxt = __shfl_sync(0xffffffffu, my_start, row + 1 < 32 ? row + 1 : 31);
+    const int seg_end = row + 1 < nr ? nxt : nblk;
+    T acc[BR];
+#pragma unroll
+    for (int r = 0; r < BR; r++) acc[r] = T(0);
+    // pattern and values are fixed during the solve: fetched before the wait
+    const long g = (long)g0 + lane;
+    int j = 0;
+    T v[BB];
+    if (lane < nblk) {
+        j = __ldg(ci + g);
+#pragma unroll
+        for (int k = 0; k < NG; k++) {
+            const uint4 t = __ldg(reinterpret_cast<const uint4*>(Pk + (size_t)k * npad * VPL + (size_t)g * VPL));
+            memcpy(v + k * VPL, &t, 16);
+        }
+#pragma unroll
+        for (int k = 0; k < REM; k++) v[NG * VPL + k] = Pk[(size_t)NG * npad * VPL + (size_t)g * REM + k];
+    }
+    pdl_wait();
+    if (lane < nblk) {
+        T xv[BC];
+#pragma unroll
+        for (int d = 0; d < BC; d += 2) {
+            if constexpr (sizeof(T) == 4) {
+                const float2 t = __ldg(reinterpret_cast<const float2*>(x + (long)BC * j + d));
+                xv[d] = t.x;
+                xv[d + 1] = t.y;
+            } else {
+                const double2 t = __ldg(reinterpret_cast<const double2*>(x + (long)BC * j + d));
+                xv[d] = t.x;
+                xv[d + 1] = t.y;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < BR; r++)
+#pragma unroll
+            for (int d = 0; d < BC; d++) acc[r] += v[r * BC + d] * xv[d];
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+        for (int r = 0; r < BR; r++) {
+            const T t = __shfl_down_sync(0xffffffffu, acc[r], o);
+            if (lane + o < seg_end) acc[r] += t;
+        }
+    if (lane < nblk && lane == seg_start) {
+        const long o = (long)BR * (ra + row);
+#pragma unroll
+        for (int r = 0; r < BR; r++) {
+            if (mode == 2) y[o + r] += acc[r];
+            else y[o + r] += dinv[o + r] * acc[r];
+        }
     }
 }
 
@@ -143,17 +270,31 @@ __global__ void k_bsr_spmv(int nrows, const int* __restrict__ rp, const int* __r
 // dnew = c1 dold + c2 Dinv r; x += dnew (c1, c2 from rho and the step's
 // recurrence numbers cr = rho_k rho_{k-1}, cq = 2 rho_k)
 template <class T, int BS, int G>
-__global__ void k_bsr_cheb(int nrows, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ A,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (BS <= 3 ? 5 : 4) : 2) k_bsr_cheb(int nrows, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ A,
                            const T* __restrict__ dold, T* __restrict__ dnew, T* __restrict__ r, T* __restrict__ x,
                            const T* __restrict__ dinv, const double* __restrict__ rho, double cr, double cq) {
+    pdl_trigger();
     const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     const int gl = threadIdx.x % G;
     const bool active = gid < nrows;
+    const long o = (long)BS * gid + gl;
+    int r0 = 0, nb = 0;
+    T r_o = T(0), d_o = T(0), di_o = T(0);
+    if (active) {
+        r0 = rp[gid];
+        nb = rp[gid + 1] - r0;
+        if (gl < BS) di_o = dinv[o];
+    }
+    pdl_wait();
+    // the update's own operands, loaded ahead of the row's products
+    if (active && gl < BS) {
+        r_o = r[o];
+        d_o = dold[o];
+    }
     T acc[BS];
 #pragma unroll
     for (int q = 0; q < BS; q++) acc[q] = T(0);
     if (active) {
-        const int r0 = rp[gid], nb = rp[gid + 1] - r0;
         const T* Ar = A + (size_t)r0 * BS * BS;
         for (int s = gl; s < nb; s += G) {
             const int j = ci[r0 + s];
@@ -175,11 +316,10 @@ __global__ void k_bsr_cheb(int nrows, const int* __restrict__ rp, const int* __r
 #pragma unroll
         for (int q = 0; q < BS; q++)
             if (q == gl) v = acc[q];
-        const long o = (long)BS * gid + gl;
         const double delta = 0.5 * (*rho);
         const T c2 = T(cq / delta);
-        T rn = r[o] - v;
-        T dn = T(cr) * dold[o] + c2 * dinv[o] * rn;
+        T rn = r_o - v;
+        T dn = T(cr) * d_o + c2 * di_o * rn;
         r[o] = rn;
         dnew[o] = dn;
         x[o] += dn;
@@ -192,28 +332,51 @@ __global__ void k_bsr_cheb(int nrows, const int* __restrict__ rp, const int* __r
 // values in slot sp[s]/32 + k of the value array (sell_idx: two 16-byte
 // vectors and one scalar per row, each a coalesced run over the warp).
 // mode 0: y = A x; 1: y = b - A x; 3: y = sigma Dinv A x
+// One row's product with the sliced-ELLPACK operator: w slots, three at a
+// time, with the column ids of the next three slots loaded while the current
+// three are gathered, so each group waits for one memory round trip (the
+// values and x) instead of two (column id, then x).
+template <class T>
+__device__ __forceinline__ void sell_row_product(const T* __restrict__ S, size_t sb, int lane, const int* __restrict__ cp,
+                                                 int w, const T* __restrict__ x, T (&acc)[3]) {
+    int jn[3];
+#pragma unroll
+    for (int u = 0; u < 3; u++) jn[u] = u < w ? __ldg(cp + 32 * u) : 0;
+    pdl_wait();  // x may come from the previous kernel
+    for (int k = 0; k < w; k += 3) {
+        const int jc[3] = {jn[0], jn[1], jn[2]};
+#pragma unroll
+        for (int u = 0; u < 3; u++) jn[u] = k + 3 + u < w ? __ldg(cp + 32 * (k + 3 + u)) : 0;
+#pragma unroll
+        for (int u = 0; u < 3; u++) {
+            if (k + u < w) {
+                const int j = jc[u];
+                const T x0 = x[3L * j], x1 = x[3L * j + 1], x2 = x[3L * j + 2];
+                T av[9];
+                sell_load9<T>(S, sb + k + u, lane, av);
+                acc[0] += av[0] * x0 + av[1] * x1 + av[2] * x2;
+                acc[1] += av[3] * x0 + av[4] * x1 + av[5] * x2;
+                acc[2] += av[6] * x0 + av[7] * x1 + av[8] * x2;
+            }
+        }
+    }
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) k_sell_spmv(int nrows, const int* __restrict__ sp, const int* __restrict__ sci,
                                                    const T* __restrict__ S, const T* __restrict__ x,
                                                    T* __restrict__ y, const T* __restrict__ b, int mode,
                                                    const T* __restrict__ dinv, const double* __restrict__ scal) {
+    pdl_trigger();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nrows) return;
     const int s = i >> 5, lane = i & 31;
     const int b0 = sp[s], w = (sp[s + 1] - b0) >> 5;
     const size_t sb = (size_t)(b0 >> 5);
     const int* cp = sci + b0 + lane;
-    T a0 = T(0), a1 = T(0), a2 = T(0);
-#pragma unroll 3
-    for (int k = 0; k < w; k++) {
-        const int j = __ldg(cp + 32 * k);
-        const T x0 = x[3L * j], x1 = x[3L * j + 1], x2 = x[3L * j + 2];
-        T av[9];
-        sell_load9<T>(S, sb + k, lane, av);
-        a0 += av[0] * x0 + av[1] * x1 + av[2] * x2;
-        a1 += av[3] * x0 + av[4] * x1 + av[5] * x2;
-        a2 += av[6] * x0 + av[7] * x1 + av[8] * x2;
-    }
+    T acc[3] = {T(0), T(0), T(0)};
+    sell_row_product<T>(S, sb, lane, cp, w, x, acc);
+    const T a0 = acc[0], a1 = acc[1], a2 = acc[2];
     const long o = 3L * i;
     if (mode == 0) { y[o] = a0; y[o + 1] = a1; y[o + 2] = a2; }
     else if (mode == 1) { y[o] = b[o] - a0; y[o + 1] = b[o + 1] - a1; y[o + 2] = b[o + 2] - a2; }
@@ -230,6 +393,7 @@ __global__ void __launch_bounds__(256) k_sell_cheb(int nrows, const int* __restr
                                                    T* __restrict__ dnew, T* __restrict__ r, T* __restrict__ x,
                                                    const T* __restrict__ dinv, const double* __restrict__ rho,
                                                    double cr, double cq) {
+    pdl_trigger();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nrows) return;
     const int s = i >> 5, lane = i & 31;
@@ -237,16 +401,7 @@ __global__ void __launch_bounds__(256) k_sell_cheb(int nrows, const int* __restr
     const size_t sb = (size_t)(b0 >> 5);
     const int* cp = sci + b0 + lane;
     T t[3] = {T(0), T(0), T(0)};
-#pragma unroll 3
-    for (int k = 0; k < w; k++) {
-        const int j = __ldg(cp + 32 * k);
-        const T x0 = dold[3L * j], x1 = dold[3L * j + 1], x2 = dold[3L * j + 2];
-        T av[9];
-        sell_load9<T>(S, sb + k, lane, av);
-        t[0] += av[0] * x0 + av[1] * x1 + av[2] * x2;
-        t[1] += av[3] * x0 + av[4] * x1 + av[5] * x2;
-        t[2] += av[6] * x0 + av[7] * x1 + av[8] * x2;
-    }
+    sell_row_product<T>(S, sb, lane, cp, w, dold, t);
     const double delta = 0.5 * (*rho);
     const T c2 = T(cq / delta), c1 = T(cr);
 #pragma unroll
@@ -379,8 +534,10 @@ __global__ void k_from_hat(long n, const float* __restrict__ sinv, float* __rest
 template <class T>
 __global__ void k_cheb_first(long n, const T* __restrict__ b, T* __restrict__ r, T* __restrict__ d, T* __restrict__ x,
                              const T* __restrict__ dinv, const double* __restrict__ rho, int zero_init) {
+    pdl_trigger();
     const double theta = 0.6 * (*rho);
     const T it = T(1.0 / theta);
+    pdl_wait();
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         if (zero_init) {
             T bi = b[i];
@@ -636,6 +793,8 @@ __global__ void k_gauss_jordan(int n, double* __restrict__ Mg, double* __restric
 }
 template <class T>
 __global__ void k_dense_apply(int n, const double* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x) {
+    pdl_trigger();
+    pdl_wait();
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (i >= n) return;
     double s = 0.0;
@@ -844,6 +1003,7 @@ static int alloc_vals(Ctx& c) {
             TRET(v.T_[l].alloc((size_t)D.P.nnzb * bs * 6));
             TRET(v.AP[l].alloc((size_t)D.AP.nnzb * bs * 6));
             TRET(v.R[l].alloc((size_t)D.R.nnzb * bs * 6));
+            if (D.pnw) TRET(v.Pk[l].alloc((size_t)D.P.nnzb * bs * 6));
         }
         k_power_seed<T><<<grid_for(D.ndof, 256), 256, 0, c.s>>>(D.ndof, v.pv[l].p, c.rho.p + kMaxLevels + l), note_launch();
     }
@@ -896,24 +1056,71 @@ static int spgemm_plan(Ctx& c, const DevPattern& Ap, const T* A, const DevPatter
 
 template <class T, int BR, int BC>
 static int spmv(Ctx& c, const DevPattern& Ap, const T* A, const T* x, T* y, const T* b, int mode, const T* dinv = nullptr,
-                const double* scal = nullptr) {
+                const double* scal = nullptr, int gsel = 0) {
     const long nrows = Ap.nrows;
     const double avg = nrows ? (double)Ap.nnzb / nrows : 1.0;
-    if (avg <= 6.0) {
-        constexpr int G = 8;
-        k_bsr_spmv<T, BR, BC, G><<<(int)((nrows * G + 255) / 256), 256, 0, c.s>>>(
-            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal), note_launch();
-    } else if (avg <= 20.0) {
-        constexpr int G = 16;
-        k_bsr_spmv<T, BR, BC, G><<<(int)((nrows * G + 255) / 256), 256, 0, c.s>>>(
-            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal), note_launch();
+    int G = gsel;
+    if (G != 8 && G != 16 && G != 32) G = avg <= 6.0 ? 8 : (avg <= 20.0 ? 16 : 32);
+    if (G == 8) {
+        TCK(launch_k(c.vc_pdl, k_bsr_spmv<T, BR, BC, 8>, dim3((unsigned)((nrows * 8 + 255) / 256)), dim3(256), 0, c.s,
+                     (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal));
+    } else if (G == 16) {
+        TCK(launch_k(c.vc_pdl, k_bsr_spmv<T, BR, BC, 16>, dim3((unsigned)((nrows * 16 + 255) / 256)), dim3(256), 0, c.s,
+                     (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal));
     } else {
-        constexpr int G = 32;
-        k_bsr_spmv<T, BR, BC, G><<<(int)((nrows * G + 255) / 256), 256, 0, c.s>>>(
-            (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal), note_launch();
+        TCK(launch_k(c.vc_pdl, k_bsr_spmv<T, BR, BC, 32>, dim3((unsigned)((nrows * 32 + 255) / 256)), dim3(256), 0, c.s,
+                     (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal));
     }
     TCK(cudaGetLastError());
     return 0;
+}
+
+// fused Chebyshev step on level l >= 1 with G lanes per block row
+template <class T, int BS>
+static int bsr_cheb(Ctx& c, int l, const T* dcur, T* dnxt, T* x, const double* rho, double cr, double cq) {
+    AmgVals<T>& v = vals<T>(c);
+    const AmgDevLevel& D = c.dl[l];
+    const int nrows = D.nnode, G = c.tune.bsr_g[l];
+    auto kern = G == 8 ? k_bsr_cheb<T, BS, 8> : (G == 16 ? k_bsr_cheb<T, BS, 16> : k_bsr_cheb<T, BS, 32>);
+    const int g = (G == 8 || G == 16) ? G : 32;
+    TCK(launch_k(c.vc_pdl, kern, dim3((unsigned)((nrows * g + 255) / 256)), dim3(256), 0, c.s, nrows, D.A.rp.p,
+                 D.A.ci.p, v.A[l].p, dcur, dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr, cq));
+    return 0;
+}
+
+// P in the packed layout, after each numeric setup of P
+template <class T>
+static int pack_p(Ctx& c, int l) {
+    AmgDevLevel& D = c.dl[l];
+    AmgVals<T>& v = vals<T>(c);
+    if (!D.pnw) return 0;
+    const int grid = (int)(((long)D.P.nrows * 32 + 255) / 256);
+    if (D.bs == 3)
+        k_bsr_pack<T, 18><<<grid, 256, 0, c.s>>>(D.P.nrows, D.P.rp.p, v.P[l].p, v.Pk[l].p, D.P.nnzb), note_launch();
+    else
+        k_bsr_pack<T, 36><<<grid, 256, 0, c.s>>>(D.P.nrows, D.P.rp.p, v.P[l].p, v.Pk[l].p, D.P.nnzb), note_launch();
+    TCK(cudaGetLastError());
+    return 0;
+}
+
+// xf += P xc (mode 2) or xf += dinv (P xc) (mode 4)
+template <class T>
+static int prolong(Ctx& c, int l, const T* xc, T* xf, int mode, const T* dinv) {
+    AmgDevLevel& D = c.dl[l];
+    AmgVals<T>& v = vals<T>(c);
+    if (D.pnw) {
+        const int grid = (int)(((long)D.pnw * 32 + 255) / 256);
+        if (D.bs == 3)
+            TCK(launch_k(c.vc_pdl, k_bsr_lane<T, 3, 6>, dim3(grid), dim3(256), 0, c.s, D.pnw, D.pwrow.p, D.P.rp.p,
+                         D.P.ci.p, v.Pk[l].p, D.P.nnzb, xc, xf, mode, dinv));
+        else
+            TCK(launch_k(c.vc_pdl, k_bsr_lane<T, 6, 6>, dim3(grid), dim3(256), 0, c.s, D.pnw, D.pwrow.p, D.P.rp.p,
+                         D.P.ci.p, v.Pk[l].p, D.P.nnzb, xc, xf, mode, dinv));
+        TCK(cudaGetLastError());
+        return 0;
+    }
+    if (D.bs == 3) return spmv<T, 3, 6>(c, D.P, v.P[l].p, xc, xf, nullptr, mode, dinv);
+    return spmv<T, 6, 6>(c, D.P, v.P[l].p, xc, xf, nullptr, mode, dinv);
 }
 
 // level 0 of the mixed form runs on the FP16 scaled operator (single load case)
@@ -961,14 +1168,14 @@ static int level_spmv(Ctx& c, int l, const T* x, T* y, const T* b, int mode, con
         const bool rec = mode == 1;
         if (rec) prof_begin(c, PS_RES0, &e0);
         const int sb = c.tune.sell_block;
-        k_sell_spmv<T><<<(D.nnode + sb - 1) / sb, sb, 0, c.s>>>(D.nnode, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, x, y, b,
-                                                               mode, dinv, scal), note_launch();
+        TCK(launch_k(c.vc_pdl, k_sell_spmv<T>, dim3((D.nnode + sb - 1) / sb), dim3(sb), 0, c.s, D.nnode, D.sell_ptr.p,
+                     D.sell_ci.p, v.A0s.p, x, y, b, mode, dinv, scal));
         if (rec) prof_end(c, PS_RES0, e0);
         TCK(cudaGetLastError());
         return 0;
     }
-    if (c.dl[l].bs == 3) return spmv<T, 3, 3>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal);
-    return spmv<T, 6, 6>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal);
+    if (c.dl[l].bs == 3) return spmv<T, 3, 3>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal, c.tune.bsr_g[l]);
+    return spmv<T, 6, 6>(c, c.dl[l].A, v.A[l].p, x, y, b, mode, dinv, scal, c.tune.bsr_g[l]);
 }
 
 template <class T>
@@ -1083,6 +1290,7 @@ static int numeric(Ctx& c) {
                                                                              D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();
             TRET((spgemm_plan<6, 6, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
         }
+        TRET(pack_p<T>(c, l));
         TCK(cudaGetLastError());
         prof_end(c, PS_SETUP_GAL, pe);
     }
@@ -1166,7 +1374,8 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
             TRET(level_spmv<T>(c, l, x, v.r[l].p, b, 1));
         }
     }
-    k_cheb_first<T><<<grid_for(n, 256), 256, 0, c.s>>>(n, b, v.r[l].p, v.d[l].p, x, v.dinv[l].p, rho, zero_init ? 1 : 0), note_launch();
+    TCK(launch_k(c.vc_pdl, k_cheb_first<T>, dim3(grid_for(n, 256)), dim3(256), 0, c.s, n, b, v.r[l].p, v.d[l].p, x,
+                 v.dinv[l].p, rho, zero_init ? 1 : 0));
     T* dcur = v.d[l].p;
     T* dnxt = v.d2[l].p;
     for (int k = 1; k < deg && k < 16; k++) {
@@ -1179,21 +1388,14 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
             if (l == 0) {
                 cudaEvent_t e0;
                 prof_begin(c, PS_CHEB0, &e0);
-                k_sell_cheb<T><<<(nrows + c.tune.sell_block - 1) / c.tune.sell_block, c.tune.sell_block, 0, c.s>>>(
-                    nrows, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, dcur,
-                                                                     dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr[k],
-                                                                     cq[k]), note_launch();
+                TCK(launch_k(c.vc_pdl, k_sell_cheb<T>, dim3((nrows + c.tune.sell_block - 1) / c.tune.sell_block),
+                             dim3(c.tune.sell_block), 0, c.s, nrows, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, dcur, dnxt,
+                             v.r[l].p, x, v.dinv[l].p, rho, cr[k], cq[k]));
                 prof_end(c, PS_CHEB0, e0);
             } else if (D.bs == 3) {
-                constexpr int G = 32;
-                k_bsr_cheb<T, 3, G><<<(nrows * G + 255) / 256, 256, 0, c.s>>>(nrows, D.A.rp.p, D.A.ci.p, v.A[l].p, dcur,
-                                                                            dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr[k],
-                                                                            cq[k]), note_launch();
+                TRET((bsr_cheb<T, 3>(c, l, dcur, dnxt, x, rho, cr[k], cq[k])));
             } else {
-                constexpr int G = 32;
-                k_bsr_cheb<T, 6, G><<<(nrows * G + 255) / 256, 256, 0, c.s>>>(nrows, D.A.rp.p, D.A.ci.p, v.A[l].p, dcur,
-                                                                            dnxt, v.r[l].p, x, v.dinv[l].p, rho, cr[k],
-                                                                            cq[k]), note_launch();
+                TRET((bsr_cheb<T, 6>(c, l, dcur, dnxt, x, rho, cr[k], cq[k])));
             }
             std::swap(dcur, dnxt);
         }
@@ -1210,8 +1412,16 @@ static int coarse_cta_level(const Ctx& c) {
     return -1;
 }
 
+// V-cycle launches use programmatic dependent launch while one is in flight
+struct PdlScope {
+    Ctx& c;
+    PdlScope(Ctx& cc, bool on) : c(cc) { c.vc_pdl = on; }
+    ~PdlScope() { c.vc_pdl = false; }
+};
+
 template <class T>
 static int vcycle(Ctx& c, const T* b0, T* x0) {
+    PdlScope pdl_scope(c, c.p.pdl != 0);
     AmgVals<T>& v = vals<T>(c);
     const int L = c.nlev - 1;
     const T* bl[kMaxLevels];
@@ -1279,16 +1489,16 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
         TRET(launch_coarse_cycle<T>(c, a));
     } else {
         const int n = c.dl[L].ndof;
-        k_dense_apply<T><<<(n * 32 + 255) / 256, 256, 0, c.s>>>(n, c.cinv.p, v.b[L].p, v.x[L].p), note_launch();
+        TCK(launch_k(c.vc_pdl, k_dense_apply<T>, dim3((n * 32 + 255) / 256), dim3(256), 0, c.s, n, c.cinv.p, v.b[L].p,
+                     v.x[L].p));
         TCK(cudaGetLastError());
     }
     for (int l = ldown - 1; l >= 0; l--) {
-        AmgDevLevel& D = c.dl[l];
         if (l == 0) prof_end(c, PS_VC_COARSE, ecoarse);
         if (half_level<T>(c, l))  // x^ += D^1/2 P e
-            TRET((spmv<T, 3, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 4, reinterpret_cast<const T*>(c.h0.s.p))));
-        else if (D.bs == 3) TRET((spmv<T, 3, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 2)));
-        else TRET((spmv<T, 6, 6>(c, D.P, v.P[l].p, v.x[l + 1].p, xl[l], nullptr, 2)));
+            TRET(prolong<T>(c, l, v.x[l + 1].p, xl[l], 4, reinterpret_cast<const T*>(c.h0.s.p)));
+        else
+            TRET(prolong<T>(c, l, v.x[l + 1].p, xl[l], 2, nullptr));
         TRET(smooth<T>(c, l, bl[l], xl[l], false));
     }
     if (half_level<T>(c, 0)) {
@@ -1371,6 +1581,50 @@ int amg_level0_apply(Ctx& c, const void* x, void* y) {
     }
     if (!c.v64.allocated) return -1;
     return level_spmv<double>(c, 0, static_cast<const double*>(x), static_cast<double*>(y), nullptr, 0);
+}
+
+// Lanes per block row (8, 16 or 32) of the smoothing and residual products
+// on each level >= 1 that is smoothed, timed (best of 3, CUDA events) as the
+// residual t = b - A x on the current hierarchy's own matrices.
+template <class T>
+static int tune_levels(Ctx& c) {
+    AmgVals<T>& v = vals<T>(c);
+    if (!v.allocated) return 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TCK(cudaEventCreate(&e0));
+    TCK(cudaEventCreate(&e1));
+    int rc = 0;
+    for (int l = 1; l + 1 < c.nlev && rc == 0; l++) {
+        float best = 1e30f;
+        int pick = 0;
+        for (int g : {8, 16, 32}) {
+            c.tune.bsr_g[l] = g;
+            for (int rep = 0; rep < 3 && rc == 0; rep++) {
+                float t = 0.f;
+                if (cudaEventRecord(e0, c.s) != cudaSuccess) { rc = TOPO_ERR_CUDA; break; }
+                rc = level_spmv<T>(c, l, v.x[l].p, v.t[l].p, v.b[l].p, 1);
+                if (rc == 0 && (cudaEventRecord(e1, c.s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                                cudaEventElapsedTime(&t, e0, e1) != cudaSuccess))
+                    rc = TOPO_ERR_CUDA;
+                if (rc == 0 && t < best) { best = t; pick = g; }
+            }
+        }
+        c.tune.bsr_g[l] = pick;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != 0) {
+        cudaGetLastError();
+        for (int l = 0; l < kMaxLevels; l++) c.tune.bsr_g[l] = 0;
+        set_error("AMG level tuning failed");
+    }
+    return rc;
+}
+
+int amg_tune_levels(Ctx& c) {
+    if (c.nlev < 3) return 0;
+    if (c.p.precision == TOPO_PREC_MIXED) return tune_levels<float>(c);
+    return tune_levels<double>(c);
 }
 
 int amg_numeric(Ctx& c) {

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <cstdio>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/topo.h"
@@ -33,6 +34,37 @@ int cuda_fail(cudaError_t e, const char* file, int line);
 // site is followed by note_launch()); read through topo_kernel_launches().
 long& launch_counter();
 inline void note_launch() { __atomic_fetch_add(&launch_counter(), 1L, __ATOMIC_RELAXED); }
+
+// ----------------------------------------------------------------- programmatic dependent launch
+// A kernel launched by launch_k(pdl = true, ...) may be scheduled while the
+// previous kernel in the stream is still running, once that kernel has
+// executed pdl_trigger() in all its CTAs.  It must call pdl_wait() -- which
+// returns when every prerequisite grid has completed and its writes are
+// visible -- before it reads or writes anything a kernel still running could
+// touch; before the wait it may only read data written ahead of the solve
+// (matrix values and patterns, diagonal inverses).  Both are no-ops for a
+// kernel launched without the attribute.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+#endif
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                            Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    note_launch();
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 // ----------------------------------------------------------------- buffers
 // Owning device allocation (cudaMalloc); never copied, only moved.

@@ -82,6 +82,11 @@ struct AmgDevLevel {
     long sell_blocks = 0;
     DBuf<int> sell_ptr, sell_ci;
     ProductPlan plan_T, plan_AP, plan_RAP;  // A Pt, A P, R (A P)
+    // prolongation with one block per lane: warp w owns the P rows
+    // [pwrow[w], pwrow[w+1]) (at most 32 rows and 32 blocks); pnw = 0 when a
+    // P row has more than 32 blocks
+    DBuf<int> pwrow;
+    int pnw = 0;
     DevPattern Ptp;             // tentative prolongator: one block per aggregated node
     DBuf<double> Pt64c;         // its bs x 6 blocks (compact, FP64)
     DBuf<float> Pt32c;          // (FP32 copy for the mixed form)
@@ -95,6 +100,7 @@ struct AmgVals {
     DBuf<T> x[kMaxLevels], b[kMaxLevels], r[kMaxLevels], d[kMaxLevels], d2[kMaxLevels], t[kMaxLevels];
     DBuf<T> pv[kMaxLevels], pw[kMaxLevels];   // power-iteration vectors (warm start)
     DBuf<T> A0s;                // level-0 operator in the sliced-ELLPACK layout
+    DBuf<T> Pk[kMaxLevels];     // P in the packed block-major layout (pk_off)
     bool allocated = false;
 };
 
@@ -248,10 +254,12 @@ struct Ctx {
         int sell_block = 256;       // level-0 sliced-ELLPACK kernels
         int red_blocks = 1184;      // grid of the vector reductions / Gram-Schmidt sweeps
         int blk_ctas = 0;           // block operator CTAs per SM (0: occupancy limit)
+        int bsr_g[kMaxLevels] = {}; // lanes per block row of the level-l (>= 1) smoother/residual (0: by row length)
         bool single_done = false, block_done = false;
     } tune;
 
     topo_solve_info info{};
+    bool vc_pdl = false;            // V-cycle kernels launched with programmatic dependent launch
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
     // per-kernel CUDA-event timing of the hot kernels (off unless enabled)
@@ -320,6 +328,7 @@ int blk_check_error(Ctx& c);
 int amg_alloc(Ctx& c);                                             // amg.cu
 int amg_numeric(Ctx& c);
 int amg_level0_apply(Ctx& c, const void* x, void* y);
+int amg_tune_levels(Ctx& c);  // lanes per block row of the levels >= 1, timed on the current hierarchy
 int amg_reset_warm_start(Ctx& c);
 int amg_level_copy(Ctx& c, int l, int which, std::vector<double>& vals_out, std::vector<int>& rp, std::vector<int>& ci,
                    int& nrows, int& ncols, int& br, int& bc);

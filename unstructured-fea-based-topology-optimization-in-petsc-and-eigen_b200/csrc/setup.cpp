@@ -466,6 +466,29 @@ int build_amg_host(Ctx& c) {
         }
         if (l + 1 < c.nlev) {
             TRET(D.P.upload(H.P, s));
+            {
+                // greedy packing of consecutive P rows into warps of <= 32 rows and <= 32 blocks
+                std::vector<int> wr(1, 0);
+                bool ok = true;
+                int rows = 0, blocks = 0;
+                for (int i = 0; i < H.P.nrows && ok; i++) {
+                    const int nb = H.P.rp[i + 1] - H.P.rp[i];
+                    if (nb > 32) ok = false;
+                    if (rows == 32 || blocks + nb > 32) {
+                        wr.push_back(i);
+                        rows = 0;
+                        blocks = 0;
+                    }
+                    rows++;
+                    blocks += nb;
+                }
+                wr.push_back(H.P.nrows);
+                D.pnw = 0;
+                if (ok && H.P.nrows > 0) {
+                    TRET(D.pwrow.upload(wr, s));
+                    D.pnw = (int)wr.size() - 1;
+                }
+            }
             TRET(D.AP.upload(H.AP, s));
             TRET(D.R.upload(H.R, s));
             TRET(D.ptpos.upload(H.ptpos, s));

@@ -239,10 +239,13 @@ int autotune_single(Ctx& c) {
         }
         c.tune.red_blocks = pick;
     }
+    const int rc = amg_tune_levels(c);
     c.prof.on = prof;
+    TRET(rc);
     c.info.tuned[0] = c.tune.kmv_block;
     c.info.tuned[1] = c.tune.sell_block;
     c.info.tuned[2] = c.tune.red_blocks;
+    for (int l = 0; l < 8 && l < kMaxLevels; l++) c.info.tuned_lanes[l] = c.tune.bsr_g[l];
     return 0;
 }
 
@@ -427,8 +430,10 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
                        (uint64_t)(uintptr_t)c.dsc.p, (uint64_t)(uintptr_t)c.hsc.h, (uint64_t)(uintptr_t)c.Ee64.p,
                        (uint64_t)(uintptr_t)c.v32.A0s.p, (uint64_t)(uintptr_t)c.v64.A0s.p,
                        (uint64_t)(uintptr_t)c.h0.S.p, (uint64_t)c.p.amg_half_fine, (uint64_t)(uintptr_t)c.cinv.p, (uint64_t)(uintptr_t)c.rho.p, (uint64_t)c.p.precision,
-                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.p.amg_coarse_cta, (uint64_t)c.p.fine_smoother_matfree,
+                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.p.amg_coarse_cta, (uint64_t)c.p.fine_smoother_matfree, (uint64_t)c.p.pdl,
                        (uint64_t)c.tune.kmv_block, (uint64_t)c.tune.sell_block, (uint64_t)c.tune.red_blocks,
+                       (uint64_t)c.tune.bsr_g[1] | (uint64_t)c.tune.bsr_g[2] << 8 | (uint64_t)c.tune.bsr_g[3] << 16 |
+                           (uint64_t)c.tune.bsr_g[4] << 24,
                        (uint64_t)n})
         sig = sig_mix(sig, v);
     StepGraphs& G = c.graphs;
