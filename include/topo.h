@@ -80,9 +80,9 @@ typedef struct topo_params {
     int fem_graphs;        /* 1 (default): replay each FGMRES Arnoldi step from a CUDA graph
                               captured in an earlier solve with the same buffers */
     int cheb_degree_post;  /* post-smoothing Chebyshev degree (0: same as cheb_degree) */
-    int cheb_degree_coarse; /* Chebyshev degree below the finest level (0: as the finest; default 4:
+    int cheb_degree_coarse; /* Chebyshev degree below the finest level (0: as the finest; default 6:
                                the coarse levels are small and latency-bound, and stronger
-                               smoothing there cuts FGMRES iterations by about a quarter) */
+                               smoothing there cuts FGMRES iterations by about a third) */
     int autotune;          /* 1 (default): time candidate launch shapes of the hot kernels on
                               this context's own data at its first solve and keep the fastest */
     int amg_coarse_cta;    /* 1: the V-cycle below the first level with <= 8192 DOFs runs in one

@@ -32,17 +32,35 @@ __host__ __device__ __forceinline__ int pk_index_amg(int i, int j, int n) {
 }
 
 // ----------------------------------------------------------------- level-0 assembly
-// One warp per node row: for each incident element (sequential, so the sum
-// order is fixed) lanes own the element's 3*NEN columns and add the three
-// rows of that node into a shared-memory row buffer, then the row is written
+// Node-row copy of the element matrices, built once per mesh: for n2e
+// position p (n2e[p] = e * NEN + l) the three rows of local node l of Ke(e),
+// 3 x 3NEN values in one contiguous run, so the assembly below reads each
+// (node, element) pair with coalesced loads instead of one scattered
+// 4-byte load per 128-byte line of the element-major (AoSoA) matrices.
+template <class T, int NEN>
+__global__ void k_ke_node_rows(long np, const int* __restrict__ n2e, const T* __restrict__ ke, T* __restrict__ kst) {
+    constexpr int ND = 3 * NEN, NPK = ND * (ND + 1) / 2, W = 3 * ND;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < np * W; t += (long)gridDim.x * blockDim.x) {
+        const long p = t / W;
+        const int r = (int)(t - p * W), cc = r / ND, k = r % ND;
+        const int q = n2e[p], e = q / NEN, l = q % NEN;
+        kst[t] = ke[((size_t)(e >> 5) * NPK + pk_index_amg(cc * NEN + l, k, ND)) * 32 + (e & 31)];
+    }
+}
+
+// One warp per node row: lane k owns column k of the element's 3*NEN columns
+// and adds the node's three rows into a shared-memory row buffer, element by
+// element in n2e order (so the sum order is fixed); the loads of four
+// elements are issued together before their sums.  The row is then written
 // out with the Dirichlet identity applied.
 template <class T, int NEN>
 __global__ void k_assemble_A0(int nn, const int* __restrict__ n2e_ptr, const int* __restrict__ n2e,
-                              const uint16_t* __restrict__ bpos, const T* __restrict__ ke, const T* __restrict__ Ee,
+                              const uint16_t* __restrict__ bpos, const T* __restrict__ kst, const T* __restrict__ Ee,
                               const int* __restrict__ rp, const int* __restrict__ ci,
                               const unsigned char* __restrict__ dfix, T* __restrict__ A, int maxdeg,
                               T* __restrict__ S, const int* __restrict__ sp) {
-    constexpr int ND = 3 * NEN, NPK = ND * (ND + 1) / 2;
+    constexpr int ND = 3 * NEN, U = 4;
+    static_assert(ND <= 32, "one lane per element column");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -51,29 +69,43 @@ __global__ void k_assemble_A0(int nn, const int* __restrict__ n2e_ptr, const int
     const int r0 = rp[i], nb = rp[i + 1] - r0;
     for (int q = lane; q < 9 * nb; q += 32) buf[q] = T(0);
     __syncwarp();
-    for (int p = n2e_ptr[i]; p < n2e_ptr[i + 1]; p++) {
-        const int q = n2e[p], e = q / NEN, l = q % NEN;
-        const T E = Ee[e];
-        const int tile = e >> 5, el = e & 31;
-        const T* kp = ke + (size_t)tile * NPK * 32 + el;
-        for (int k = lane; k < ND; k += 32) {
-            const int m = k % NEN, d = k / NEN;
-            const int slot = bpos[((size_t)e * NEN + l) * NEN + m];
+    const int m = lane % NEN, d = lane / NEN;
+    const int pbeg = n2e_ptr[i], pend = n2e_ptr[i + 1];
+    for (int pc = pbeg; pc < pend; pc += 32) {
+        const int np = min(32, pend - pc);
+        const int myq = lane < np ? n2e[pc + lane] : 0;  // (element, local node) of the chunk, one per lane
+        for (int u0 = 0; u0 < np; u0 += U) {
+            T val[U][3], Eu[U];
+            int slot[U];
 #pragma unroll
-            for (int cc = 0; cc < 3; cc++) {
-                const int rl = cc * NEN + l;
-                buf[(cc * 3 + d) * nb + slot] += E * kp[(size_t)pk_index_amg(rl, k, ND) * 32];
+            for (int u = 0; u < U; u++) {
+                const int q = __shfl_sync(0xffffffffu, myq, (u0 + u) & 31);
+                slot[u] = 0;
+                Eu[u] = val[u][0] = val[u][1] = val[u][2] = T(0);
+                if (u0 + u < np && lane < ND) {
+                    const int e = q / NEN, l = q % NEN;
+                    Eu[u] = Ee[e];
+                    const T* kr = kst + (size_t)(pc + u0 + u) * 3 * ND;
+                    slot[u] = bpos[((size_t)e * NEN + l) * NEN + m];
+#pragma unroll
+                    for (int cc = 0; cc < 3; cc++) val[u][cc] = kr[cc * ND + lane];
+                }
             }
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                if (u0 + u < np && lane < ND)
+#pragma unroll
+                    for (int cc = 0; cc < 3; cc++) buf[(cc * 3 + d) * nb + slot[u]] += Eu[u] * val[u][cc];
         }
-        __syncwarp();
     }
+    __syncwarp();
     for (int idx = lane; idx < 9 * nb; idx += 32) {
         const int ent = idx / nb, slot = idx - ent * nb;
-        const int cc = ent / 3, d = ent % 3;
+        const int cc = ent / 3, dd = ent % 3;
         const int j = ci[r0 + slot];
         T v = buf[idx];
-        const bool rf = dfix[3L * i + cc], cf = dfix[3L * j + d];
-        if (rf || cf) v = (rf && j == i && cc == d) ? T(1) : T(0);
+        const bool rf = dfix[3L * i + cc], cf = dfix[3L * j + dd];
+        if (rf || cf) v = (rf && j == i && cc == dd) ? T(1) : T(0);
         A[(size_t)r0 * 9 + idx] = v;
         // the smoother's sliced-ELLPACK copy (its padding stays zero)
         if (S) S[sell_idx<T>((size_t)(sp[i >> 5] >> 5) + slot, ent, i & 31)] = v;
@@ -98,7 +130,7 @@ __global__ void k_diag_inv(int nnode, const int* __restrict__ rp, const int* __r
 // G lanes per block row.  mode 0: y = A x; 1: y = b - A x; 2: y += A x;
 // 3 (power iteration): y = sigma * Dinv A x with sigma = *scal.
 template <class T, int BR, int BC, int G>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (BR * BC <= 18 ? 5 : 4) : 2) k_bsr_spmv(int nrows, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ A,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_bsr_spmv(int nrows, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ A,
                            const T* __restrict__ x, T* __restrict__ y, const T* __restrict__ b, int mode,
                            const T* __restrict__ dinv, const double* __restrict__ scal) {
     pdl_trigger();
@@ -332,37 +364,69 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (BS <= 3 ? 5 : 4) : 2) k
 // values in slot sp[s]/32 + k of the value array (sell_idx: two 16-byte
 // vectors and one scalar per row, each a coalesced run over the warp).
 // mode 0: y = A x; 1: y = b - A x; 3: y = sigma Dinv A x
-// One row's product with the sliced-ELLPACK operator: w slots, three at a
-// time, with the column ids of the next three slots loaded while the current
-// three are gathered, so each group waits for one memory round trip (the
-// values and x) instead of two (column id, then x).
-template <class T>
+// One row's product with the sliced-ELLPACK operator: w slots, U at a time,
+// with the column ids of the next U slots loaded while the current U are
+// gathered, so each group waits for one memory round trip (the values and
+// x) instead of two (column id, then x).  BATCH issues all of a group's
+// loads before its arithmetic (more bytes in flight, more registers);
+// otherwise slot by slot (fewer registers, more warps per SM).
+template <class T, int U, bool BATCH>
 __device__ __forceinline__ void sell_row_product(const T* __restrict__ S, size_t sb, int lane, const int* __restrict__ cp,
                                                  int w, const T* __restrict__ x, T (&acc)[3]) {
-    int jn[3];
+    int jn[U];
 #pragma unroll
-    for (int u = 0; u < 3; u++) jn[u] = u < w ? __ldg(cp + 32 * u) : 0;
+    for (int u = 0; u < U; u++) jn[u] = u < w ? __ldg(cp + 32 * u) : 0;
     pdl_wait();  // x may come from the previous kernel
-    for (int k = 0; k < w; k += 3) {
-        const int jc[3] = {jn[0], jn[1], jn[2]};
+    for (int k = 0; k < w; k += U) {
+        int jc[U];
 #pragma unroll
-        for (int u = 0; u < 3; u++) jn[u] = k + 3 + u < w ? __ldg(cp + 32 * (k + 3 + u)) : 0;
+        for (int u = 0; u < U; u++) jc[u] = jn[u];
 #pragma unroll
-        for (int u = 0; u < 3; u++) {
-            if (k + u < w) {
-                const int j = jc[u];
-                const T x0 = x[3L * j], x1 = x[3L * j + 1], x2 = x[3L * j + 2];
-                T av[9];
-                sell_load9<T>(S, sb + k + u, lane, av);
-                acc[0] += av[0] * x0 + av[1] * x1 + av[2] * x2;
-                acc[1] += av[3] * x0 + av[4] * x1 + av[5] * x2;
-                acc[2] += av[6] * x0 + av[7] * x1 + av[8] * x2;
+        for (int u = 0; u < U; u++) jn[u] = k + U + u < w ? __ldg(cp + 32 * (k + U + u)) : 0;
+        if constexpr (!BATCH) {
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (k + u < w) {
+                    const int j = jc[u];
+                    const T x0 = x[3L * j], x1 = x[3L * j + 1], x2 = x[3L * j + 2];
+                    T a[9];
+                    sell_load9<T>(S, sb + k + u, lane, a);
+                    acc[0] += a[0] * x0 + a[1] * x1 + a[2] * x2;
+                    acc[1] += a[3] * x0 + a[4] * x1 + a[5] * x2;
+                    acc[2] += a[6] * x0 + a[7] * x1 + a[8] * x2;
+                }
+            }
+        } else {
+            // all of the group's loads first, then its arithmetic
+            T xv[U][3], av[U][9];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (k + u < w) {
+                    const int j = jc[u];
+                    xv[u][0] = x[3L * j];
+                    xv[u][1] = x[3L * j + 1];
+                    xv[u][2] = x[3L * j + 2];
+                    sell_load9<T>(S, sb + k + u, lane, av[u]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 3; q++) xv[u][q] = T(0);
+#pragma unroll
+                    for (int q = 0; q < 9; q++) av[u][q] = T(0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                acc[0] += av[u][0] * xv[u][0] + av[u][1] * xv[u][1] + av[u][2] * xv[u][2];
+                acc[1] += av[u][3] * xv[u][0] + av[u][4] * xv[u][1] + av[u][5] * xv[u][2];
+                acc[2] += av[u][6] * xv[u][0] + av[u][7] * xv[u][1] + av[u][8] * xv[u][2];
             }
         }
     }
 }
 
-template <class T>
+// V selects the row product's shape: 0 three slots slot by slot, 1 three
+// slots batched, 2 six slots batched (picked by the autotuner)
+template <class T, int V>
 __global__ void __launch_bounds__(256) k_sell_spmv(int nrows, const int* __restrict__ sp, const int* __restrict__ sci,
                                                    const T* __restrict__ S, const T* __restrict__ x,
                                                    T* __restrict__ y, const T* __restrict__ b, int mode,
@@ -375,7 +439,7 @@ __global__ void __launch_bounds__(256) k_sell_spmv(int nrows, const int* __restr
     const size_t sb = (size_t)(b0 >> 5);
     const int* cp = sci + b0 + lane;
     T acc[3] = {T(0), T(0), T(0)};
-    sell_row_product<T>(S, sb, lane, cp, w, x, acc);
+    sell_row_product<T, V == 2 ? 6 : 3, V != 0>(S, sb, lane, cp, w, x, acc);
     const T a0 = acc[0], a1 = acc[1], a2 = acc[2];
     const long o = 3L * i;
     if (mode == 0) { y[o] = a0; y[o + 1] = a1; y[o + 2] = a2; }
@@ -387,7 +451,7 @@ __global__ void __launch_bounds__(256) k_sell_spmv(int nrows, const int* __restr
 }
 
 // fused Chebyshev step on the sliced-ELLPACK level-0 operator
-template <class T>
+template <class T, int V>
 __global__ void __launch_bounds__(256) k_sell_cheb(int nrows, const int* __restrict__ sp, const int* __restrict__ sci,
                                                    const T* __restrict__ S, const T* __restrict__ dold,
                                                    T* __restrict__ dnew, T* __restrict__ r, T* __restrict__ x,
@@ -401,7 +465,7 @@ __global__ void __launch_bounds__(256) k_sell_cheb(int nrows, const int* __restr
     const size_t sb = (size_t)(b0 >> 5);
     const int* cp = sci + b0 + lane;
     T t[3] = {T(0), T(0), T(0)};
-    sell_row_product<T>(S, sb, lane, cp, w, dold, t);
+    sell_row_product<T, V == 2 ? 6 : 3, V != 0>(S, sb, lane, cp, w, dold, t);
     const double delta = 0.5 * (*rho);
     const T c2 = T(cq / delta), c1 = T(cr);
 #pragma unroll
@@ -573,13 +637,13 @@ __global__ void k_cheb_upd(long n, const T* __restrict__ t, T* __restrict__ r, T
 // B block) pairs in registers: no shared memory, no atomics, no searches,
 // and the C block's entries are written as coalesced runs.
 template <class T, int BR, int BK, int BC, int GS, int PS>
-__global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __restrict__ Arp, const int* __restrict__ Aci,
-                                                     const T* __restrict__ A, const int* __restrict__ Brp,
+__global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __restrict__ Arp, const T* __restrict__ A,
                                                      const T* __restrict__ B, const int* __restrict__ Crp,
                                                      T* __restrict__ C, const int* __restrict__ pptr,
-                                                     const uint32_t* __restrict__ pr) {
+                                                     const uint2* __restrict__ pr) {
     // GS C blocks of a row at a time, each summed by PS lanes (long pair
-    // lists: shorter dependent-load chains), combined by xor shuffles
+    // lists: shorter dependent-load chains), combined by xor shuffles; the
+    // next pair's plan entry is fetched while the current pair is summed
     constexpr int BRK = BR * BK, BKC = BK * BC, BRC = BR * BC, G = GS * PS;
     const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
     const int i = (int)(tid / G), gl = (int)(tid % G), gs = gl / PS, ps = gl % PS;
@@ -594,16 +658,17 @@ __global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __res
 #pragma unroll
         for (int e = 0; e < BRC; e++) acc[e] = T(0);
         const int p1 = pptr[c0 + sl + 1];
-        for (int p = pptr[c0 + sl] + ps; p < p1; p += PS) {
-            const uint32_t w = __ldg(pr + p);
-            const int a = (int)(w >> 16), s = (int)(w & 0xffffu);
-            const int k = __ldg(Aci + a0 + a);
-            const int b0 = __ldg(Brp + k), nB = __ldg(Brp + k + 1) - b0;
+        int p = pptr[c0 + sl] + ps;
+        uint2 w = p < p1 ? __ldg(pr + p) : make_uint2(0u, 0u);
+        for (; p < p1; p += PS) {
+            const int a = (int)(w.x >> 16), nB = (int)(w.x & 0xffffu);
+            const T* Bb = B + w.y;
             T ab[BRK], bb[BKC];
 #pragma unroll
             for (int e = 0; e < BRK; e++) ab[e] = __ldg(Ar + (size_t)e * nA + a);
 #pragma unroll
-            for (int e = 0; e < BKC; e++) bb[e] = __ldg(B + (size_t)b0 * BKC + (size_t)e * nB + s);
+            for (int e = 0; e < BKC; e++) bb[e] = __ldg(Bb + (size_t)e * nB);
+            if (p + PS < p1) w = __ldg(pr + p + PS);
 #pragma unroll
             for (int r = 0; r < BR; r++)
 #pragma unroll
@@ -1031,7 +1096,7 @@ static void spgemm_plan_g(Ctx& c, const DevPattern& Ap, const T* A, const DevPat
                           const DevPattern& Cp, T* C, const ProductPlan& pl) {
     const long nt = (long)Cp.nrows * GS * PS;
     k_spgemm_plan<T, BR, BK, BC, GS, PS><<<(int)((nt + 255) / 256), 256, 0, c.s>>>(
-        Cp.nrows, Ap.rp.p, Ap.ci.p, A, Bp.rp.p, B, Cp.rp.p, C, pl.ptr.p, pl.pr.p);
+        Cp.nrows, Ap.rp.p, A, B, Cp.rp.p, C, pl.ptr.p, pl.pr.p);
 }
 // C = A B from the product's plan: lanes per C block by the mean pair count,
 // C blocks per row group by the mean row length (at most 32 lanes per row)
@@ -1168,7 +1233,8 @@ static int level_spmv(Ctx& c, int l, const T* x, T* y, const T* b, int mode, con
         const bool rec = mode == 1;
         if (rec) prof_begin(c, PS_RES0, &e0);
         const int sb = c.tune.sell_block;
-        TCK(launch_k(c.vc_pdl, k_sell_spmv<T>, dim3((D.nnode + sb - 1) / sb), dim3(sb), 0, c.s, D.nnode, D.sell_ptr.p,
+        const int sv = c.tune.sell_variant;
+        TCK(launch_k(c.vc_pdl, sv == 2 ? k_sell_spmv<T, 2> : (sv == 1 ? k_sell_spmv<T, 1> : k_sell_spmv<T, 0>), dim3((D.nnode + sb - 1) / sb), dim3(sb), 0, c.s, D.nnode, D.sell_ptr.p,
                      D.sell_ci.p, v.A0s.p, x, y, b, mode, dinv, scal));
         if (rec) prof_end(c, PS_RES0, e0);
         TCK(cudaGetLastError());
@@ -1217,15 +1283,24 @@ static int numeric(Ctx& c) {
         // scaled copy built below does not need it)
         c.h0.valid = false;
         T* sell = (std::is_same<T, float>::value && use_half0(c)) ? nullptr : v.A0s.p;
+        const long np = (long)c.n2e.n;
+        if (!v.kst.p) {
+            TRET(v.kst.alloc((size_t)np * 9 * c.nen));
+            if (c.nen == 8)
+                k_ke_node_rows<T, 8><<<grid_for(np * 72, 256), 256, 0, c.s>>>(np, c.n2e.p, ke, v.kst.p), note_launch();
+            else
+                k_ke_node_rows<T, 4><<<grid_for(np * 36, 256), 256, 0, c.s>>>(np, c.n2e.p, ke, v.kst.p), note_launch();
+            TCK(cudaGetLastError());
+        }
         if (c.nen == 8) {
             auto k = k_assemble_A0<T, 8>;
             TCK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, ke, Ee, D.A.rp.p, D.A.ci.p,
+            k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, v.kst.p, Ee, D.A.rp.p, D.A.ci.p,
                                               c.dof_fixed.p, v.A[0].p, c.maxdeg, sell, D.sell_ptr.p), note_launch();
         } else {
             auto k = k_assemble_A0<T, 4>;
             TCK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, ke, Ee, D.A.rp.p, D.A.ci.p,
+            k<<<grid, wpb * 32, smem, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.bpos.p, v.kst.p, Ee, D.A.rp.p, D.A.ci.p,
                                               c.dof_fixed.p, v.A[0].p, c.maxdeg, sell, D.sell_ptr.p), note_launch();
         }
         TCK(cudaGetLastError());
@@ -1388,7 +1463,8 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
             if (l == 0) {
                 cudaEvent_t e0;
                 prof_begin(c, PS_CHEB0, &e0);
-                TCK(launch_k(c.vc_pdl, k_sell_cheb<T>, dim3((nrows + c.tune.sell_block - 1) / c.tune.sell_block),
+                const int sv = c.tune.sell_variant;
+                TCK(launch_k(c.vc_pdl, sv == 2 ? k_sell_cheb<T, 2> : (sv == 1 ? k_sell_cheb<T, 1> : k_sell_cheb<T, 0>), dim3((nrows + c.tune.sell_block - 1) / c.tune.sell_block),
                              dim3(c.tune.sell_block), 0, c.s, nrows, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, dcur, dnxt,
                              v.r[l].p, x, v.dinv[l].p, rho, cr[k], cq[k]));
                 prof_end(c, PS_CHEB0, e0);
@@ -1584,8 +1660,9 @@ int amg_level0_apply(Ctx& c, const void* x, void* y) {
 }
 
 // Lanes per block row (8, 16 or 32) of the smoothing and residual products
-// on each level >= 1 that is smoothed, timed (best of 3, CUDA events) as the
-// residual t = b - A x on the current hierarchy's own matrices.
+// on each level >= 1 that is smoothed, timed (best of 3 runs of 8 back-to-back
+// launches, CUDA events) as the residual t = b - A x on the current
+// hierarchy's own matrices.
 template <class T>
 static int tune_levels(Ctx& c) {
     AmgVals<T>& v = vals<T>(c);
@@ -1602,7 +1679,7 @@ static int tune_levels(Ctx& c) {
             for (int rep = 0; rep < 3 && rc == 0; rep++) {
                 float t = 0.f;
                 if (cudaEventRecord(e0, c.s) != cudaSuccess) { rc = TOPO_ERR_CUDA; break; }
-                rc = level_spmv<T>(c, l, v.x[l].p, v.t[l].p, v.b[l].p, 1);
+                for (int it = 0; it < 8 && rc == 0; it++) rc = level_spmv<T>(c, l, v.x[l].p, v.t[l].p, v.b[l].p, 1);
                 if (rc == 0 && (cudaEventRecord(e1, c.s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
                                 cudaEventElapsedTime(&t, e0, e1) != cudaSuccess))
                     rc = TOPO_ERR_CUDA;

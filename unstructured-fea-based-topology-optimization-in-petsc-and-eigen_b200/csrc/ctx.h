@@ -60,16 +60,16 @@ struct AmgHostLevel {
 };
 
 // Output-stationary plan of a fixed-pattern block product C = A B: for every
-// block of C (CSR order) the (A slot, B slot) pairs that contribute, packed
-// as (slot in A's row) << 16 | (slot in B's row).  Built on the host once
-// per mesh.
+// block of C (CSR order) the (A block, B block) pairs that contribute, each
+// as {slot in A's row << 16 | length of B's row, offset of the B block's
+// first value}.  Built on the host once per mesh.
 struct ProductPlan {
     DBuf<int> ptr;              // nnzb(C) + 1
-    DBuf<uint32_t> pr;          // pairs
+    DBuf<uint2> pr;             // pairs: {A slot << 16 | B row length, B block's first value offset}
     int avg_row = 0;            // mean blocks per C row (picks lanes per row)
     int avg_pairs = 0;          // mean pairs per C block (picks lanes per block)
 };
-int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, ProductPlan& out, cudaStream_t s);
+int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, int bkc, ProductPlan& out, cudaStream_t s);
 
 struct AmgDevLevel {
     int bs = 3, nnode = 0, ndof = 0, nagg = 0;
@@ -101,6 +101,7 @@ struct AmgVals {
     DBuf<T> pv[kMaxLevels], pw[kMaxLevels];   // power-iteration vectors (warm start)
     DBuf<T> A0s;                // level-0 operator in the sliced-ELLPACK layout
     DBuf<T> Pk[kMaxLevels];     // P in the packed block-major layout (pk_off)
+    DBuf<T> kst;                // node-row copy of the element matrices (k_ke_node_rows), built once
     bool allocated = false;
 };
 
@@ -252,6 +253,7 @@ struct Ctx {
     struct Tune {
         int kmv_block = 128;        // k_kmv threads per block
         int sell_block = 256;       // level-0 sliced-ELLPACK kernels
+        int sell_variant = 0;       // their row-product shape (k_sell_spmv's V)
         int red_blocks = 1184;      // grid of the vector reductions / Gram-Schmidt sweeps
         int blk_ctas = 0;           // block operator CTAs per SM (0: occupancy limit)
         int bsr_g[kMaxLevels] = {}; // lanes per block row of the level-l (>= 1) smoother/residual (0: by row length)

@@ -40,7 +40,12 @@ int cuda_fail(cudaError_t e, const char* file, int line) {
 }
 
 // ----------------------------------------------------------------- product plans
-int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, ProductPlan& out, cudaStream_t s) {
+// Pairs of C = A B per C block for the device's output-stationary product.
+// Each pair holds the A block's slot in its row with the B row's length, and
+// the offset of the B block's first value in the slot-interleaved B array
+// (bkc values per block), so the device reads both blocks without looking
+// up A's column or B's row pointer.
+int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, int bkc, ProductPlan& out, cudaStream_t s) {
     const int n = A.nrows;
     std::vector<int> ptr((size_t)C.nnzb() + 1, 0);
     const int nth = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
@@ -61,9 +66,11 @@ int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, ProductPlan
         if (na > 65535) bad = true;
         for (int a = 0; a < na; a++) {
             const int k = A.ci[A.rp[i] + a];
-            for (int sb = 0; sb < B.rp[k + 1] - B.rp[k]; sb++) {
+            const int nb = B.rp[k + 1] - B.rp[k];
+            if (nb > 65535 || ((size_t)B.rp[k + 1] * bkc) >> 32) bad = true;
+            for (int sb = 0; sb < nb; sb++) {
                 const int q = slot[B.ci[B.rp[k] + sb]];
-                if (q < 0 || sb > 65535) { bad = true; continue; }
+                if (q < 0) { bad = true; continue; }
                 ptr[q + 1]++;
             }
         }
@@ -71,7 +78,7 @@ int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, ProductPlan
     });
     if (bad) { set_error("product plan: a row is too long or a pattern is inconsistent"); return TOPO_ERR_UNSUPPORTED; }
     for (size_t q = 0; q + 1 < ptr.size(); q++) ptr[q + 1] += ptr[q];
-    std::vector<uint32_t> pr((size_t)ptr.back());
+    std::vector<uint2> pr((size_t)ptr.back());
     std::vector<int> fill(ptr.begin(), ptr.end() - 1);
     // pass 2: the pairs, in (A slot, B slot) order within each C block
     for_rows([&](int i, std::vector<int>& slot) {
@@ -79,9 +86,11 @@ int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, ProductPlan
         const int na = A.rp[i + 1] - A.rp[i];
         for (int a = 0; a < na; a++) {
             const int k = A.ci[A.rp[i] + a];
-            for (int sb = 0; sb < B.rp[k + 1] - B.rp[k]; sb++) {
+            const int nb = B.rp[k + 1] - B.rp[k];
+            for (int sb = 0; sb < nb; sb++) {
                 const int q = slot[B.ci[B.rp[k] + sb]];
-                pr[fill[q]++] = ((uint32_t)a << 16) | (uint32_t)sb;
+                pr[fill[q]++] = make_uint2(((uint32_t)a << 16) | (uint32_t)nb,
+                                           (uint32_t)((size_t)B.rp[k] * bkc + (size_t)sb));
             }
         }
         for (int q = C.rp[i]; q < C.rp[i + 1]; q++) slot[C.ci[q]] = -1;
@@ -512,9 +521,10 @@ int build_amg_host(Ctx& c) {
             TRET(D.Ptp.upload(Ptp, s));
             TRET(D.Pt64c.upload(pv, s));
             TRET(D.Pt32c.upload(pv32, s));
-            TRET(build_plan(H.A, Ptp, H.P, D.plan_T, s));
-            TRET(build_plan(H.A, H.P, H.AP, D.plan_AP, s));
-            TRET(build_plan(H.R, H.AP, c.hl[l + 1].A, D.plan_RAP, s));
+            // B blocks are bs x 6 in all three products (Pt, P, A P)
+            TRET(build_plan(H.A, Ptp, H.P, H.bs * 6, D.plan_T, s));
+            TRET(build_plan(H.A, H.P, H.AP, H.bs * 6, D.plan_AP, s));
+            TRET(build_plan(H.R, H.AP, c.hl[l + 1].A, H.bs * 6, D.plan_RAP, s));
         }
     }
     return 0;

@@ -80,7 +80,9 @@ __global__ void __launch_bounds__(256) k_mdot(long n, int nv, const double* __re
             if (j < nv) acc[j] += V[j * ld + n - 1] * w[n - 1];
     block_sum<NV>(acc, sm);
     if (threadIdx.x == 0)
-        for (int j = 0; j < nv; j++) part[(long)blockIdx.x * nv + j] = acc[j];
+#pragma unroll
+        for (int j = 0; j < NV; j++)  // unrolled with a guard: a runtime bound would put acc in local memory
+            if (j < nv) part[(long)blockIdx.x * nv + j] = acc[j];
 }
 // w -= sum_j h_j V_j ; partial ||w||^2
 template <int NV>
@@ -137,15 +139,44 @@ __global__ void k_update(long n, int kd, const TZ* __restrict__ Z, long ld, cons
 }
 
 // classical Gram-Schmidt sweeps in chunks of at most 32 basis vectors
+// Grid of a grid-stride sweep: the tuned reduction grid, capped at one full
+// wave of the kernel (its resident CTAs per SM times the SMs) so that wide
+// variants with many accumulators do not run in several rounds.
+static int wave_of(const void* kern) {
+    int dev = 0, nsm = 148, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, 0) != cudaSuccess || occ < 1) occ = 1;
+    cudaGetLastError();
+    return occ * nsm;
+}
+template <int NV>
+static int mdot_grid(int cap) {
+    static const int wave = wave_of(reinterpret_cast<const void*>(k_mdot<NV>));
+    return std::max(1, std::min(cap, wave));
+}
+template <int NV>
+static int orth_grid(int cap) {
+    static const int wave = wave_of(reinterpret_cast<const void*>(k_orth<NV>));
+    return std::max(1, std::min(cap, wave));
+}
+
 static int mdot(Ctx& c, int nv, const double* V, long ld, const double* w, double* out) {
     long n = c.ndof;
     for (int j0 = 0; j0 < nv; j0 += 32) {
         const int k = std::min(32, nv - j0);
         const double* Vj = V + (size_t)j0 * ld;
-        const int g = c.tune.red_blocks;
-        if (k <= 8) k_mdot<8><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
-        else if (k <= 16) k_mdot<16><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
-        else k_mdot<32><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
+        int g = c.tune.red_blocks;
+        if (k <= 8) {
+            g = mdot_grid<8>(g);
+            k_mdot<8><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
+        } else if (k <= 16) {
+            g = mdot_grid<16>(g);
+            k_mdot<16><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
+        } else {
+            g = mdot_grid<32>(g);
+            k_mdot<32><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
+        }
         TCK(cudaGetLastError());
         TRET(finalize_sum(c, c.red.p, g, k, out + j0));
     }
@@ -153,15 +184,24 @@ static int mdot(Ctx& c, int nv, const double* V, long ld, const double* w, doubl
 }
 static int orth(Ctx& c, int nv, const double* V, long ld, const double* h, double* w, double* hn_out) {
     long n = c.ndof;
+    int g = c.tune.red_blocks;
     for (int j0 = 0; j0 < nv; j0 += 32) {
         const int k = std::min(32, nv - j0);
         const double* Vj = V + (size_t)j0 * ld;
-        if (k <= 8) k_orth<8><<<c.tune.red_blocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
-        else if (k <= 16) k_orth<16><<<c.tune.red_blocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
-        else k_orth<32><<<c.tune.red_blocks, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
+        g = c.tune.red_blocks;
+        if (k <= 8) {
+            g = orth_grid<8>(g);
+            k_orth<8><<<g, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
+        } else if (k <= 16) {
+            g = orth_grid<16>(g);
+            k_orth<16><<<g, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
+        } else {
+            g = orth_grid<32>(g);
+            k_orth<32><<<g, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
+        }
     }
     // the last sweep's partials hold ||w||^2 of the fully orthogonalised w
-    k_final<<<1, 32, 0, c.s>>>(c.tune.red_blocks, 1, c.red.p, hn_out, 0), note_launch();
+    k_final<<<1, 32, 0, c.s>>>(g, 1, c.red.p, hn_out, 0), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -222,13 +262,17 @@ int autotune_single(Ctx& c) {
     }
     c.tune.kmv_block = pick;
     best = 1e30;
+    int pick_v = c.tune.sell_variant;
     pick = c.tune.sell_block;
-    for (int b : {128, 256}) {
-        c.tune.sell_block = b;
-        TRET(time_best(c, [&]() { return amg_level0_apply(c, u, y); }, &t));
-        if (t < best) { best = t; pick = b; }
-    }
+    for (int sv : {0, 1, 2})
+        for (int b : {128, 256}) {
+            c.tune.sell_block = b;
+            c.tune.sell_variant = sv;
+            TRET(time_best(c, [&]() { return amg_level0_apply(c, u, y); }, &t));
+            if (t < best) { best = t; pick = b; pick_v = sv; }
+        }
     c.tune.sell_block = pick;
+    c.tune.sell_variant = pick_v;
     if (c.V.n >= (size_t)17 * ldv) {
         best = 1e30;
         pick = c.tune.red_blocks;
@@ -246,6 +290,7 @@ int autotune_single(Ctx& c) {
     c.info.tuned[1] = c.tune.sell_block;
     c.info.tuned[2] = c.tune.red_blocks;
     for (int l = 0; l < 8 && l < kMaxLevels; l++) c.info.tuned_lanes[l] = c.tune.bsr_g[l];
+    c.info.tuned_lanes[0] = c.tune.sell_variant;  // level 0: row-product shape of the sliced-ELLPACK sweeps
     return 0;
 }
 
@@ -431,7 +476,7 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
                        (uint64_t)(uintptr_t)c.v32.A0s.p, (uint64_t)(uintptr_t)c.v64.A0s.p,
                        (uint64_t)(uintptr_t)c.h0.S.p, (uint64_t)c.p.amg_half_fine, (uint64_t)(uintptr_t)c.cinv.p, (uint64_t)(uintptr_t)c.rho.p, (uint64_t)c.p.precision,
                        (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.p.amg_coarse_cta, (uint64_t)c.p.fine_smoother_matfree, (uint64_t)c.p.pdl,
-                       (uint64_t)c.tune.kmv_block, (uint64_t)c.tune.sell_block, (uint64_t)c.tune.red_blocks,
+                       (uint64_t)c.tune.kmv_block, (uint64_t)c.tune.sell_block, (uint64_t)c.tune.red_blocks, (uint64_t)c.tune.sell_variant,
                        (uint64_t)c.tune.bsr_g[1] | (uint64_t)c.tune.bsr_g[2] << 8 | (uint64_t)c.tune.bsr_g[3] << 16 |
                            (uint64_t)c.tune.bsr_g[4] << 24,
                        (uint64_t)n})
