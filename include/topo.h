@@ -80,9 +80,10 @@ typedef struct topo_params {
     int fem_graphs;        /* 1 (default): replay each FGMRES Arnoldi step from a CUDA graph
                               captured in an earlier solve with the same buffers */
     int cheb_degree_post;  /* post-smoothing Chebyshev degree (0: same as cheb_degree) */
-    int cheb_degree_coarse; /* Chebyshev degree below the finest level (0: as the finest; default 6:
+    int cheb_degree_coarse; /* Chebyshev degree below the finest level (0: as the finest; default 4:
                                the coarse levels are small and latency-bound, and stronger
-                               smoothing there cuts FGMRES iterations by about a third) */
+                               smoothing there cuts FGMRES iterations by about a quarter; 6 cuts
+                               them further on one load case but spiked on the 8-case block solve) */
     int autotune;          /* 1 (default): time candidate launch shapes of the hot kernels on
                               this context's own data at its first solve and keep the fastest */
     int amg_coarse_cta;    /* 1: the V-cycle below the first level with <= 8192 DOFs runs in one

@@ -281,7 +281,7 @@ void topo_params_default(topo_params* p) {
     p->fem_block = 1;
     p->fem_graphs = 1;
     p->cheb_degree_post = 0;
-    p->cheb_degree_coarse = 6;
+    p->cheb_degree_coarse = 4;
     p->amg_half_fine = 0;
     p->amg_coarse_cta = 0;
     p->autotune = 1;
