@@ -116,6 +116,9 @@ typedef struct topo_solve_info {
 const char* topo_last_error(void);
 const char* topo_version(void);
 void topo_params_default(topo_params* p);
+/* sizeof(topo_params) and sizeof(topo_solve_info) as compiled into the
+   library, so a binding (ctypes, cgo, JNI) can check its struct mirrors */
+int topo_struct_sizes(size_t* params_bytes, size_t* info_bytes);
 
 /* Device memory for callers without the CUDA runtime. */
 int topo_device_alloc(size_t bytes, void** ptr_d);

@@ -36,6 +36,24 @@ def test_version_and_defaults(T):
     assert (p.fem_rtol, p.filter_rtol, p.filter_atol, p.filter_dtol, p.filter_maxit) == (1e-5, 1e-5, 1e-50, 1e5, 10000)
 
 
+def test_struct_mirrors_match_the_library(T):
+    """The ctypes mirrors of topo_params / topo_solve_info have the library's
+    sizes, and topo_params_default writes exactly sizeof(topo_params) bytes
+    (a guard region after the struct stays untouched) with the solver
+    defaults in the last fields."""
+    import ctypes as C
+    pb, ib = C.c_size_t(), C.c_size_t()
+    assert T.lib().topo_struct_sizes(C.byref(pb), C.byref(ib)) == 0
+    assert pb.value == C.sizeof(T.Params) and ib.value == C.sizeof(T.SolveInfo)
+    buf = (C.c_ubyte * (pb.value + 64))(*([0xAB] * (pb.value + 64)))
+    T.lib().topo_params_default(C.cast(buf, C.POINTER(T.Params)))
+    assert bytes(buf[pb.value:]) == b"\xab" * 64
+    p = T.Params.from_buffer(buf)
+    assert (p.cheb_degree, p.cheb_degree_post, p.cheb_degree_coarse) == (2, 0, 4)
+    assert (p.fem_restart, p.fem_block, p.fem_graphs, p.autotune, p.pdl) == (30, 1, 1, 1, 1)
+    assert (p.amg_coarse_cta, p.amg_half_fine, p.fem_warm_start) == (0, 0, 0)
+
+
 @pytest.mark.parametrize("nen", [8, 4])
 def test_generator_matches_oracle_bit_exact(T, O, nen):
     v, e, f, ld, lv = T.gen_cantilever(9, 5, 4, nen)

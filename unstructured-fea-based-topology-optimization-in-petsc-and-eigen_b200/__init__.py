@@ -70,6 +70,7 @@ _SIGS = {
     "topo_last_error": ([], C.c_char_p),
     "topo_version": ([], C.c_char_p),
     "topo_params_default": ([C.POINTER(Params)], None),
+    "topo_struct_sizes": ([C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)], C.c_int),
     "topo_device_alloc": ([C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
     "topo_device_free": ([C.c_void_p], C.c_int),
     "topo_memcpy_h2d": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),

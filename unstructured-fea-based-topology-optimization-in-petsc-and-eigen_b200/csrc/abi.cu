@@ -264,6 +264,12 @@ extern "C" {
 const char* topo_last_error(void) { return topo::last_error(); }
 const char* topo_version(void) { return "topo-b200 1.0 (sm_100a)"; }
 
+int topo_struct_sizes(size_t* params_bytes, size_t* info_bytes) {
+    if (params_bytes) *params_bytes = sizeof(topo_params);
+    if (info_bytes) *info_bytes = sizeof(topo_solve_info);
+    return 0;
+}
+
 void topo_params_default(topo_params* p) {
     if (!p) return;
     memset(p, 0, sizeof(*p));
