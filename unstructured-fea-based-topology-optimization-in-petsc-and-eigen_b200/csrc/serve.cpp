@@ -67,16 +67,20 @@ struct topo_server {
 extern "C" {
 
 size_t topo_estimate_job_bytes(int nen, int n_nodes, int n_elems, int precision) {
+    const double s = precision == TOPO_PREC_MIXED ? 4.0 : 8.0;  // AMG value size
     // per element: packed Ke in FP64 + FP32, connectivity, masks, element
-    // pair slots, filter matrices, SIMP moduli, design and MMA vectors
+    // pair slots, filter matrices, SIMP moduli, design and MMA vectors, and
+    // the node-row copy of Ke for the level-0 assembly (nen x 3 x 3nen values)
     const double npk = nen == 8 ? 300 : 78, nkf = nen == 8 ? 36 : 10;
-    const double per_elem = npk * 12 + 4.0 * nen + 4 + 2.0 * nen * nen + nkf * 8 + nen * 8 + 12 + 8 + 20 * 8 + 4.0 * nen;
-    // per node: level-0 operator (BSR + sliced ELLPACK), prolongator and
-    // its smoothing temporary, A*P, restriction, Krylov basis, vectors
-    const double s = precision == TOPO_PREC_MIXED ? 4.0 : 8.0;
+    const double per_elem = npk * 12 + 4.0 * nen + 4 + 2.0 * nen * nen + nkf * 8 + nen * 8 + 12 + 8 + 20 * 8 + 4.0 * nen +
+                            9.0 * nen * nen * s;
+    // per node: level-0 operator (BSR + sliced ELLPACK), prolongator (BSR and
+    // packed), its smoothing temporary, A*P, restriction, the Galerkin
+    // product plans (about 7 pairs of 8 bytes per stencil neighbour), Krylov
+    // basis, vectors
     const double deg = nen == 8 ? 27.0 : 24.0;
-    const double per_node = deg * (9 * s + 4) * 2 + 8 * 18 * s * 3 + deg * 18 * s + 31 * 24 + 30 * 3 * s + 16 * 24 + 8 * 3 * s +
-                            7 * 8;
+    const double per_node = deg * (9 * s + 4) * 2 + 8 * 18 * s * 4 + deg * 18 * s + deg * 7 * 8 + 31 * 24 + 30 * 3 * s +
+                            16 * 24 + 8 * 3 * s + 7 * 8;
     const double bytes = n_elems * per_elem + n_nodes * per_node * 1.25 + 96.0 * (1 << 20);
     return (size_t)bytes;
 }
