@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_bsr_spmv(int nr
 #pragma unroll
     for (int r = 0; r < BR; r++)
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+        for (int off = G / 2; off > 0; off >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], off);
     if (active && gl < BR) {
         T v = T(0);
 #pragma unroll
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (BS <= 3 ? 5 : 4) : 2) k
 #pragma unroll
     for (int q = 0; q < BS; q++)
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        for (int off = G / 2; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
     if (active && gl < BS) {
         T v = T(0);
 #pragma unroll
