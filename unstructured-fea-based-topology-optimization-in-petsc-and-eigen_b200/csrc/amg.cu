@@ -91,11 +91,15 @@ __global__ void k_assemble_A0(int nn, const int* __restrict__ n2e_ptr, const int
                     for (int cc = 0; cc < 3; cc++) val[u][cc] = kr[cc * ND + lane];
                 }
             }
+            // two lanes may add into the same row entry for different
+            // elements: each element's adds are separated by a warp barrier
 #pragma unroll
-            for (int u = 0; u < U; u++)
+            for (int u = 0; u < U; u++) {
                 if (u0 + u < np && lane < ND)
 #pragma unroll
                     for (int cc = 0; cc < 3; cc++) buf[(cc * 3 + d) * nb + slot[u]] += Eu[u] * val[u][cc];
+                __syncwarp();
+            }
         }
     }
     __syncwarp();
