@@ -1096,8 +1096,8 @@ static const T* pt_vals(Ctx& c, int l) {
 }
 
 template <int BR, int BK, int BC, class T, int GS, int PS>
-static void spgemm_plan_g(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp, const T* B,
-                          const DevPattern& Cp, T* C, const ProductPlan& pl) {
+static void spgemm_plan_g(Ctx& c, const DevPattern& Ap, const T* A, const T* B, const DevPattern& Cp, T* C,
+                          const ProductPlan& pl) {
     const long nt = (long)Cp.nrows * GS * PS;
     k_spgemm_plan<T, BR, BK, BC, GS, PS><<<(int)((nt + 255) / 256), 256, 0, c.s>>>(
         Cp.nrows, Ap.rp.p, A, B, Cp.rp.p, C, pl.ptr.p, pl.pr.p);
@@ -1105,18 +1105,18 @@ static void spgemm_plan_g(Ctx& c, const DevPattern& Ap, const T* A, const DevPat
 // C = A B from the product's plan: lanes per C block by the mean pair count,
 // C blocks per row group by the mean row length (at most 32 lanes per row)
 template <int BR, int BK, int BC, class T>
-static int spgemm_plan(Ctx& c, const DevPattern& Ap, const T* A, const DevPattern& Bp, const T* B, const DevPattern& Cp,
-                       T* C, const ProductPlan& pl) {
+static int spgemm_plan(Ctx& c, const DevPattern& Ap, const T* A, const T* B, const DevPattern& Cp, T* C,
+                       const ProductPlan& pl) {
     if (pl.avg_pairs >= 48) {
-        if (pl.avg_row > 2) spgemm_plan_g<BR, BK, BC, T, 4, 8>(c, Ap, A, Bp, B, Cp, C, pl);
-        else spgemm_plan_g<BR, BK, BC, T, 2, 8>(c, Ap, A, Bp, B, Cp, C, pl);
+        if (pl.avg_row > 2) spgemm_plan_g<BR, BK, BC, T, 4, 8>(c, Ap, A, B, Cp, C, pl);
+        else spgemm_plan_g<BR, BK, BC, T, 2, 8>(c, Ap, A, B, Cp, C, pl);
     } else if (pl.avg_pairs >= 16) {
-        if (pl.avg_row > 4) spgemm_plan_g<BR, BK, BC, T, 8, 4>(c, Ap, A, Bp, B, Cp, C, pl);
-        else spgemm_plan_g<BR, BK, BC, T, 4, 4>(c, Ap, A, Bp, B, Cp, C, pl);
+        if (pl.avg_row > 4) spgemm_plan_g<BR, BK, BC, T, 8, 4>(c, Ap, A, B, Cp, C, pl);
+        else spgemm_plan_g<BR, BK, BC, T, 4, 4>(c, Ap, A, B, Cp, C, pl);
     } else {
-        if (pl.avg_row > 12) spgemm_plan_g<BR, BK, BC, T, 16, 1>(c, Ap, A, Bp, B, Cp, C, pl);
-        else if (pl.avg_row > 6) spgemm_plan_g<BR, BK, BC, T, 8, 1>(c, Ap, A, Bp, B, Cp, C, pl);
-        else spgemm_plan_g<BR, BK, BC, T, 4, 1>(c, Ap, A, Bp, B, Cp, C, pl);
+        if (pl.avg_row > 12) spgemm_plan_g<BR, BK, BC, T, 16, 1>(c, Ap, A, B, Cp, C, pl);
+        else if (pl.avg_row > 6) spgemm_plan_g<BR, BK, BC, T, 8, 1>(c, Ap, A, B, Cp, C, pl);
+        else spgemm_plan_g<BR, BK, BC, T, 4, 1>(c, Ap, A, B, Cp, C, pl);
     }
     note_launch();
     TCK(cudaGetLastError());
@@ -1346,28 +1346,28 @@ static int numeric(Ctx& c) {
         const T* ptv = pt_vals<T>(c, l);
         if (D.bs == 3) {
             if (c.p.amg_smooth_p) {
-                TRET((spgemm_plan<3, 3, 6, T>(c, D.A, v.A[l].p, D.Ptp, ptv, D.P, v.T_[l].p, D.plan_T)));
+                TRET((spgemm_plan<3, 3, 6, T>(c, D.A, v.A[l].p, ptv, D.P, v.T_[l].p, D.plan_T)));
                 k_smooth_p<T, 3><<<(D.nnode * 32 + 255) / 256, 256, 0, c.s>>>(
                     D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p), note_launch();
             } else {
                 TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 18, cudaMemcpyDeviceToDevice, c.s));
             }
-            TRET((spgemm_plan<3, 3, 6, T>(c, D.A, v.A[l].p, D.P, v.P[l].p, D.AP, v.AP[l].p, D.plan_AP)));
+            TRET((spgemm_plan<3, 3, 6, T>(c, D.A, v.A[l].p, v.P[l].p, D.AP, v.AP[l].p, D.plan_AP)));
             k_transpose<T, 3><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
                                                                              D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();
-            TRET((spgemm_plan<6, 3, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
+            TRET((spgemm_plan<6, 3, 6, T>(c, D.R, v.R[l].p, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
         } else {
             if (c.p.amg_smooth_p) {
-                TRET((spgemm_plan<6, 6, 6, T>(c, D.A, v.A[l].p, D.Ptp, ptv, D.P, v.T_[l].p, D.plan_T)));
+                TRET((spgemm_plan<6, 6, 6, T>(c, D.A, v.A[l].p, ptv, D.P, v.T_[l].p, D.plan_T)));
                 k_smooth_p<T, 6><<<(D.nnode * 32 + 255) / 256, 256, 0, c.s>>>(
                     D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p), note_launch();
             } else {
                 TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 36, cudaMemcpyDeviceToDevice, c.s));
             }
-            TRET((spgemm_plan<6, 6, 6, T>(c, D.A, v.A[l].p, D.P, v.P[l].p, D.AP, v.AP[l].p, D.plan_AP)));
+            TRET((spgemm_plan<6, 6, 6, T>(c, D.A, v.A[l].p, v.P[l].p, D.AP, v.AP[l].p, D.plan_AP)));
             k_transpose<T, 6><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
                                                                              D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();
-            TRET((spgemm_plan<6, 6, 6, T>(c, D.R, v.R[l].p, D.AP, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
+            TRET((spgemm_plan<6, 6, 6, T>(c, D.R, v.R[l].p, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
         }
         TRET(pack_p<T>(c, l));
         TCK(cudaGetLastError());
