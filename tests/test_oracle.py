@@ -254,3 +254,46 @@ def test_design_change_and_movelimit(O):
     xo = x[::-1].copy()
     ch, xo2 = orc.mma_design_change(x, xo)
     assert ch == np.abs(x - x[::-1]).max() and np.array_equal(xo2, x)
+
+
+def test_heaviside_continuation_and_projected_sens(O, small):
+    """Heaviside projection with the reference's beta continuation
+    (PDEFilter.cpp:242-290: beta0 while itr < 30, then on every tenth
+    iteration beta = min(betamax, previous beta + 1), clamp at Xmin) and the
+    chain rule of ComputeProjectedSens (PDEFilter.cpp:292-341), restated in
+    numpy, against the oracle over a 0..75 iteration sequence; the projected
+    sensitivity is also checked against a central difference of the
+    projection."""
+    v, e, f, ld, lv = small
+    orc = O.Oracle(v, e, f, ld, lv, Emax=1.0, rmin=1.5)
+    rng = np.random.default_rng(5)
+    x0, beta0, betamax, Xmin = 0.5, 1.0, 8.0, 0.01
+    beta, prev = beta0, beta0
+    ne = e.shape[0]
+    for itr in range(76):
+        xf = rng.uniform(0.0, 1.0, ne)
+        if itr < 30:
+            beta = beta0
+        elif itr % 10 == 0:
+            beta = min(betamax, prev + 1.0)
+        den = np.tanh(beta * x0) + np.tanh(beta * (1.0 - x0))
+        ref = np.maximum((np.tanh(beta * x0) + np.tanh(beta * (xf - x0))) / den, Xmin)
+        prev = beta
+        xp = orc.heaviside(xf, itr, x0, beta0, betamax, Xmin, proj=1)
+        assert rel(xp, ref) < 1e-14, itr
+        df, dg = rng.standard_normal(ne), rng.standard_normal((1, ne))
+        pdf, pdg = orc.projected_sens(xf, df, dg, x0)
+        dx = beta * (1.0 - np.tanh(beta * (xf - x0)) ** 2) / den
+        assert rel(pdf, df * dx) < 1e-14 and rel(pdg, dg * dx) < 1e-14, itr
+    # beta reached betamax: 30 -> 2, 40 -> 3, ..., 70 -> 6
+    assert beta == 6.0
+    h = 1e-6
+    xf = rng.uniform(0.3, 0.7, ne)  # away from the Xmin clamp
+    up = (np.tanh(beta * x0) + np.tanh(beta * (xf + h - x0))) / den
+    dn = (np.tanh(beta * x0) + np.tanh(beta * (xf - h - x0))) / den
+    pdf, _ = orc.projected_sens(xf, np.ones(ne), np.ones((1, ne)), x0)
+    assert rel(pdf, (up - dn) / (2 * h)) < 1e-7
+    # proj = 0 copies the filtered field
+    xf = rng.uniform(0.0, 1.0, ne)
+    assert np.array_equal(orc.heaviside(xf, 80, x0, beta0, betamax, Xmin, proj=0), xf)
+    orc.close()
