@@ -297,3 +297,32 @@ def test_heaviside_continuation_and_projected_sens(O, small):
     xf = rng.uniform(0.0, 1.0, ne)
     assert np.array_equal(orc.heaviside(xf, 80, x0, beta0, betamax, Xmin, proj=0), xf)
     orc.close()
+
+
+def test_von_mises_matches_restatement(O):
+    """The oracle's element von Mises stress against a numpy restatement of
+    stress/ComputeStress.cpp:53-104: strains at the element centre from the
+    inverse Jacobian, E = Emax isotropic stress scaled by sqrt(x), and the
+    von Mises norm, on jittered elements with random displacements."""
+    rng = np.random.default_rng(9)
+    nu, Emax = 0.3, 2.5
+    lam = nu / ((1 + nu) * (1 - 2 * nu))
+    mu = 1 / (2 * (1 + nu))
+    D = np.array([[lam + 2 * mu, lam, lam, 0, 0, 0], [lam, lam + 2 * mu, lam, 0, 0, 0],
+                  [lam, lam, lam + 2 * mu, 0, 0, 0], [0, 0, 0, mu, 0, 0], [0, 0, 0, 0, mu, 0],
+                  [0, 0, 0, 0, 0, mu]])
+    # diagonal local numbering: node l at (xi, eta, zeta) = signs of bits 0, 1, 2
+    sg = np.array([[1 if l & 1 else -1, 1 if l & 2 else -1, 1 if l & 4 else -1] for l in range(8)], dtype=float)
+    Nd = 0.125 * sg.T  # dN/d(xi, eta, zeta) at the centre, 3 x 8
+    for _ in range(20):
+        co = (sg + 1) / 2 * rng.uniform(0.5, 2.0, 3) + rng.uniform(-0.1, 0.1, (8, 3))
+        ue = rng.standard_normal(24)  # [x0..x7, y0..y7, z0..z7]
+        x = rng.uniform(0.01, 1.0)
+        dN = np.linalg.solve(Nd @ co, Nd)
+        z = np.zeros(8)
+        B = np.array([np.r_[dN[0], z, z], np.r_[z, dN[1], z], np.r_[z, z, dN[2]],
+                      np.r_[dN[1], dN[0], z], np.r_[z, dN[2], dN[1]], np.r_[dN[2], z, dN[0]]])
+        s = np.sqrt(x) * Emax * D @ B @ ue
+        ref = np.sqrt(0.5 * ((s[0] - s[1]) ** 2 + (s[0] - s[2]) ** 2 + (s[1] - s[2]) ** 2
+                             + 6 * (s[3] ** 2 + s[4] ** 2 + s[5] ** 2)))
+        assert abs(O.von_mises_hex8(co, nu, Emax, x, ue) - ref) <= 1e-12 * ref
