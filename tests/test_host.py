@@ -143,3 +143,21 @@ def test_invalid_mesh_rejected_before_any_device_work(T):
     with pytest.raises(T.TopoError) as ei:
         _create(T, v, e, f, ld, lv, m=9)
     assert ei.value.code == -1
+
+
+def test_driver_program_fails_loudly_without_a_gpu(tmp_path):
+    """The main.cpp-shaped driver (`topopt`, over include/topopt.hpp) has no
+    CPU fallback: without a CUDA device it stops at topo_create with the
+    library's error and a nonzero status.  On a GPU machine it must run a
+    tiny lattice to the end instead."""
+    import subprocess
+    import torch
+    exe = os.path.join(ROOT, "unstructured-fea-based-topology-optimization-in-petsc-and-eigen_b200", "topopt")
+    assert os.path.exists(exe)
+    r = subprocess.run([exe, "-lattice", "4", "2", "2", "-maxItr", "2"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=120)
+    if torch.cuda.is_available():
+        assert r.returncode == 0, r.stderr
+    else:
+        assert r.returncode != 0
+        assert "no CPU fallback" in r.stderr
