@@ -151,6 +151,25 @@ def _pkg():
     return G.package()
 
 
+# ------------------------------------------------------------------ ranks
+def max_over_ranks(values, dist=None, device="cpu"):
+    """Per-rank timings (ms) -> their element-wise maximum over all ranks: one
+    all-reduce, which every rank must reach at the same point."""
+    values = [float(v) for v in values]
+    if not dist:
+        return values
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def job_rate(world, steps, ms):
+    """Whole-job design iterations per second: each of `world` replicas ran
+    `steps` design iterations and the slowest rank took `ms` milliseconds."""
+    return world * steps / (ms / 1e3)
+
+
 # ------------------------------------------------------------------ GPU side
 def run_device(ctx, T, torch, steps, warmup, stream, dist=None, profile=True):
     """W untimed + K timed design iterations with resident data; CUDA events on
@@ -387,8 +406,9 @@ def main():
     clocks = sampler.stop()
     if args.only:
         ctx.close()
+        ms = max_over_ranks([ms], dist, "cuda")[0]
         if rank == 0:
-            print(json.dumps({"only": args.only, "value": world * args.steps / (ms / 1e3), "ms": ms,
+            print(json.dumps({"only": args.only, "value": job_rate(world, args.steps, ms), "ms": ms,
                               "fgmres_its": its, "gpu_launches": launches}), flush=True)
         return
     e2e_ms, h2d, d2h = run_e2e(ctx, T, torch, args.steps, args.warmup, stream, dist)
@@ -415,19 +435,12 @@ def main():
                                                                            "kmv", "orth", "cheb0", "res0") if k in prof},
                  "note": "CUDA events around each part, steps launched directly (no graph replay)"}
 
-    def maxr(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    ms, e2e_ms, ms64, msz, ms64w, ms16 = maxr(ms), maxr(e2e_ms), maxr(ms64), maxr(msz), maxr(ms64w), maxr(ms16)
-    value = world * args.steps / (ms / 1e3)
-    e2e_val = world * args.steps / (e2e_ms / 1e3)
-    val64 = world * args.steps / (ms64 / 1e3)
-    valz = world * args.steps / (msz / 1e3)
-    val64w = world * args.steps / (ms64w / 1e3)
+    ms, e2e_ms, ms64, msz, ms64w, ms16 = max_over_ranks([ms, e2e_ms, ms64, msz, ms64w, ms16], dist, "cuda")
+    value = job_rate(world, args.steps, ms)
+    e2e_val = job_rate(world, args.steps, e2e_ms)
+    val64 = job_rate(world, args.steps, ms64)
+    valz = job_rate(world, args.steps, msz)
+    val64w = job_rate(world, args.steps, ms64w)
 
     peak, peak_kind = peaks()
     info = ctx.info()
@@ -487,7 +500,7 @@ def main():
                      "form": "plain FP64 drop-in, zero initial guess as the reference"},
             "fp64_warm": {"value": val64w, "ms_per_step": ms64w / args.steps, "fgmres_its": its64w},
             "mixed_zero_start": {"value": valz, "ms_per_step": msz / args.steps, "fgmres_its": itsz},
-            "mixed_fp16_fine": {"value": world * args.steps / (ms16 / 1e3), "ms_per_step": ms16 / args.steps,
+            "mixed_fp16_fine": {"value": job_rate(world, args.steps, ms16), "ms_per_step": ms16 / args.steps,
                                 "fgmres_its": its16,
                                 "form": "opt-in amg_half_fine=1: level-0 smoother matrix D^-1/2 A D^-1/2 in FP16; "
                                         "same stopping rule, compliance within ~5e-6 of the FP64 form"},
