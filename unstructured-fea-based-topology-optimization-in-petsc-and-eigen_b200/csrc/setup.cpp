@@ -103,29 +103,54 @@ int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, int bkc, Pr
 }
 
 // ----------------------------------------------------------------- patterns
+// Rows [0, n) split over up to 16 host threads; fn(i, mark) with a per-thread
+// scratch array of `width` ints set to -1.
+template <class F>
+static void for_rows_mt(int n, int width, F&& fn) {
+    const int nth = std::max(1, std::min({16, (int)std::thread::hardware_concurrency(), n / 4096 + 1}));
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+        th.emplace_back([&, t]() {
+            std::vector<int> mark(width, -1);
+            for (int i = (int)((long)n * t / nth); i < (int)((long)n * (t + 1) / nth); i++) fn(i, mark);
+        });
+    for (auto& x : th) x.join();
+}
+
+// Pattern of A B, each row's columns sorted: a counting pass and a filling
+// pass over the rows, both split over host threads (the rows are
+// independent, so the result does not depend on the split).
 Pattern sym_spgemm(const Pattern& A, const Pattern& B) {
     Pattern C;
     C.nrows = A.nrows;
     C.ncols = B.ncols;
     C.rp.assign(A.nrows + 1, 0);
-    std::vector<int> mark(B.ncols, -1);
-    std::vector<int> row;
-    std::vector<std::vector<int>> rows(A.nrows);
-    for (int i = 0; i < A.nrows; i++) {
-        row.clear();
+    for_rows_mt(A.nrows, B.ncols, [&](int i, std::vector<int>& mark) {
+        int cnt = 0;
         for (int p = A.rp[i]; p < A.rp[i + 1]; p++) {
-            int k = A.ci[p];
-            for (int q = B.rp[k]; q < B.rp[k + 1]; q++) {
-                int j = B.ci[q];
-                if (mark[j] != i) { mark[j] = i; row.push_back(j); }
-            }
+            const int k = A.ci[p];
+            for (int q = B.rp[k]; q < B.rp[k + 1]; q++)
+                if (mark[B.ci[q]] != i) {
+                    mark[B.ci[q]] = i;
+                    cnt++;
+                }
         }
-        std::sort(row.begin(), row.end());
-        rows[i] = row;
-        C.rp[i + 1] = C.rp[i] + (int)row.size();
-    }
+        C.rp[i + 1] = cnt;
+    });
+    for (int i = 0; i < A.nrows; i++) C.rp[i + 1] += C.rp[i];
     C.ci.resize(C.rp[A.nrows]);
-    for (int i = 0; i < A.nrows; i++) std::copy(rows[i].begin(), rows[i].end(), C.ci.begin() + C.rp[i]);
+    for_rows_mt(A.nrows, B.ncols, [&](int i, std::vector<int>& mark) {
+        int w = C.rp[i];
+        for (int p = A.rp[i]; p < A.rp[i + 1]; p++) {
+            const int k = A.ci[p];
+            for (int q = B.rp[k]; q < B.rp[k + 1]; q++)
+                if (mark[B.ci[q]] != i) {
+                    mark[B.ci[q]] = i;
+                    C.ci[w++] = B.ci[q];
+                }
+        }
+        std::sort(C.ci.begin() + C.rp[i], C.ci.begin() + w);
+    });
     return C;
 }
 
