@@ -161,3 +161,16 @@ def test_driver_program_fails_loudly_without_a_gpu(tmp_path):
     else:
         assert r.returncode != 0
         assert "no CPU fallback" in r.stderr
+
+
+@pytest.mark.parametrize("field,value", [("cheb_degree_coarse", 16), ("cheb_degree_post", -1), ("amg_max_levels", 0),
+                                         ("amg_max_levels", 9), ("amg_rho_its", -2), ("cheb_safety", -0.5),
+                                         ("pdl", 2), ("fem_graphs", -1), ("autotune", 3), ("amg_half_fine", 2),
+                                         ("fem_block", 5), ("proj", 2), ("amg_coarse_max", 5), ("cheb_degree", 0)])
+def test_invalid_solver_options_rejected_before_any_device_work(T, field, value):
+    """Out-of-range solver options are refused at creation with the option's
+    name in the message (no silent clamping), before any device call."""
+    v, e, f, ld, lv = T.gen_cantilever(3, 2, 2, 8)
+    with pytest.raises(T.TopoError) as ei:
+        _create(T, v, e, f, ld, lv, **{field: value})
+    assert ei.value.code == -1 and field in str(ei.value)

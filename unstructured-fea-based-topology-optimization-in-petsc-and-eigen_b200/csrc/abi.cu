@@ -334,6 +334,26 @@ static int check_params(const topo_params* p) {
     if (p->cheb_degree < 1 || p->cheb_degree > 15) { set_error("cheb_degree must be in [1,15]"); return TOPO_ERR_ARG; }
     if (p->precision != TOPO_PREC_FP64 && p->precision != TOPO_PREC_MIXED) { set_error("bad precision"); return TOPO_ERR_ARG; }
     if (p->amg_coarse_max < 6 || p->amg_coarse_max > 4000) { set_error("amg_coarse_max must be in [6,4000]"); return TOPO_ERR_ARG; }
+    if (p->amg_max_levels < 1 || p->amg_max_levels > kMaxLevels) {
+        set_error("amg_max_levels must be in [1,%d]", kMaxLevels);
+        return TOPO_ERR_ARG;
+    }
+    if (p->cheb_degree_post < 0 || p->cheb_degree_post > 15 || p->cheb_degree_coarse < 0 || p->cheb_degree_coarse > 15) {
+        set_error("cheb_degree_post and cheb_degree_coarse must be in [0,15] (0: as cheb_degree)");
+        return TOPO_ERR_ARG;
+    }
+    if (p->amg_rho_its < 0 || p->amg_rho_its > 1000) { set_error("amg_rho_its must be in [0,1000]"); return TOPO_ERR_ARG; }
+    if (!(p->cheb_safety >= 0.0 && p->cheb_safety <= 10.0)) {
+        set_error("cheb_safety must be in [0,10] (0: 1)");
+        return TOPO_ERR_ARG;
+    }
+    const struct { int v; const char* name; } flags[] = {
+        {p->proj, "proj"}, {p->amg_smooth_p, "amg_smooth_p"}, {p->fine_smoother_matfree, "fine_smoother_matfree"},
+        {p->fem_warm_start, "fem_warm_start"}, {p->fem_block, "fem_block"}, {p->fem_graphs, "fem_graphs"},
+        {p->autotune, "autotune"}, {p->amg_coarse_cta, "amg_coarse_cta"}, {p->amg_half_fine, "amg_half_fine"},
+        {p->pdl, "pdl"}};
+    for (const auto& f : flags)
+        if (f.v != 0 && f.v != 1) { set_error("%s must be 0 or 1", f.name); return TOPO_ERR_ARG; }
     return 0;
 }
 
