@@ -3,7 +3,7 @@ against the CPU oracle on the same seeded inputs.
 
 Tolerances (FP64): element matrices, volumes, K u: 1e-12 relative (summation
 order only); tightly converged solves (rtol 1e-10 / 1e-12 on both sides):
-compliance 1e-8 and displacements 1e-7 relative (the north-star parity bar);
+compliance 1e-8 and displacements 1e-7 relative (the parity bar of the FP64 solve);
 filter 1e-9; MMA update 1e-8; design change exact to 1e-12."""
 import numpy as np
 import pytest
