@@ -7,9 +7,15 @@
 //          Dirichlet rows/columns identity (MatZeroRowsColumns, SolveFem.cpp:324)
 //   rho <- power iteration on D^-1 A (warm-started across design iterations)
 //   P   <- (I - 4/(3 rho) D^-1 A) Pt        (smoothed aggregation)
-//   A+  <- P^T (A P)                         (Galerkin, two fixed-pattern SpGEMMs)
+//   A+  <- P^T (A P)                         (Galerkin, two fixed-pattern SpGEMMs
+//                                             from host-built per-mesh pair plans)
 //   coarsest: explicit FP64 inverse (Gauss-Jordan, partial pivoting)
-// V-cycle: Chebyshev(k)-Jacobi pre/post smoothing on [0.1, 1.1] rho.
+// V-cycle: Chebyshev(k)-Jacobi pre/post smoothing on [0.1, 1.1] rho; level 0
+// on a sliced-ELLPACK copy of A0 whose sweeps fetch the next slot group's
+// column ids while gathering the current group; levels >= 1 on BSR with a
+// tuned number of lanes per block row; prolongation with one packed P block
+// per lane; every V-cycle kernel started early by programmatic dependent
+// launch (it waits on the GPU for its predecessor's output).
 //
 // BSR values are slot-interleaved (see ctx.h) so that the lanes of a warp
 // walking the blocks of one row read every block entry as a coalesced run.
