@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 
 #include "ctx.h"
@@ -1013,8 +1014,11 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(CoarseArgs<T> a) {
 template <class T>
 static int launch_coarse_cycle(Ctx& c, const CoarseArgs<T>& a) {
     auto kern = k_coarse_cycle<T>;
-    static int csize_cache[2] = {0, 0};
-    int& csize = csize_cache[std::is_same<T, double>::value ? 1 : 0];
+    // cluster size that can be co-scheduled, found once per precision (threads
+    // that race here compute the same value)
+    static std::atomic<int> csize_cache[2] = {{0}, {0}};
+    std::atomic<int>& csize_a = csize_cache[std::is_same<T, double>::value ? 1 : 0];
+    int csize = csize_a.load(std::memory_order_relaxed);
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];
     cfg.blockDim = dim3(512, 1, 1);
@@ -1034,6 +1038,7 @@ static int launch_coarse_cycle(Ctx& c, const CoarseArgs<T>& a) {
             if (cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg) == cudaSuccess && nclusters >= 1) csize = 16;
         }
         cudaGetLastError();
+        csize_a.store(csize, std::memory_order_relaxed);
     }
     cfg.gridDim = dim3(csize, 1, 1);
     attr[0].val.clusterDim.x = csize;

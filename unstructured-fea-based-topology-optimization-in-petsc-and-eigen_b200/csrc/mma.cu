@@ -467,10 +467,9 @@ static int update_m(Ctx& c, double* x, const double* dfdx, const double* gx_dev,
     TCK(cudaMemcpyAsync(c.xo2.p, c.xo1.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, c.s));
     TCK(cudaMemcpyAsync(c.xo1.p, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, c.s));
     // SolveDIP as one cooperative launch
-    static int dev_sms = 0;
-    int dev;
+    int dev, dev_sms = 0;
     TCK(cudaGetDevice(&dev));
-    if (!dev_sms) TCK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, dev));
+    TCK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, dev));
     int occ = 0;
     TCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solvedip<M>, 256, 0));
     int blocks = std::max(1, std::min(dev_sms * std::max(occ, 1), std::min(2048, (n + 255) / 256)));
