@@ -356,9 +356,14 @@ static void tentative(const Ctx& c, int lvl, const AmgHostLevel& L, const std::v
         for (int i = 0; i < nnode; i++)
             if (L.agg[i] >= 0) mem[fill[L.agg[i]]++] = i;
     }
+    // aggregates are independent (disjoint rows of Pt, their own rows of
+    // Bnext): split over host threads, which also overlaps the scattered
+    // reads of member coordinates
+    const int nth = std::max(1, std::min({16, (int)std::thread::hardware_concurrency(), na / 512 + 1}));
+    auto work = [&](int a_begin, int a_end) {
     std::vector<double> Q;
     std::vector<long> rid;
-    for (int a = 0; a < na; a++) {
+    for (int a = a_begin; a < a_end; a++) {
         int m0 = cnt[a], m1 = cnt[a + 1];
         Q.clear();
         rid.clear();
@@ -412,6 +417,11 @@ static void tentative(const Ctx& c, int lvl, const AmgHostLevel& L, const std::v
         for (int i2 = 0; i2 < 6; i2++)
             for (int j = 0; j < 6; j++) Bnext[((size_t)a * 6 + i2) * 6 + j] = R[i2 * 6 + j];
     }
+    };
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+        th.emplace_back(work, (int)((long)na * t / nth), (int)((long)na * (t + 1) / nth));
+    for (auto& x : th) x.join();
 }
 
 int build_amg_host(Ctx& c) {
