@@ -216,6 +216,61 @@ int aggregate_graph(int nn, const std::vector<int>& rp, const std::vector<int>& 
     return na;
 }
 
+// Node graph (each row: the nodes sharing an element with it, itself
+// included, sorted) = block pattern of K.  Counting and filling passes over
+// the rows split across host threads; an isolated node keeps its diagonal.
+Pattern node_graph(int nn, int ne, int nen, const int32_t* element, const std::vector<int>& n2e_ptr,
+                   const std::vector<int>& n2e) {
+    (void)ne;
+    Pattern G;
+    G.nrows = G.ncols = nn;
+    G.rp.assign(nn + 1, 0);
+    for_rows_mt(nn, nn, [&](int i, std::vector<int>& mark) {
+        int cnt = 0;
+        for (int p = n2e_ptr[i]; p < n2e_ptr[i + 1]; p++) {
+            const int e = n2e[p] / nen;
+            for (int l = 0; l < nen; l++) {
+                const int j = element[(long)e * nen + l];
+                if (mark[j] != i) { mark[j] = i; cnt++; }
+            }
+        }
+        G.rp[i + 1] = cnt ? cnt : 1;
+    });
+    for (int i = 0; i < nn; i++) G.rp[i + 1] += G.rp[i];
+    G.ci.resize(G.rp[nn]);
+    for_rows_mt(nn, nn, [&](int i, std::vector<int>& mark) {
+        int w = G.rp[i];
+        for (int p = n2e_ptr[i]; p < n2e_ptr[i + 1]; p++) {
+            const int e = n2e[p] / nen;
+            for (int l = 0; l < nen; l++) {
+                const int j = element[(long)e * nen + l];
+                if (mark[j] != i) { mark[j] = i; G.ci[w++] = j; }
+            }
+        }
+        if (w == G.rp[i]) G.ci[w++] = i;
+        std::sort(G.ci.begin() + G.rp[i], G.ci.begin() + w);
+    });
+    return G;
+}
+
+// For every element and pair of its local nodes (p, q): the slot of node q in
+// node p's row of G (elements split across host threads).
+std::vector<uint16_t> block_positions(int ne, int nen, const int32_t* element, const Pattern& G) {
+    std::vector<uint16_t> bpos((size_t)ne * nen * nen);
+    for_rows_mt(ne, 1, [&](int e, std::vector<int>&) {
+        for (int p = 0; p < nen; p++) {
+            const int np = element[(long)e * nen + p];
+            const int* b = G.ci.data() + G.rp[np];
+            const int len = G.rp[np + 1] - G.rp[np];
+            for (int q = 0; q < nen; q++) {
+                const int nq = element[(long)e * nen + q];
+                bpos[((size_t)e * nen + p) * nen + q] = (uint16_t)(std::lower_bound(b, b + len, nq) - b);
+            }
+        }
+    });
+    return bpos;
+}
+
 // ----------------------------------------------------------------- mesh
 int build_mesh(Ctx& c, const double* vertex, const int32_t* element, int n_fixed, const int32_t* fixed, int n_cases,
                const int32_t* case_ptr, const int32_t* load_dofs, const double* load_vals) {
@@ -288,43 +343,10 @@ int build_mesh(Ctx& c, const double* vertex, const int32_t* element, int n_fixed
         for (long q = 0; q < (long)ne * nen; q++) n2e[pos[element[q]]++] = (int)q;
     }
     // node graph (self included, sorted) = block pattern of K
-    Pattern G;
-    G.nrows = G.ncols = nn;
-    G.rp.assign(nn + 1, 0);
-    {
-        std::vector<int> mark(nn, -1), row;
-        std::vector<int> ci;
-        ci.reserve((size_t)nn * 27);
-        for (int i = 0; i < nn; i++) {
-            row.clear();
-            for (int p = n2e_ptr[i]; p < n2e_ptr[i + 1]; p++) {
-                int e = n2e[p] / nen;
-                for (int l = 0; l < nen; l++) {
-                    int j = element[(long)e * nen + l];
-                    if (mark[j] != i) { mark[j] = i; row.push_back(j); }
-                }
-            }
-            if (row.empty()) row.push_back(i);  // isolated node: keep its diagonal
-            std::sort(row.begin(), row.end());
-            ci.insert(ci.end(), row.begin(), row.end());
-            G.rp[i + 1] = (int)ci.size();
-        }
-        G.ci.swap(ci);
-    }
+    Pattern G = node_graph(nn, ne, nen, element, n2e_ptr, n2e);
     c.maxdeg = G.max_row();
     if (c.maxdeg > 65535) { set_error("node degree too large"); return TOPO_ERR_MESH; }
-    std::vector<uint16_t> bpos((size_t)ne * nen * nen);
-    for (int e = 0; e < ne; e++)
-        for (int p = 0; p < nen; p++) {
-            int np = element[(long)e * nen + p];
-            const int* b = G.ci.data() + G.rp[np];
-            int len = G.rp[np + 1] - G.rp[np];
-            for (int q = 0; q < nen; q++) {
-                int nq = element[(long)e * nen + q];
-                int slot = (int)(std::lower_bound(b, b + len, nq) - b);
-                bpos[((size_t)e * nen + p) * nen + q] = (uint16_t)slot;
-            }
-        }
+    std::vector<uint16_t> bpos = block_positions(ne, nen, element, G);
     TRET(c.n2e_ptr.upload(n2e_ptr, s));
     TRET(c.n2e.upload(n2e, s));
     TRET(c.bpos.upload(bpos, s));
