@@ -39,6 +39,22 @@ int cuda_fail(cudaError_t e, const char* file, int line) {
     return e == cudaErrorMemoryAllocation ? TOPO_ERR_OOM : TOPO_ERR_CUDA;
 }
 
+// ----------------------------------------------------------------- host threads
+// body(t) for t in [0, nth) on nth threads; if a thread cannot be started,
+// the started ones are joined before the error propagates (the callers'
+// GUARD turns it into an error return).
+template <class F>
+static void run_threads(int nth, F&& body) {
+    std::vector<std::thread> th;
+    try {
+        for (int t = 0; t < nth; t++) th.emplace_back(body, t);
+    } catch (...) {
+        for (auto& x : th) x.join();
+        throw;
+    }
+    for (auto& x : th) x.join();
+}
+
 // ----------------------------------------------------------------- product plans
 // Pairs of C = A B per C block for the device's output-stationary product.
 // Each pair holds the A block's slot in its row with the B row's length, and
@@ -50,13 +66,10 @@ int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, int bkc, Pr
     std::vector<int> ptr((size_t)C.nnzb() + 1, 0);
     const int nth = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
     auto for_rows = [&](auto&& fn) {
-        std::vector<std::thread> th;
-        for (int t = 0; t < nth; t++)
-            th.emplace_back([&, t]() {
-                std::vector<int> slot(C.ncols, -1);
-                for (int i = (int)((long)n * t / nth); i < (int)((long)n * (t + 1) / nth); i++) fn(i, slot);
-            });
-        for (auto& x : th) x.join();
+        run_threads(nth, [&](int t) {
+            std::vector<int> slot(C.ncols, -1);
+            for (int i = (int)((long)n * t / nth); i < (int)((long)n * (t + 1) / nth); i++) fn(i, slot);
+        });
     };
     std::atomic<bool> bad(false);
     // pass 1: pairs per C block
@@ -108,13 +121,10 @@ int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, int bkc, Pr
 template <class F>
 static void for_rows_mt(int n, int width, F&& fn) {
     const int nth = std::max(1, std::min({16, (int)std::thread::hardware_concurrency(), n / 4096 + 1}));
-    std::vector<std::thread> th;
-    for (int t = 0; t < nth; t++)
-        th.emplace_back([&, t]() {
-            std::vector<int> mark(width, -1);
-            for (int i = (int)((long)n * t / nth); i < (int)((long)n * (t + 1) / nth); i++) fn(i, mark);
-        });
-    for (auto& x : th) x.join();
+    run_threads(nth, [&](int t) {
+        std::vector<int> mark(width, -1);
+        for (int i = (int)((long)n * t / nth); i < (int)((long)n * (t + 1) / nth); i++) fn(i, mark);
+    });
 }
 
 // Pattern of A B, each row's columns sorted: a counting pass and a filling
@@ -440,10 +450,7 @@ static void tentative(const Ctx& c, int lvl, const AmgHostLevel& L, const std::v
             for (int j = 0; j < 6; j++) Bnext[((size_t)a * 6 + i2) * 6 + j] = R[i2 * 6 + j];
     }
     };
-    std::vector<std::thread> th;
-    for (int t = 0; t < nth; t++)
-        th.emplace_back(work, (int)((long)na * t / nth), (int)((long)na * (t + 1) / nth));
-    for (auto& x : th) x.join();
+    run_threads(nth, [&](int t) { work((int)((long)na * t / nth), (int)((long)na * (t + 1) / nth)); });
 }
 
 int build_amg_host(Ctx& c) {
