@@ -212,7 +212,16 @@ int topo_server_run(topo_server* s) {
                 s->peak_reserved = std::max(s->peak_reserved, s->reserved);
                 s->active++;
                 s->max_seen = std::max(s->max_seen, s->active);
-                workers.emplace_back(run_job, s, &j, t0);
+                try {
+                    workers.emplace_back(run_job, s, &j, t0);
+                } catch (...) {
+                    // no host thread for this job: it fails, the others go on
+                    j.status = TOPO_ERR_OOM;
+                    j.state = 3;
+                    j.finish_s = now;
+                    s->reserved -= j.est_bytes;
+                    s->active--;
+                }
                 next++;
             }
             if (next == order.size() && s->active == 0) break;
