@@ -217,6 +217,7 @@ int topo_server_run(topo_server* s) {
                 } catch (...) {
                     // no host thread for this job: it fails, the others go on
                     j.status = TOPO_ERR_OOM;
+                    j.error = "could not start a host thread for the job";
                     j.state = 3;
                     j.finish_s = now;
                     s->reserved -= j.est_bytes;
