@@ -478,6 +478,7 @@ int topo_fem_element_matrix(topo_ctx* ctx, int e, double* ke) {
     if (!ctx || !ke) { set_error("null argument"); return TOPO_ERR_ARG; }
     Ctx& c = ctx->c;
     if (e < 0 || e >= c.ne) { set_error("element index out of range"); return TOPO_ERR_ARG; }
+    GUARD_BEGIN
     const int nd = c.nde, npk = c.npk;
     std::vector<double> pk(npk);
     const size_t base = (size_t)(e >> 5) * npk * 32 + (e & 31);
@@ -488,6 +489,7 @@ int topo_fem_element_matrix(topo_ctx* ctx, int e, double* ke) {
     for (int i = 0; i < nd; i++)
         for (int j = i; j < nd; j++, k++) { ke[i * nd + j] = pk[k]; ke[j * nd + i] = pk[k]; }
     return 0;
+    GUARD_END
 }
 
 int topo_fem_apply(topo_ctx* ctx, const double* xphys_d, const double* u_d, double* y_d) {
@@ -777,6 +779,7 @@ int topo_profile_enable(topo_ctx* ctx, int on) {
 int topo_profile_read(topo_ctx* ctx, int slot, long* launches, double* total_ms) {
     if (!ctx || !launches || !total_ms || slot < 0 || slot >= PS_COUNT) { set_error("bad argument"); return TOPO_ERR_ARG; }
     Ctx& c = ctx->c;
+    GUARD_BEGIN
     TCK(cudaStreamSynchronize(c.s));
     double tot = 0.0;
     for (auto& pr : c.prof.rec[slot]) {
@@ -790,6 +793,7 @@ int topo_profile_read(topo_ctx* ctx, int slot, long* launches, double* total_ms)
     *total_ms = tot;
     c.prof.rec[slot].clear();
     return 0;
+    GUARD_END
 }
 
 int topo_amg_level(topo_ctx* ctx, int level, int which, int* nrows, int* ncols, int* bs_r, int* bs_c, long* nnzb,

@@ -190,11 +190,18 @@ int topo_server_run(topo_server* s) {
     if (!s) { set_error("null server"); return TOPO_ERR_ARG; }
     if (s->ran) { set_error("the server already ran"); return TOPO_ERR_ARG; }
     s->ran = true;
-    std::vector<int> order(s->jobs.size());
+    std::vector<int> order;
+    std::vector<std::thread> workers;
+    try {  // before any worker starts; thread starts are guarded below
+        order.resize(s->jobs.size());
+        workers.reserve(s->jobs.size());
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return TOPO_ERR_OOM;
+    }
     for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
     std::stable_sort(order.begin(), order.end(),
                      [&](int a, int b) { return s->jobs[a].arrival_s < s->jobs[b].arrival_s; });
-    std::vector<std::thread> workers;
     const auto t0 = Clock::now();
     size_t next = 0;
     {
@@ -262,6 +269,7 @@ int topo_server_job(topo_server* s, int job_id, int* status, int* n_iters, doubl
 
 int topo_server_stats_get(topo_server* s, topo_server_stats* st) {
     if (!s || !st) { set_error("null argument"); return TOPO_ERR_ARG; }
+    try {
     std::vector<double> lat, wait;
     int done = 0, failed = 0;
     long iters = 0;
@@ -296,6 +304,10 @@ int topo_server_stats_get(topo_server* s, topo_server_stats* st) {
     st->p50_queue_s = pct(wait, 0.5);
     st->p99_queue_s = pct(wait, 0.99);
     return 0;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return TOPO_ERR_OOM;
+    }
 }
 
 }  // extern "C"
