@@ -159,23 +159,30 @@ static void run_job(topo_server* s, Job* j, Clock::time_point t0) {
     int rc = topo_create(&j->p, j->nen, j->nn, j->vertex.data(), j->ne, j->element.data(), (int)j->fixed.size(),
                          j->fixed.data(), j->ncases, j->case_ptr.data(), j->load_dofs.data(), j->load_vals.data(),
                          nullptr, &ctx);
-    if (rc >= 0) rc = topo_opt_init(ctx);
-    for (int it = 0; rc >= 0 && it < j->iterations; it++) {
-        auto a = Clock::now();
-        int itr = 0;
-        double fx = 0.0, gx = 0.0, ch = 0.0;
-        rc = topo_opt_step(ctx, &itr, &fx, &gx, &ch);
-        auto b = Clock::now();
-        j->iter_ms.push_back(std::chrono::duration<double, std::milli>(b - a).count());
-        j->fx_hist.push_back(fx);
+    try {  // an exception must not leave this thread
+        if (rc >= 0) rc = topo_opt_init(ctx);
+        j->iter_ms.reserve(j->iterations);
+        j->fx_hist.reserve(j->iterations);
+        for (int it = 0; rc >= 0 && it < j->iterations; it++) {
+            auto a = Clock::now();
+            int itr = 0;
+            double fx = 0.0, gx = 0.0, ch = 0.0;
+            rc = topo_opt_step(ctx, &itr, &fx, &gx, &ch);
+            auto b = Clock::now();
+            j->iter_ms.push_back(std::chrono::duration<double, std::milli>(b - a).count());
+            j->fx_hist.push_back(fx);
+        }
+        if (rc >= 0) {
+            double* xp = nullptr;
+            j->xphys.resize(j->ne);
+            rc = topo_opt_vector(ctx, 1, &xp);
+            if (rc >= 0) rc = topo_memcpy_d2h(j->xphys.data(), xp, sizeof(double) * j->ne, ctx);
+        }
+        if (rc < 0) j->error = topo::last_error();
+    } catch (...) {
+        rc = TOPO_ERR_OOM;
+        j->error = "host allocation failed";
     }
-    if (rc >= 0) {
-        double* xp = nullptr;
-        j->xphys.resize(j->ne);
-        rc = topo_opt_vector(ctx, 1, &xp);
-        if (rc >= 0) rc = topo_memcpy_d2h(j->xphys.data(), xp, sizeof(double) * j->ne, ctx);
-    }
-    if (rc < 0) j->error = topo::last_error();
     if (ctx) topo_destroy(ctx);
     std::lock_guard<std::mutex> lk(s->mu);
     j->status = rc;
