@@ -174,3 +174,16 @@ def test_invalid_solver_options_rejected_before_any_device_work(T, field, value)
     with pytest.raises(T.TopoError) as ei:
         _create(T, v, e, f, ld, lv, **{field: value})
     assert ei.value.code == -1 and field in str(ei.value)
+
+
+def test_job_footprint_estimate_is_monotone(T):
+    """The serving admission estimate grows with the mesh, is larger for the
+    FP64 form than for the mixed one, and covers the per-element node-row Ke
+    copy of the level-0 assembly (3 x 3nen values per (element, node) pair)."""
+    for nen in (8, 4):
+        small = T.estimate_job_bytes(nen, 10_000, 9_000, T.PREC_MIXED)
+        big = T.estimate_job_bytes(nen, 400_000, 390_000, T.PREC_MIXED)
+        assert big > small > 96 * (1 << 20)
+        assert T.estimate_job_bytes(nen, 400_000, 390_000, T.PREC_FP64) > big
+        more_elems = T.estimate_job_bytes(nen, 400_000, 780_000, T.PREC_MIXED)
+        assert more_elems - big >= 390_000 * 9 * nen * nen * 4
