@@ -30,3 +30,26 @@ def test_roofline_byte_model_inputs(T, O):
     assert bench.kmv_bytes(ctx, 8) == ctx.ne * (32 + 4 + 8 + 2400) + ctx.nn * 3 * 16
     assert bench.cheb0_bytes(ctx, nnzb, 4) == nnzb * 40 + (ctx.nn + 1) * 4 + ctx.ndof * 28
     orc.close()
+
+
+def test_reference_arm_line_contract(tmp_path):
+    """`bench.py --impl reference` (the CPU restatement timed on the host
+    cores) prints one JSON line with the bench contract's keys, its own
+    cpu_baseline and an e2e entry without host-device copies."""
+    import json
+    import os
+    import subprocess
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", "hex8-8k",
+                        "--steps", "1", "--warmup", "0"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert d["config"]["workload"].startswith("hex8-8k")
