@@ -42,6 +42,7 @@ extern "C" {
 #define TOPO_ERR_UNSUPPORTED (-6)
 #define TOPO_ERR_TIMEOUT (-7)
 #define TOPO_ERR_IO (-8)
+#define TOPO_ERR_CANCELLED (-9)
 
 #define TOPO_PREC_FP64 0  /* FP64 everywhere (the drop-in form) */
 #define TOPO_PREC_MIXED 1 /* FP32 AMG V-cycle inside FP64 FGMRES */
@@ -290,11 +291,30 @@ int topo_server_submit(topo_server* s, const topo_params* p, int nen, int n_node
                        double arrival_s, int* job_id);
 /* runs every submitted job to completion (real-time arrivals); blocks */
 int topo_server_run(topo_server* s);
+/* Cancels a job; safe to call from another thread while topo_server_run is
+ * running.  A queued job is never admitted; a running job stops between two
+ * design iterations (none of its work is in flight then) and frees its slot
+ * and memory.  Its status becomes TOPO_ERR_CANCELLED and the iterations it
+ * finished stay readable through topo_server_job. */
+int topo_server_cancel(topo_server* s, int job_id);
 /* per-job results (host arrays sized by the caller; NULL to skip):
  * iteration latencies (ms) and compliance history, final XPhys */
 int topo_server_job(topo_server* s, int job_id, int* status, int* n_iters, double* iter_ms, double* fx_hist,
                     double* xphys, double* admit_s, double* finish_s);
 int topo_server_stats_get(topo_server* s, topo_server_stats* st);
+
+/* Bounds of the device-side waits of this context, for tests of the timeout
+ * path (no counterpart in the reference, which has no device waits).
+ *   barrier_spins  polls of the MMA dual solve's grid barrier before it gives
+ *                  up (0 = default, about a second)
+ *   copy_cycles    clock cycles the block operator waits for one bulk copy of
+ *                  element matrices (0 = default, about a second)
+ *   hold           1: the waits are made to run out without any fault: the
+ *                  barrier's last arrival does not release the others and the
+ *                  block operator issues no copy.  The call then returns
+ *                  TOPO_ERR_TIMEOUT and the context stays usable; 0 restores
+ *                  normal operation. */
+int topo_test_wait_limits(topo_ctx* ctx, unsigned barrier_spins, unsigned long long copy_cycles, int hold);
 
 /* ---------------------------------------------------------------- instrumentation */
 /* Kernel launches issued by this library in this process (all contexts). */

@@ -183,10 +183,12 @@ class MMA {
     int Update(Vec& xval, const Vec& dfdx, const double* gx, const Vec& dgdx, const Vec& xmin, const Vec& xmax) {
         return topo_mma_update(c_, xval.data(), dfdx.data(), gx, dgdx.data(), xmin.data(), xmax.data());
     }
-    double DesignChange(const Vec& x, Vec& xold) {
-        double ch = -1.0;
-        if (topo_mma_design_change(c_, x.data(), xold.data(), &ch) < 0) return -1.0;
-        return ch;
+    // MMA::DesignChange (MMA.cpp:391-410) returns ch; here ch comes back
+    // through the out-parameter and the status is returned, so that a failed
+    // call reaches the caller's TOPO_CHKERR instead of looking like a
+    // converged design
+    int DesignChange(const Vec& x, Vec& xold, double* ch) {
+        return topo_mma_design_change(c_, x.data(), xold.data(), ch);
     }
     int SetAsymptotes(double init, double decrease, double increase) {
         return topo_mma_set_asymptotes(c_, init, decrease, increase);

@@ -1244,12 +1244,12 @@ int or_amg_aggregates(or_ctx* c, int level, int* agg) {
 }
 
 /* SolveFem::ComputeObjectiveAndSensitivities (SolveFem.cpp:159-265) */
-int or_fem_obj_sens(or_ctx* c, const double* xphys, double* fx, double* gx, double* dfdx, double* dgdx, double* Uout) {
+/* the sums of ComputeObjectiveAndSensitivities (SolveFem.cpp:208-249) for a
+ * given displacement U: fx = sum E_e u_e'Ke u_e, dfdx, gx[0], dgdx[0] */
+void or_obj_sens_given_u(or_ctx* c, const double* xphys, const double* U, double* fx, double* gx, double* dfdx,
+                         double* dgdx) {
     const or_params* p = &c->p;
-    int n = c->n, nen = c->nen, nd = c->ndof_e, ne = c->ne;
-    or_assemble(c, xphys);
-    double* U = Uout ? Uout : malloc(n * sizeof(double));
-    int rc = or_solve(c, U, NULL, NULL);
+    int nen = c->nen, nd = c->ndof_e, ne = c->ne;
     double f = 0.0, g = 0.0;
 #pragma omp parallel for schedule(static) reduction(+ : f, g)
     for (int e = 0; e < ne; e++) {
@@ -1269,6 +1269,13 @@ int or_fem_obj_sens(or_ctx* c, const double* xphys, double* fx, double* gx, doub
     *fx = f;
     for (int i = 0; i < p->m; i++) gx[i] = 0.0;
     gx[0] = g / c->TV - p->volfrac;
+}
+
+int or_fem_obj_sens(or_ctx* c, const double* xphys, double* fx, double* gx, double* dfdx, double* dgdx, double* Uout) {
+    or_assemble(c, xphys);
+    double* U = Uout ? Uout : malloc(c->n * sizeof(double));
+    int rc = or_solve(c, U, NULL, NULL);
+    or_obj_sens_given_u(c, xphys, U, fx, gx, dfdx, dgdx);
     if (!Uout) free(U);
     return rc;
 }
@@ -1622,6 +1629,55 @@ void or_mma_state(or_ctx* c, double* xo1, double* xo2, double* L, double* U, int
     if (L) memcpy(L, c->L, b);
     if (U) memcpy(U, c->U, b);
     if (k) *k = c->mk;
+}
+
+/* MMA::SetAsymptotes (MMA.cpp:345-353), SetRobustAsymptotesType (MMA.cpp:355-368; any
+ * value other than 0 or 1 falls back to 0) and the constraintModification flag
+ * (MMA.h:32-35) */
+void or_mma_options(or_ctx* c, double asyminit, double asymdec, double asyminc, int robust, int constraint_mod) {
+    c->asyminit = asyminit; c->asymdec = asymdec; c->asyminc = asyminc;
+    c->RobustAsymptotesType = (robust == 0 || robust == 1) ? robust : 0;
+    c->constraintModification = constraint_mod ? 1 : 0;
+}
+
+/* the restart constructor MMA(n, m, k, xo1, xo2, U, L) (MMA.cpp:91-176): the
+ * history vectors and the iteration counter k are loaded */
+void or_mma_restart_set(or_ctx* c, const double* xo1, const double* xo2, const double* U, const double* L, int k) {
+    size_t b = c->ne * sizeof(double);
+    memcpy(c->xo1, xo1, b); memcpy(c->xo2, xo2, b); memcpy(c->U, U, b); memcpy(c->L, L, b);
+    c->mk = k;
+}
+
+/* MMA::KKTresidual (MMA.cpp:412-480) with the multipliers of the last
+ * Update: per element the stationarity residual of the box-constrained
+ * Lagrangian and the two complementarity terms; then the constraint term
+ * lam_j (a_j z + y_j - g_j); norm2 is the root of the sum of squares */
+void or_mma_kkt_residual(or_ctx* c, const double* x, const double* dfdx, const double* gx, const double* dgdx,
+                         const double* xmin, const double* xmax, double* norm2, double* norm_inf) {
+    int n = c->ne, m = c->p.m;
+    double n2 = 0.0, ni = 0.0;
+    for (int i = 0; i < n; i++) {
+        double ri = dfdx[i];
+        for (int j = 0; j < m; j++) ri += c->lam[j] * dgdx[(size_t)j * n + i];
+        double mu_min = 0.0, mu_max = 0.0;
+        if (x[i] < xmin[i] + 1.0e-5 && ri > 0.0) mu_min = ri;
+        if (x[i] > xmax[i] - 1.0e-5 && ri < 0.0) mu_max = -ri;
+        ri += -mu_min + mu_max;
+        n2 += ri * ri;
+        ni = dmax(fabs(ri), ni);
+        double resi = mu_min * (x[i] - xmin[i]);
+        n2 += resi * resi;
+        ni = dmax(fabs(resi), ni);
+        resi = mu_max * (xmax[i] - x[i]);
+        n2 += resi * resi;
+        ni = dmax(fabs(resi), ni);
+    }
+    double ri = 0.0;
+    for (int j = 0; j < m; j++) ri += c->lam[j] * (c->a[j] * c->z + c->y[j] - gx[j]);
+    n2 += ri * ri;
+    ni = dmax(fabs(ri), ni);
+    *norm2 = sqrt(n2);
+    *norm_inf = ni;
 }
 
 /* main.cpp:64-119 loop */

@@ -73,6 +73,8 @@ int     or_kmatvec(or_ctx* c, const double* u, double* y);
 int     or_solve(or_ctx* c, double* U, int* its, double* relres);
 int     or_fem_obj_sens(or_ctx* c, const double* xphys, double* fx, double* gx,
                         double* dfdx, double* dgdx, double* U);
+void    or_obj_sens_given_u(or_ctx* c, const double* xphys, const double* U, double* fx, double* gx,
+                            double* dfdx, double* dgdx);
 /* PDEFilter */
 int     or_filter(or_ctx* c, const double* x, double* xf, double Xmin);
 int     or_filter_sens(or_ctx* c, double* dfdx, double* dgdx, int m);
@@ -88,6 +90,10 @@ int     or_mma_update(or_ctx* c, double* xval, const double* dfdx, const double*
                       const double* dgdx, const double* xmin, const double* xmax);
 double  or_mma_design_change(or_ctx* c, const double* x, double* xold);
 void    or_mma_state(or_ctx* c, double* xo1, double* xo2, double* L, double* U, int* k);
+void    or_mma_options(or_ctx* c, double asyminit, double asymdec, double asyminc, int robust, int constraint_mod);
+void    or_mma_restart_set(or_ctx* c, const double* xo1, const double* xo2, const double* U, const double* L, int k);
+void    or_mma_kkt_residual(or_ctx* c, const double* x, const double* dfdx, const double* gx, const double* dgdx,
+                            const double* xmin, const double* xmax, double* norm2, double* norm_inf);
 /* AMG introspection (aggregation is integer work: compared bit-exactly) */
 int     or_amg_aggregates(or_ctx* c, int level, int* agg /*rows of level*/);
 /* main.cpp loop: returns iterations done; hist = [fx, gx0, ch] per iteration */

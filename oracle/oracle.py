@@ -78,6 +78,7 @@ def lib():
         L.or_kmatvec.argtypes = [C.c_void_p, _f64p, _f64p]
         L.or_solve.argtypes = [C.c_void_p, _f64p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.or_fem_obj_sens.argtypes = [C.c_void_p, _f64p, C.POINTER(C.c_double), _f64p, _f64p, _f64p, C.c_void_p]
+        L.or_obj_sens_given_u.argtypes = [C.c_void_p, _f64p, _f64p, C.POINTER(C.c_double), _f64p, _f64p, _f64p]
         L.or_filter.argtypes = [C.c_void_p, _f64p, _f64p, C.c_double]
         L.or_filter_sens.argtypes = [C.c_void_p, _f64p, _f64p, C.c_int]
         L.or_filter_state.argtypes = [C.c_void_p, _f64p, C.c_int]
@@ -91,6 +92,9 @@ def lib():
         L.or_mma_design_change.argtypes = [C.c_void_p, _f64p, _f64p]
         L.or_mma_design_change.restype = C.c_double
         L.or_mma_state.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.POINTER(C.c_int)]
+        L.or_mma_options.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]
+        L.or_mma_restart_set.argtypes = [C.c_void_p, _f64p, _f64p, _f64p, _f64p, C.c_int]
+        L.or_mma_kkt_residual.argtypes = [C.c_void_p] + [_f64p] * 6 + [C.POINTER(C.c_double)] * 2
         L.or_amg_aggregates.argtypes = [C.c_void_p, C.c_int, _i32p]
         L.or_run.argtypes = [C.c_void_p, C.c_int, C.c_double, _f64p, _f64p]
         _lib = L
@@ -283,6 +287,17 @@ class Oracle:
         out = (fx.value, gx, df, dg.reshape(m, self.ne))
         return out + (U,) if return_u else out
 
+    def obj_sens_given_u(self, xphys, U):
+        """Compliance, volume constraint and sensitivities for a given U (no solve)."""
+        m = self.p.m
+        fx = C.c_double()
+        gx = np.zeros(m)
+        df = np.zeros(self.ne)
+        dg = np.zeros(self.ne * m)
+        lib().or_obj_sens_given_u(self.h, np.ascontiguousarray(xphys, dtype=np.float64),
+                                  np.ascontiguousarray(U, dtype=np.float64), C.byref(fx), gx, df, dg)
+        return fx.value, gx, df, dg.reshape(m, self.ne)
+
     def filter(self, x, Xmin):
         xf = np.zeros(self.ne)
         lib().or_filter(self.h, np.ascontiguousarray(x, dtype=np.float64), xf, Xmin)
@@ -337,6 +352,20 @@ class Oracle:
         k = C.c_int()
         lib().or_mma_state(self.h, *[x.ctypes.data for x in a], C.byref(k))
         return a + [k.value]
+
+    def mma_options(self, asyminit=0.5, asymdec=0.7, asyminc=1.2, robust=0, constraint_mod=0):
+        lib().or_mma_options(self.h, asyminit, asymdec, asyminc, robust, constraint_mod)
+
+    def mma_restart_set(self, xo1, xo2, U, L, k):
+        f = lambda a: np.ascontiguousarray(a, dtype=np.float64).ravel()
+        lib().or_mma_restart_set(self.h, f(xo1), f(xo2), f(U), f(L), k)
+
+    def mma_kkt(self, x, dfdx, gx, dgdx, xmin, xmax):
+        f = lambda a: np.ascontiguousarray(a, dtype=np.float64).ravel()
+        n2, ni = C.c_double(), C.c_double()
+        lib().or_mma_kkt_residual(self.h, f(x), f(dfdx), f(gx), f(dgdx), f(xmin), f(xmax), C.byref(n2),
+                                  C.byref(ni))
+        return n2.value, ni.value
 
     def amg_aggregates(self, level):
         nnode = self.nn if level == 0 else None

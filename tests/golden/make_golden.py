@@ -17,6 +17,7 @@ present.
 """
 import json
 import os
+import shutil
 import sys
 
 import numpy as np
@@ -146,7 +147,11 @@ def cases():
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    """usage: make_golden.py REFERENCE_ROOT (or TOPO_REFERENCE_ROOT in the environment): the checkout of the
+    reference whose mesh/ boundary-condition files are copied into tests/golden/reference_mesh/"""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TOPO_REFERENCE_ROOT")
+    if not ref:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT (or set TOPO_REFERENCE_ROOT)")
     out = {"nu": 0.3, "rmin": 1.5, "cases": {}}
     for name, co in cases().items():
         rec = {"coords": co.tolist()}
@@ -172,6 +177,13 @@ def main():
             "n_fixed_nodes": int(fixed.size // 3), "n_load": int(ld.size),
             "load_dofs_mod3": sorted(set(int(x) for x in ld % 3)), "load_values": sorted(set(float(x) for x in lv)),
             "lattice": [140, 70, 40]}
+        # the reference's own boundary-condition files, byte for byte, so that
+        # tests can read them through the library's mesh reader where the
+        # reference checkout is absent
+        dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_mesh")
+        os.makedirs(dst, exist_ok=True)
+        for name in ("fixeddofs.txt", "loaddof_1.txt", "load_1.txt"):
+            shutil.copyfile(os.path.join(mesh, name), os.path.join(dst, name))
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "element_kat.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1)

@@ -121,6 +121,46 @@ def test_mesh_dir_roundtrip(T, tmp_path):
     assert ei.value.code == -8  # TOPO_ERR_IO ("Can't found document")
 
 
+REF_MESH = os.path.join(ROOT, "tests", "golden", "reference_mesh")
+
+
+def read_reference_bcs(T, tmp_path):
+    """The reference's own boundary-condition files (mesh/fixeddofs.txt,
+    loaddof_1.txt, load_1.txt, copied byte for byte by
+    tests/golden/make_golden.py) read through topo_read_mesh_dir, beside a
+    one-element vertex/element pair (the reference's mesh blobs are not
+    in its repository)."""
+    import shutil
+    for name in ("fixeddofs.txt", "loaddof_1.txt", "load_1.txt"):
+        shutil.copyfile(os.path.join(REF_MESH, name), tmp_path / name)
+    v, e, _, _, _ = T.gen_cantilever(1, 1, 1, 8)
+    np.savetxt(tmp_path / "vertex.txt", v, fmt="%.17g")
+    np.savetxt(tmp_path / "element.txt", e, fmt="%d")
+    return T.read_mesh_dir(str(tmp_path), 8, 1)
+
+
+def test_reference_bc_files_through_the_reader(T, tmp_path):
+    """InputMeshData::GetBcs (InputMeshData.cpp:228-285) reads Load = 41 load
+    DOFs and values and StrucDofs = 8733 fixed DOFs (OptPara.cpp:5-11); the
+    library's reader returns exactly the files' numbers: whole nodes clamped
+    (DOF triples 3n, 3n+1, 3n+2) and unit loads on y DOFs (3n+1)."""
+    _, _, f, ld, lv, cp = read_reference_bcs(T, tmp_path)
+    assert f.size == 8733 and ld.size == 41 and lv.size == 41 and list(cp) == [0, 41]
+    raw = lambda n: np.loadtxt(os.path.join(REF_MESH, n)).ravel()
+    assert np.array_equal(f, raw("fixeddofs.txt").astype(np.int32))
+    assert np.array_equal(ld, raw("loaddof_1.txt").astype(np.int32))
+    assert np.array_equal(lv, raw("load_1.txt"))
+    trip = f.reshape(-1, 3)
+    assert np.all(trip[:, 0] % 3 == 0) and np.all(trip == trip[:, :1] + np.arange(3))
+    assert np.all(ld % 3 == 1) and np.all(lv == 1.0)
+    assert np.unique(f).size == f.size and np.unique(ld).size == ld.size
+    ref = os.environ.get("TOPO_REFERENCE_ROOT")  # where a checkout of the reference is at hand
+    if ref and os.path.isdir(os.path.join(ref, "mesh")):
+        for name in ("fixeddofs.txt", "loaddof_1.txt", "load_1.txt"):
+            with open(os.path.join(ref, "mesh", name), "rb") as a, open(os.path.join(REF_MESH, name), "rb") as b:
+                assert a.read() == b.read(), name
+
+
 def _create(T, v, e, f, ld, lv, **kw):
     return T.Context(v, e, f, ld, lv, stream=0, **kw)
 

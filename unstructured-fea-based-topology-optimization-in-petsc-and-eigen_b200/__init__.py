@@ -23,6 +23,10 @@ LIB_PATH = os.path.join(HERE, "libtopo.so")
 
 TOPO_OK = 0
 TOPO_NOT_CONVERGED = 1
+TOPO_ERR_ARG = -1
+TOPO_ERR_NAN = -5
+TOPO_ERR_TIMEOUT = -7
+TOPO_ERR_CANCELLED = -9
 PREC_FP64 = 0
 PREC_MIXED = 1
 
@@ -120,6 +124,8 @@ _SIGS = {
                             C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
                             C.POINTER(C.c_int)], C.c_int),
     "topo_server_run": ([C.c_void_p], C.c_int),
+    "topo_server_cancel": ([C.c_void_p, C.c_int], C.c_int),
+    "topo_test_wait_limits": ([C.c_void_p, C.c_uint, C.c_ulonglong, C.c_int], C.c_int),
     "topo_server_job": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)] + [C.c_void_p] * 3 +
                         [_dp, _dp], C.c_int),
     "topo_server_stats_get": ([C.c_void_p, C.c_void_p], C.c_int),
@@ -428,6 +434,20 @@ class Context:
                "mma_restart")
         return [xo1, xo2, L, U, k.value]
 
+    def mma_options(self, asyminit=0.5, asymdec=0.7, asyminc=1.2, robust=0, constraint_mod=0):
+        """MMA::SetAsymptotes, SetRobustAsymptotesType and the
+        constraintModification flag."""
+        L = lib()
+        _check(L.topo_mma_set_asymptotes(self.h, asyminit, asymdec, asyminc), "mma_set_asymptotes")
+        _check(L.topo_mma_set_robust_asymptotes_type(self.h, robust), "mma_set_robust_asymptotes_type")
+        _check(L.topo_mma_constraint_modification(self.h, constraint_mod), "mma_constraint_modification")
+
+    def mma_restart_set(self, xo1, xo2, U, L, k):
+        """The restart constructor's import of the MMA history (MMA.h:15-18)."""
+        kk = C.c_int(k)
+        _check(lib().topo_mma_restart(self.h, _dptr(xo1.contiguous()), _dptr(xo2.contiguous()),
+                                      _dptr(U.contiguous()), _dptr(L.contiguous()), C.byref(kk), 1), "mma_restart")
+
     def mma_kkt(self, x, dfdx, gx, dgdx, xmin, xmax):
         n2, ni = C.c_double(), C.c_double()
         g = np.ascontiguousarray(gx, dtype=np.float64)
@@ -493,6 +513,11 @@ class Context:
         n = n or (self.ne * self.m if which == 5 else self.ne)
         return device_view(self.opt_vector(which), n).clone()
 
+    def test_wait_limits(self, barrier_spins=0, copy_cycles=0, hold=0):
+        """Bounds of the device-side waits; hold=1 makes them run out (tests of
+        the timeout path)."""
+        _check(lib().topo_test_wait_limits(self.h, barrier_spins, copy_cycles, hold), "test_wait_limits")
+
     def write_vtu(self, directory, itr, xphys=None):
         _check(lib().topo_write_vtu(self.h, directory.encode(), itr, _dptr(xphys)), "write_vtu")
 
@@ -548,6 +573,10 @@ class Server:
 
     def run(self):
         return _check(lib().topo_server_run(self.h), "server_run")
+
+    def cancel(self, jid):
+        """Cancel a job (safe while run() is blocking in another thread)."""
+        _check(lib().topo_server_cancel(self.h, jid), "server_cancel")
 
     def job(self, jid):
         _, ne, iters = self.jobs[jid]

@@ -689,6 +689,15 @@ int topo_mma_kkt_residual(topo_ctx* ctx, const double* x_d, const double* dfdx_d
     return mma_kkt(c, x_d, dfdx_d, c.dsc.p + DS_TMP + 1, dgdx_d, xmin_d, xmax_d, norm2, norm_inf);
 }
 
+int topo_test_wait_limits(topo_ctx* ctx, unsigned barrier_spins, unsigned long long copy_cycles, int hold) {
+    if (!ctx || (hold != 0 && hold != 1)) { set_error("bad argument"); return TOPO_ERR_ARG; }
+    Ctx::WaitLimits d;
+    ctx->c.wait.barrier_spins = barrier_spins ? barrier_spins : d.barrier_spins;
+    ctx->c.wait.copy_cycles = copy_cycles ? copy_cycles : d.copy_cycles;
+    ctx->c.wait.hold = hold;
+    return 0;
+}
+
 // ---------------------------------------------------------------- main loop
 int topo_opt_init(topo_ctx* ctx) {
     if (!ctx) { set_error("null context"); return TOPO_ERR_ARG; }

@@ -33,7 +33,6 @@ namespace topo {
 constexpr int kWarps = 8;      // warps (= elements per phase) per CTA
 constexpr int kStages = 3;     // Ke copies in flight per warp
 constexpr int kChunkElems = 64;
-constexpr unsigned long long kWaitCycles = 2000000000ull;  // ~1 s at 2 GHz
 
 // ----------------------------------------------------------------- host: chunks and phases
 // spread the low 21 bits of v to every third bit (3D Morton code)
@@ -220,12 +219,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// bounded wait: false after ~kWaitCycles
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// bounded wait: false after `limit` clock cycles (Ctx::WaitLimits, about a
+// second by default)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long limit) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 // global -> shared bulk copy through the TMA engine (no multicast)
@@ -265,6 +265,8 @@ struct BlkArgs {
     const double* Es;        // slot -> element modulus
     int max_nodes;           // largest chunk node count (shared image rows)
     int* err;
+    unsigned long long wait_cycles;  // bound of each copy wait
+    int hold;                // test form: issue no copy, so every wait runs out
 };
 
 // MODE 0: y[dof][case] += alpha E_e (Ke_e U_e) over all elements, Dirichlet
@@ -308,7 +310,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
     auto issue = [&]() {
         const int s0 = a.ph_sl[pp], cnt = a.ph_sl[pp + 1] - s0;
         const int st = pq % kStages;
-        if (warp < cnt) {
+        if (warp < cnt && !a.hold) {
             if (lane == 0) {
                 fence_proxy_async();
                 mbar_expect_tx(&bar[warp * kStages + st], NPK * 8);
@@ -402,7 +404,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
         load_meta(c2, p2, mnn);
         load_b(mn, bnxt);
         if (mc.has) {
-            if (mbar_wait(&bar[warp * kStages + st], (parity >> st) & 1u)) {
+            if (mbar_wait(&bar[warp * kStages + st], (parity >> st) & 1u, a.wait_cycles)) {
                 parity ^= 1u << st;
                 pending &= ~(1u << st);
             } else {
@@ -481,7 +483,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
     // on an abort, let this warp's copies in flight land before the CTA exits
     if (lane == 0 && pending) {
         for (int s = 0; s < kStages; s++)
-            if ((pending >> s) & 1u) mbar_wait(&bar[warp * kStages + s], (parity >> s) & 1u);
+            if ((pending >> s) & 1u) mbar_wait(&bar[warp * kStages + s], (parity >> s) & 1u, a.wait_cycles);
     }
 }
 
@@ -539,7 +541,7 @@ static int launch_blk(Ctx& c, const TU* u, double* y, double alpha, double* uku)
     const int per_sm = c.tune.blk_ctas > 0 ? std::min(std::max(1, occ), c.tune.blk_ctas) : std::max(1, occ);
     const int grid = std::max(1, std::min(B.nchunks, per_sm * nsm));
     BlkArgs a{B.nchunks, B.ch_ph.p, B.ph_sl.p, B.ch_np.p, B.ch_nodes.p, B.sl_elem.p, B.sl_gn.p, B.sl_lc.p,
-              B.sl_mask.p, B.keb.p, B.Es.p, B.max_nodes, B.err.p};
+              B.sl_mask.p, B.keb.p, B.Es.p, B.max_nodes, B.err.p, c.wait.copy_cycles, c.wait.hold};
     kern<<<grid, kWarps * 32, smem, c.s>>>(a, u, y, alpha, uku), note_launch();
     TCK(cudaGetLastError());
     return 0;
@@ -633,7 +635,13 @@ int blk_check_error(Ctx& c) {
     int h = 0;
     TCK(cudaMemcpyAsync(&h, c.blk.err.p, sizeof(int), cudaMemcpyDeviceToHost, c.s));
     TCK(cudaStreamSynchronize(c.s));
-    if (h) { set_error("block operator: a TMA copy did not complete in time"); return TOPO_ERR_CUDA; }
+    if (h) {
+        // reported once; the flag is cleared so the context stays usable
+        TCK(cudaMemsetAsync(c.blk.err.p, 0, sizeof(int), c.s));
+        TCK(cudaStreamSynchronize(c.s));
+        set_error("block operator: a TMA copy did not complete in time");
+        return TOPO_ERR_TIMEOUT;
+    }
     return 0;
 }
 

@@ -185,14 +185,19 @@ __device__ __forceinline__ double block_max(double v, double* smem) {
 
 // Bounded grid barrier for kernels launched with cudaLaunchCooperativeKernel
 // (co-residency guaranteed by the launch).  Every wait polls at most
-// kBarrierSpin times; on expiry it raises *err and returns false so the
-// kernel can unwind instead of hanging the device.
+// spin_limit times (kBarrierSpin by default, about a second); on expiry it
+// raises *err and returns false so the kernel can unwind instead of hanging
+// the device.  hold != 0 is the test form of a barrier that never opens:
+// the last block to arrive does not release the others, so every block's
+// wait runs out and the kernel reports the timeout.
 constexpr unsigned kBarrierSpin = 1u << 24;
 
 struct GridBarrier {
     unsigned* count;   // arrivals in the current generation
     unsigned* gen;     // generation counter
     int* err;          // set to 1 on timeout
+    unsigned spin_limit;
+    int hold;
 };
 
 __device__ __forceinline__ bool grid_sync(const GridBarrier& b) {
@@ -204,14 +209,14 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& b) {
         unsigned g = *vgen;
         __threadfence();
         unsigned arrived = atomicAdd(b.count, 1u) + 1u;
-        if (arrived == gridDim.x) {
+        if (arrived == gridDim.x && !b.hold) {
             *b.count = 0;
             __threadfence();
             atomicAdd(b.gen, 1u);
         } else {
             unsigned spins = 0;
             while (*vgen == g) {
-                if (++spins > kBarrierSpin || *(volatile int*)b.err) {
+                if (++spins > b.spin_limit || *(volatile int*)b.err) {
                     atomicExch(b.err, 1);
                     s_ok = 0;
                     break;

@@ -232,6 +232,13 @@ struct Ctx {
 
     // ---- MMA (MMA.cpp state)
     int mma_k = 0;
+    // bounds of the device-side waits (grid barrier spins, bulk-copy wait
+    // cycles) and the test form that makes them run out (topo_test_wait_limits)
+    struct WaitLimits {
+        unsigned barrier_spins = 1u << 24;
+        unsigned long long copy_cycles = 2000000000ull;  // about a second at 2 GHz
+        int hold = 0;
+    } wait;
     double asyminit = 0.5, asymdec = 0.7, asyminc = 1.2;
     int constraint_mod = 0, robust_type = 0;
     std::vector<double> a, c, d;

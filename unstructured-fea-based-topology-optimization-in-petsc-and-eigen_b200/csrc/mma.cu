@@ -480,7 +480,7 @@ static int update_m(Ctx& c, double* x, const double* dfdx, const double* gx_dev,
     double* part2 = part + (size_t)2048 * (M + M * M);
     TCK(cudaMemsetAsync(c.bar.p, 0, 2 * sizeof(unsigned), c.s));
     TCK(cudaMemsetAsync(c.bar_err.p, 0, sizeof(int), c.s));
-    GridBarrier gb{c.bar.p, c.bar.p + 1, c.bar_err.p};
+    GridBarrier gb{c.bar.p, c.bar.p + 1, c.bar_err.p, c.wait.barrier_spins, c.wait.hold};
     const double* p0 = c.p0.p; const double* q0 = c.q0.p; const double* pij = c.pij.p; const double* qij = c.qij.p;
     const double* Lp = c.L.p; const double* Up = c.Uas.p; const double* al = c.alpha.p; const double* be = c.beta.p;
     int nn = n;

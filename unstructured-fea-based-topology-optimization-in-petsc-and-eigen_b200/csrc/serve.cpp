@@ -12,9 +12,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <thread>
@@ -41,8 +43,9 @@ struct Job {
     std::vector<int32_t> element, fixed, case_ptr, load_dofs;
     double arrival_s = 0.0;
     size_t est_bytes = 0;
+    std::shared_ptr<std::atomic<int>> cancel = std::make_shared<std::atomic<int>>(0);
     // results
-    int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
+    int state = 0;  // 0 queued, 1 running, 2 done, 3 failed, 4 cancelled
     int status = 0;
     std::string error;
     double admit_s = 0.0, finish_s = 0.0;
@@ -164,6 +167,13 @@ static void run_job(topo_server* s, Job* j, Clock::time_point t0) {
         j->iter_ms.reserve(j->iterations);
         j->fx_hist.reserve(j->iterations);
         for (int it = 0; rc >= 0 && it < j->iterations; it++) {
+            // cancellation is honoured between design iterations, when none
+            // of this job's work is in flight
+            if (j->cancel->load()) {
+                rc = TOPO_ERR_CANCELLED;
+                j->error = "cancelled";
+                break;
+            }
             auto a = Clock::now();
             int itr = 0;
             double fx = 0.0, gx = 0.0, ch = 0.0;
@@ -178,7 +188,7 @@ static void run_job(topo_server* s, Job* j, Clock::time_point t0) {
             rc = topo_opt_vector(ctx, 1, &xp);
             if (rc >= 0) rc = topo_memcpy_d2h(j->xphys.data(), xp, sizeof(double) * j->ne, ctx);
         }
-        if (rc < 0) j->error = topo::last_error();
+        if (rc < 0 && rc != TOPO_ERR_CANCELLED) j->error = topo::last_error();
     } catch (...) {
         rc = TOPO_ERR_OOM;
         j->error = "host allocation failed";
@@ -186,7 +196,7 @@ static void run_job(topo_server* s, Job* j, Clock::time_point t0) {
     if (ctx) topo_destroy(ctx);
     std::lock_guard<std::mutex> lk(s->mu);
     j->status = rc;
-    j->state = rc < 0 ? 3 : 2;
+    j->state = rc == TOPO_ERR_CANCELLED ? 4 : rc < 0 ? 3 : 2;
     j->finish_s = std::chrono::duration<double>(Clock::now() - t0).count();
     s->reserved -= j->est_bytes;
     s->active--;
@@ -219,6 +229,14 @@ int topo_server_run(topo_server* s) {
             // arrived and fits (slot + estimated footprint)
             while (next < order.size()) {
                 Job& j = s->jobs[order[next]];
+                if (j.cancel->load()) {  // cancelled while queued: never admitted
+                    j.status = TOPO_ERR_CANCELLED;
+                    j.error = "cancelled";
+                    j.state = 4;
+                    j.admit_s = j.finish_s = now;
+                    next++;
+                    continue;
+                }
                 if (j.arrival_s > now || s->active >= s->max_active || s->reserved + j.est_bytes > s->budget) break;
                 j.state = 1;
                 j.admit_s = now;
@@ -259,6 +277,16 @@ int topo_server_run(topo_server* s) {
     return 0;
 }
 
+int topo_server_cancel(topo_server* s, int job_id) {
+    if (!s || job_id < 0 || job_id >= (int)s->jobs.size()) { set_error("no such job"); return TOPO_ERR_ARG; }
+    s->jobs[job_id].cancel->store(1);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->cv.notify_all();
+    }
+    return 0;
+}
+
 int topo_server_job(topo_server* s, int job_id, int* status, int* n_iters, double* iter_ms, double* fx_hist,
                     double* xphys, double* admit_s, double* finish_s) {
     if (!s || job_id < 0 || job_id >= (int)s->jobs.size()) { set_error("no such job"); return TOPO_ERR_ARG; }
@@ -270,8 +298,8 @@ int topo_server_job(topo_server* s, int job_id, int* status, int* n_iters, doubl
     if (xphys && !j.xphys.empty()) std::copy(j.xphys.begin(), j.xphys.end(), xphys);
     if (admit_s) *admit_s = j.admit_s;
     if (finish_s) *finish_s = j.finish_s;
-    if (j.state == 3) set_error("%s", j.error.c_str());
-    return j.state == 3 ? j.status : 0;
+    if (j.state >= 3) set_error("%s", j.error.c_str());
+    return j.state >= 3 ? j.status : 0;
 }
 
 int topo_server_stats_get(topo_server* s, topo_server_stats* st) {
@@ -285,7 +313,7 @@ int topo_server_stats_get(topo_server* s, topo_server_stats* st) {
         failed += j.state == 3;
         iters += (long)j.iter_ms.size();
         lat.insert(lat.end(), j.iter_ms.begin(), j.iter_ms.end());
-        if (j.state >= 2) wait.push_back(j.admit_s - j.arrival_s);
+        if (j.state == 2 || j.state == 3) wait.push_back(j.admit_s - j.arrival_s);
     }
     auto pct = [](std::vector<double> v, double q) {
         if (v.empty()) return 0.0;

@@ -542,9 +542,23 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
     return 0;
 }
 
-// SolveFem::ComputeFem (SolveFem.cpp:91-157): moduli, AMG numeric setup,
-// U = 0, FGMRES, then the true relative residual.
+static int fem_solve_impl(Ctx& c, const double* xphys, double* u);
+
+// SolveFem::ComputeFem (SolveFem.cpp:91-157).  A non-finite density (or any
+// breakdown) leaves NaNs in the warm-started spectral estimates and in U; they
+// are reset here so that the context stays usable after the error.
 int fem_solve(Ctx& c, const double* xphys, double* u) {
+    const int rc = fem_solve_impl(c, xphys, u);
+    if (rc < 0) {
+        c.u_valid = false;
+        c.blk.u_valid = c.blk.u_fresh = false;
+        amg_reset_warm_start(c);
+    }
+    return rc;
+}
+
+// moduli, AMG numeric setup, U = 0, FGMRES, then the true relative residual
+static int fem_solve_impl(Ctx& c, const double* xphys, double* u) {
     if (c.ncases > 1 && c.p.fem_block) return fem_solve_block(c, xphys, u);
     c.blk.u_valid = c.blk.u_fresh = false;
     TRET(compute_moduli(c, xphys));

@@ -62,7 +62,7 @@ int main(int argc, char** argv) {
         TOPO_CHKERR(pde.ComputeFilteredSens(opt.dfdx, opt.dgdx, opt.m));
         TOPO_CHKERR(mma.SetOuterMovelimit(opt.Xmin, opt.Xmax, opt.movlim, opt.X, opt.xmin, opt.xmax));
         TOPO_CHKERR(mma.Update(opt.X, opt.dfdx, opt.gx.data(), opt.dgdx, opt.xmin, opt.xmax));
-        ch = mma.DesignChange(opt.X, opt.Xold);
+        TOPO_CHKERR(mma.DesignChange(opt.X, opt.Xold, &ch));
         TOPO_CHKERR(pde.Filter(opt.X, opt.XFiled, opt.Xmin));
         TOPO_CHKERR(pde.HeavisideFilter(opt.XFiled, opt.XPhys, opt.x0, opt.beta0, opt.betamax, itr, opt.Xmin, opt.proj));
         double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
