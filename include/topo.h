@@ -95,6 +95,11 @@ typedef struct topo_params {
     int pdl;               /* 1 (default): V-cycle kernels use programmatic dependent launch (each
                               starts while its predecessor drains and waits on the GPU before it
                               reads the predecessor's output); 0: plain stream order */
+    int step_graph;        /* 1: from the second design iteration of a run on, the whole iteration is
+                              replayed from CUDA graphs captured once, with the FGMRES and filter-CG
+                              loops as conditional graph nodes decided on the device (no host
+                              round trip inside an iteration); 0 (default): host-driven iterations.
+                              One load case (the block solver always steps directly). */
 } topo_params;
 
 typedef struct topo_solve_info {
@@ -111,6 +116,8 @@ typedef struct topo_solve_info {
                               level-0 smoother block, reduction grid, block-operator CTAs/SM */
     int tuned_lanes[8];    /* lanes per block row picked for the smoothing and residual products
                               of AMG level l >= 1 (0: not tuned) */
+    int step_graph;        /* last design iteration: 1 replayed from the step graph, 0 stepped
+                              directly, -1 the capture failed (direct steps from then on) */
 } topo_solve_info;
 
 /* ---------------------------------------------------------------- basics */
@@ -255,6 +262,17 @@ int topo_opt_step(topo_ctx* ctx, int* itr, double* fx, double* gx0, double* ch);
 /* Runs the loop `while (itr < maxItr && ch > ch_tol)` (main.cpp:70);
  * hist (host, may be NULL) receives [fx, gx0, ch] per iteration. */
 int topo_opt_run(topo_ctx* ctx, int max_itr, double* hist, int* iterations);
+/* Advances n independent contexts (design instances) by one design iteration
+ * each (no counterpart in the reference, which runs one design per MPI job).
+ * Instances whose options select step_graph = 1 and that have done their first
+ * iteration are replayed from their step graphs: all of them are launched,
+ * each on its own context stream, before the host waits for any, so their
+ * iterations overlap on the device (the cooperative MMA dual solves run one
+ * after another); the other instances step directly, after those launches.
+ * status[i] (may be NULL) receives each instance's status, fx[i] (may be NULL)
+ * its compliance.  Returns the most severe status: the first error (< 0)
+ * met, else the largest warning.  Contexts that share a stream serialise. */
+int topo_opt_step_batch(topo_ctx* const* ctxs, int n, int* status, double* fx);
 /* Host-buffer form used end to end: uploads the design X (host, n_elems),
  * runs one iteration, downloads the updated X and XPhys (host) and fx. */
 int topo_opt_step_host(topo_ctx* ctx, const double* x_in, double* x_out, double* xphys_out, double* fx);

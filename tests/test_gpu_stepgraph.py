@@ -1,0 +1,127 @@
+"""The device-driven design iteration (step_graph = 1) and the batch of
+independent design instances (topo_opt_step_batch).
+
+From the second iteration of a run on, the whole main.cpp:72-112 loop body is
+replayed from CUDA graphs in which the FGMRES restart cycles, the Arnoldi
+steps and the filter CG iterations are conditional nodes decided on the
+device.  The same kernels run in the same order as in a host-driven step, so
+the trajectories agree to rounding: bar 1e-6 relative compliance per
+iteration (the element scatter's float atomics make two runs differ in the
+last bits, which an FGMRES stopping test can turn into one more or one fewer
+iteration), volume constraint 1e-9.  A batch advances several instances of
+different sizes and options at once; each instance's trajectory must equal
+its own solo run by the same bar.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(Emax=1.0, rmin=1.5, volfrac=0.12, fem_rtol=1e-5, ch_tol=0.0)
+
+
+def run(T, mesh, n, **kw):
+    ctx = T.Context(*mesh, stream="own", **dict(KW, **kw))
+    ctx.opt_init()
+    h = ctx.opt_run(n)
+    its = ctx.info().fem_its
+    assert ctx.info().step_graph == kw.get("step_graph", 0)  # replayed (1) or direct (0) as asked
+    xp = ctx.opt_tensor(1).cpu().numpy()
+    ctx.close()
+    return h, xp, its
+
+
+@pytest.mark.parametrize("prec,nen", [("fp64", 8), ("mixed", 8), ("mixed", 4)])
+def test_graph_step_matches_direct_step(T, cuda, prec, nen):
+    mesh = T.gen_cantilever(40, 20, 10, 8) if nen == 8 else T.gen_cantilever(12, 6, 6, 4)
+    pr = T.PREC_MIXED if prec == "mixed" else T.PREC_FP64
+    hd, xd, _ = run(T, mesh, 12, precision=pr, step_graph=0)
+    hg, xg, its = run(T, mesh, 12, precision=pr, step_graph=1)
+    assert its > 0
+    assert rel(hg[:, 0], hd[:, 0]) < 1e-6
+    assert np.abs(hg[:, 1] - hd[:, 1]).max() < 1e-9
+    assert np.abs(hg[:, 2] - hd[:, 2]).max() < 1e-6
+    assert np.abs(xg - xd).max() < 1e-5
+
+
+def test_graph_step_with_projection_crosses_beta_steps(T, cuda):
+    """proj = 1 through iteration 32: beta moves at iteration 30 on the device
+    (PDEFilter.cpp:260-268) exactly as on the host."""
+    mesh = T.gen_cantilever(16, 8, 6, 8)
+    hd, xd, _ = run(T, mesh, 32, proj=1, step_graph=0)
+    hg, xg, _ = run(T, mesh, 32, proj=1, step_graph=1)
+    assert rel(hg[:, 0], hd[:, 0]) < 1e-6
+    assert np.abs(xg - xd).max() < 1e-5
+
+
+def test_graph_step_info_and_launch_count(T, cuda):
+    mesh = T.gen_cantilever(24, 12, 8, 8)
+    ctx = T.Context(*mesh, stream="own", step_graph=1, **KW)
+    ctx.opt_init()
+    ctx.opt_step()                      # direct: allocates, tunes
+    assert ctx.info().step_graph == 0
+    l0 = T.kernel_launches()
+    it, fx, gx, ch = ctx.opt_step()     # captured, then replayed
+    l1 = T.kernel_launches()
+    inf = ctx.info()
+    assert it == 2 and np.isfinite(fx) and ch > 0
+    assert inf.fem_its > 0 and inf.fem_status == 0 and 0 < inf.fem_relres < 1e-5
+    assert inf.filter_its[0] > 0 and inf.filter_its[1] > 0 and inf.mma_inner_its > 0
+    assert inf.step_graph == 1
+    assert l1 - l0 > 100                # the replay counts the kernels it ran
+    ctx.close()
+
+
+def test_graph_step_iteration_cap_and_nan(T, cuda):
+    mesh = T.gen_cantilever(16, 8, 6, 8)
+    ctx = T.Context(*mesh, stream="own", step_graph=1, **KW)
+    ctx.opt_init()
+    ctx.opt_step()
+    ctx.set_params(fem_maxit=3)         # a new graph with the new cap
+    rc = T.lib().topo_opt_step(ctx.h, None, None, None, None)
+    assert rc == T.TOPO_NOT_CONVERGED and ctx.info().fem_its == 3 and ctx.info().fem_status == 1
+    assert ctx.info().step_graph == 1
+    ctx.set_params(fem_maxit=10000)
+    # a non-finite density inside the device-resident design is reported
+    xp = T.device_view(ctx.opt_vector(1), ctx.ne)
+    xp[5] = float("nan")
+    with pytest.raises(T.TopoError) as ei:
+        ctx.opt_step()
+    assert ei.value.code == T.TOPO_ERR_NAN
+    ctx.opt_init()                      # a fresh run works again
+    h = ctx.opt_run(4)
+    assert np.all(np.isfinite(h)) and h.shape == (4, 3)
+    ctx.close()
+
+
+def test_batch_of_instances_equals_solo_runs(T, cuda):
+    """Four independent design instances (hex8 and tet4, different sizes,
+    volume fractions and filter radii, FP64 and mixed) advanced together by
+    topo_opt_step_batch for 10 iterations: each trajectory equals the
+    instance's solo host-driven run."""
+    specs = [((24, 12, 8, 8), dict(volfrac=0.12, rmin=1.5, precision=1)),
+             ((16, 8, 8, 4), dict(volfrac=0.2, rmin=1.3, precision=1)),
+             ((30, 15, 10, 8), dict(volfrac=0.25, rmin=1.8, precision=0)),
+             ((12, 6, 4, 8), dict(volfrac=0.15, rmin=2.0, precision=1))]
+    n = 10
+    solo = []
+    for dims, kw in specs:
+        h, _, _ = run(T, T.gen_cantilever(*dims), n, step_graph=0, **kw)
+        solo.append(h[:, 0])
+    ctxs = []
+    for dims, kw in specs:
+        c = T.Context(*T.gen_cantilever(*dims), stream="own", step_graph=1, **dict(KW, **kw))
+        c.opt_init()
+        ctxs.append(c)
+    hist = np.zeros((n, len(ctxs)))
+    for it in range(n):
+        st, fx = T.opt_step_batch(ctxs)
+        assert np.all(st == 0), st
+        hist[it] = fx
+    for k in range(len(ctxs)):
+        assert rel(hist[:, k], solo[k]) < 1e-6, k
+        assert ctxs[k].info().fem_its > 0 and ctxs[k].info().step_graph == 1
+    for c in ctxs:
+        c.close()

@@ -51,7 +51,8 @@ class Params(C.Structure):
         ("autotune", C.c_int),
         ("amg_coarse_cta", C.c_int),
         ("amg_half_fine", C.c_int),
-        ("pdl", C.c_int)]
+        ("pdl", C.c_int),
+        ("step_graph", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -60,7 +61,7 @@ class SolveInfo(C.Structure):
                 ("mma_inner_its", C.c_int), ("last_fx", C.c_double), ("last_gx0", C.c_double),
                 ("last_ch", C.c_double), ("t_fem_ms", C.c_double), ("t_filter_ms", C.c_double),
                 ("t_mma_ms", C.c_double), ("t_setup_ms", C.c_double), ("tuned", C.c_int * 4),
-                ("tuned_lanes", C.c_int * 8)]
+                ("tuned_lanes", C.c_int * 8), ("step_graph", C.c_int)]
 
 
 class TopoError(RuntimeError):
@@ -115,6 +116,7 @@ _SIGS = {
     "topo_opt_step": ([C.c_void_p, C.POINTER(C.c_int), _dp, _dp, _dp], C.c_int),
     "topo_opt_run": ([C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)], C.c_int),
     "topo_opt_step_host": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _dp], C.c_int),
+    "topo_opt_step_batch": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
     "topo_fem_sensitivities_noalloc": ([C.c_int, C.c_int] + [C.c_void_p] * 5 + [C.c_double] * 5 +
                                        [C.c_void_p] * 4, C.c_int),
     "topo_estimate_job_bytes": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_size_t),
@@ -285,6 +287,8 @@ class Context:
             # passed as cudaStreamLegacy (1) so that the library's work stays
             # ordered with torch's instead of getting a stream of its own
             stream = torch.cuda.current_stream().cuda_stream or 1
+        elif stream == "own":
+            stream = 0  # the library creates a stream for this context
         self.stream = stream
         h = C.c_void_p()
         _check(lib().topo_create(C.byref(self.params), nen, self.nn, _ptr(vertex), self.ne, _ptr(element.reshape(-1)),
@@ -520,6 +524,18 @@ class Context:
 
     def write_vtu(self, directory, itr, xphys=None):
         _check(lib().topo_write_vtu(self.h, directory.encode(), itr, _dptr(xphys)), "write_vtu")
+
+
+def opt_step_batch(contexts):
+    """One design iteration of every context at once (topo_opt_step_batch):
+    returns (statuses, compliances).  Errors are reported per instance in the
+    statuses, not raised."""
+    n = len(contexts)
+    arr = (C.c_void_p * max(n, 1))(*[c.h for c in contexts])
+    st = np.zeros(max(n, 1), dtype=np.int32)
+    fx = np.zeros(max(n, 1))
+    lib().topo_opt_step_batch(arr, n, _ptr(st), _ptr(fx))
+    return st[:n], fx[:n]
 
 
 def device_view(ptr, n):

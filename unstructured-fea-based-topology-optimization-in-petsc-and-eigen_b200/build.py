@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
          "--expt-relaxed-constexpr", "-I", INCLUDE]
 
-SOURCES = ["setup.cpp", "serve.cpp", "kernels_elem.cu", "amg.cu", "solver.cu", "mma.cu", "abi.cu", "noalloc.cu", "block.cu", "block_solve.cu"]
+SOURCES = ["setup.cpp", "serve.cpp", "kernels_elem.cu", "amg.cu", "solver.cu", "mma.cu", "abi.cu", "noalloc.cu", "block.cu", "block_solve.cu", "stepgraph.cu"]
 HEADERS = ["common.cuh", "ctx.h"]
 
 

@@ -35,24 +35,37 @@ __global__ void k_filter_diag(int nn, int nen, int nkf, const int* __restrict__ 
     }
     dinv[i] = s != 0.0 ? 1.0 / s : 1.0;
 }
-// HeavisideFilter (PDEFilter.cpp:271-279)
+// HeavisideFilter (PDEFilter.cpp:271-279); beta from the argument, or from
+// device memory (beta_dev) in the device-driven step
 __global__ void k_heaviside(int n, const double* __restrict__ xf, double* __restrict__ xp, double beta, double x0,
-                            double Xmin) {
+                            double Xmin, const double* __restrict__ beta_dev) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (beta_dev) beta = *beta_dev;
     double v = (tanh(beta * x0) + tanh(beta * (xf[i] - x0))) / (tanh(beta * x0) + tanh(beta * (1 - x0)));
     if (v < Xmin) v = Xmin;
     xp[i] = v;
 }
 // ComputeProjectedSens (PDEFilter.cpp:309-333)
 __global__ void k_projsens(int n, int m, const double* __restrict__ xf, double* __restrict__ df, double* __restrict__ dg,
-                           double beta, double x0) {
+                           double beta, double x0, const double* __restrict__ beta_dev) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (beta_dev) beta = *beta_dev;
     double t = tanh(beta * (xf[i] - x0));
     double dx = beta * (1.0 - pow(t, 2.0)) / (tanh(beta * x0) + tanh(beta * (1 - x0)));
     df[i] = df[i] * dx;
     for (int j = 0; j < m; j++) dg[(long)j * n + i] = dg[(long)j * n + i] * dx;
+}
+
+// HeavisideFilter's beta schedule (PDEFilter.cpp:260-268) on the device
+__global__ void k_beta_schedule(const int* __restrict__ itr, double beta0, double betamax, double* __restrict__ beta,
+                                double* __restrict__ beta_tmp) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int it = *itr;
+    if (it < 30) *beta = beta0;
+    else if (it % 10 == 0) *beta = fmin(betamax, *beta_tmp + 1);
+    *beta_tmp = *beta;
 }
 
 // ----------------------------------------------------------------- internal stages
@@ -67,7 +80,7 @@ static int sum_device(Ctx& c, const double* v, long n, double* host_out) {
 int filter_apply(Ctx& c, const double* x, double* xf, double Xmin) {
     TRET(filter_tf(c, x, c.TX.p));
     int its = 0;
-    int rc = filter_cg(c, c.TX.p, c.RX.p, &its);
+    int rc = filter_cg(c, c.TX.p, c.RX.p, &its, 0);
     c.info.filter_its[0] = its;
     TRET(rc);
     TRET(filter_tfxT(c, c.RX.p, xf, true, Xmin));
@@ -77,7 +90,7 @@ int filter_apply(Ctx& c, const double* x, double* xf, double Xmin) {
 int filter_sens(Ctx& c, double* df, double* dg, int m) {
     int rc = 0, its = 0;
     TRET(filter_tf(c, df, c.TX.p));
-    int r = filter_cg(c, c.TX.p, c.RX.p, &its);
+    int r = filter_cg(c, c.TX.p, c.RX.p, &its, 1);
     TRET(r);
     rc = std::max(rc, r);
     c.info.filter_its[1] = its;
@@ -85,7 +98,7 @@ int filter_sens(Ctx& c, double* df, double* dg, int m) {
     for (int j = 0; j < m; j++) {
         double* dj = dg + (size_t)j * c.ne;
         TRET(filter_tf(c, dj, c.TX.p));
-        r = filter_cg(c, c.TX.p, c.RX.p, &its);
+        r = filter_cg(c, c.TX.p, c.RX.p, &its, std::min(j + 2, 3));
         TRET(r);
         rc = std::max(rc, r);
         if (j + 2 < 4) c.info.filter_its[j + 2] = its;
@@ -100,16 +113,25 @@ int heaviside(Ctx& c, const double* xf, double* xp, double x0, double beta0, dou
         TCK(cudaMemcpyAsync(xp, xf, sizeof(double) * c.ne, cudaMemcpyDeviceToDevice, c.s));
         return 0;
     }
+    if (c.sg.dd) {
+        // the same beta schedule on the device, from the device's itr
+        k_beta_schedule<<<1, 32, 0, c.s>>>(c.di.p + DI_ITR, beta0, betamax, c.dsc.p + DS_BETA, c.dsc.p + DS_BETA_TMP),
+            note_launch();
+        k_heaviside<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, xf, xp, 0.0, x0, Xmin, c.dsc.p + DS_BETA), note_launch();
+        TCK(cudaGetLastError());
+        return 0;
+    }
     if (itr < 30) c.beta_proj = beta0;
     else if (itr % 10 == 0) c.beta_proj = std::min(betamax, c.beta_tmp + 1);
-    k_heaviside<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, xf, xp, c.beta_proj, x0, Xmin), note_launch();
+    k_heaviside<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, xf, xp, c.beta_proj, x0, Xmin, nullptr), note_launch();
     c.beta_tmp = c.beta_proj;
     TCK(cudaGetLastError());
     return 0;
 }
 
 int projected_sens(Ctx& c, const double* xf, double* df, double* dg, int m, double x0) {
-    k_projsens<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, m, xf, df, dg, c.beta_proj, x0), note_launch();
+    k_projsens<<<(c.ne + 255) / 256, 256, 0, c.s>>>(c.ne, m, xf, df, dg, c.beta_proj, x0,
+                                                    c.sg.dd ? c.dsc.p + DS_BETA : nullptr), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -140,6 +162,17 @@ static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 // one pass of main.cpp:72-112
 int opt_step(Ctx& c) {
     const topo_params& p = c.p;
+    if (p.step_graph) {
+        bool ok = false;
+        TRET(opt_step_graph_prepare(c, &ok));
+        if (ok) {
+            for (int part = 0; part < 3; part++) TRET(opt_step_graph_part(c, part));
+            return opt_step_graph_finish(c);
+        }
+    } else {
+        c.info.step_graph = 0;
+    }
+    c.sg.state_dirty = true;  // the host-side itr and beta move on
     c.itr++;
     cudaEventRecord(c.ev[0], c.s);
     int rc_fem = fem_obj_sens_dev(c, c.XP.p, c.dfdx.p, c.dgdx.p);
@@ -181,7 +214,7 @@ int opt_init(Ctx& c) {
     c.ch = 1.0;
     // a fresh optimisation: MMA history, filter warm start and beta state
     // start over as in a new process (MMA.cpp:178-224, PDEFilter.cpp:64-67)
-    c.mma_k = 0;
+    TCK(cudaMemsetAsync(c.di.p + DI_MMA_K, 0, sizeof(int), c.s));
     c.u_valid = false;
     for (DBuf<double>* b : {&c.xo1, &c.xo2, &c.L, &c.Uas, &c.RX}) TRET(b->zero(c.s));
     c.beta_proj = c.beta_tmp = c.p.beta0;
@@ -201,6 +234,8 @@ int create(Ctx& c, int nen, int n_nodes, const double* vertex, int n_elems, cons
     for (int i = 0; i < 4; i++) TCK(cudaEventCreate(&c.ev[i]));
     TRET(c.dsc.alloc(DS_COUNT));
     TRET(c.dsc.zero(c.s));
+    TRET(c.di.alloc(DI_COUNT));
+    TRET(c.di.zero(c.s));
     TRET(c.hsc.alloc(1024));
     TRET(build_mesh(c, vertex, element, n_fixed, fixed, n_cases, case_ptr, load_dofs, load_vals));
     TRET(elem_setup(c));
@@ -292,6 +327,7 @@ void topo_params_default(topo_params* p) {
     p->amg_coarse_cta = 0;
     p->autotune = 1;
     p->pdl = 1;
+    p->step_graph = 0;
 }
 
 int topo_device_alloc(size_t bytes, void** ptr) {
@@ -351,7 +387,7 @@ static int check_params(const topo_params* p) {
         {p->proj, "proj"}, {p->amg_smooth_p, "amg_smooth_p"}, {p->fine_smoother_matfree, "fine_smoother_matfree"},
         {p->fem_warm_start, "fem_warm_start"}, {p->fem_block, "fem_block"}, {p->fem_graphs, "fem_graphs"},
         {p->autotune, "autotune"}, {p->amg_coarse_cta, "amg_coarse_cta"}, {p->amg_half_fine, "amg_half_fine"},
-        {p->pdl, "pdl"}};
+        {p->pdl, "pdl"}, {p->step_graph, "step_graph"}};
     for (const auto& f : flags)
         if (f.v != 0 && f.v != 1) { set_error("%s must be 0 or 1", f.name); return TOPO_ERR_ARG; }
     return 0;
@@ -668,11 +704,11 @@ int topo_mma_restart(topo_ctx* ctx, double* xo1_d, double* xo2_d, double* U_d, d
     if (set) {
         TCK(cudaMemcpyAsync(c.xo1.p, xo1_d, b, kind, c.s)); TCK(cudaMemcpyAsync(c.xo2.p, xo2_d, b, kind, c.s));
         TCK(cudaMemcpyAsync(c.Uas.p, U_d, b, kind, c.s)); TCK(cudaMemcpyAsync(c.L.p, L_d, b, kind, c.s));
-        if (k) c.mma_k = *k;
+        if (k) TCK(cudaMemcpyAsync(c.di.p + DI_MMA_K, k, sizeof(int), cudaMemcpyHostToDevice, c.s));
     } else {
         TCK(cudaMemcpyAsync(xo1_d, c.xo1.p, b, kind, c.s)); TCK(cudaMemcpyAsync(xo2_d, c.xo2.p, b, kind, c.s));
         TCK(cudaMemcpyAsync(U_d, c.Uas.p, b, kind, c.s)); TCK(cudaMemcpyAsync(L_d, c.L.p, b, kind, c.s));
-        if (k) *k = c.mma_k;
+        if (k) TCK(cudaMemcpyAsync(k, c.di.p + DI_MMA_K, sizeof(int), cudaMemcpyDeviceToHost, c.s));
     }
     TCK(cudaStreamSynchronize(c.s));
     return 0;
@@ -743,6 +779,50 @@ int topo_opt_run(topo_ctx* ctx, int max_itr, double* hist, int* iterations) {
     return worst;
     GUARD_END
 }
+int topo_opt_step_batch(topo_ctx* const* ctxs, int n, int* status, double* fx) {
+    if (!ctxs || n < 0) { set_error("bad argument"); return TOPO_ERR_ARG; }
+    for (int i = 0; i < n; i++)
+        if (!ctxs[i]) { set_error("null context %d", i); return TOPO_ERR_ARG; }
+    GUARD_BEGIN
+    std::vector<int> rc(n, 0);
+    std::vector<char> replay(n, 0);
+    for (int i = 0; i < n; i++) {
+        Ctx& c = ctxs[i]->c;
+        if (!c.opt_ready) rc[i] = opt_init(c);
+        bool ok = false;
+        if (rc[i] >= 0 && c.p.step_graph) rc[i] = opt_step_graph_prepare(c, &ok);
+        replay[i] = rc[i] >= 0 && ok;
+    }
+    // every replayed instance's three parts, with the cooperative dual solves
+    // (part 1) one after another across the instances
+    for (int part = 0; part < 3; part++) {
+        Ctx* prev = nullptr;
+        for (int i = 0; i < n; i++) {
+            if (!replay[i] || rc[i] < 0) continue;
+            Ctx& c = ctxs[i]->c;
+            if (part == 1 && prev) {
+                cudaError_t e = cudaStreamWaitEvent(c.s, prev->sg.mma_done, 0);
+                if (e != cudaSuccess) { rc[i] = cuda_fail(e, __FILE__, __LINE__); continue; }
+            }
+            rc[i] = opt_step_graph_part(c, part);
+            if (part == 1) prev = &c;
+        }
+    }
+    for (int i = 0; i < n; i++)
+        if (!replay[i] && rc[i] >= 0) rc[i] = opt_step(ctxs[i]->c);
+    for (int i = 0; i < n; i++)
+        if (replay[i] && rc[i] >= 0) rc[i] = opt_step_graph_finish(ctxs[i]->c);
+    int worst = 0, err = 0;
+    for (int i = 0; i < n; i++) {
+        if (status) status[i] = rc[i];
+        if (fx) fx[i] = ctxs[i]->c.info.last_fx;
+        if (rc[i] < 0 && !err) err = rc[i];
+        worst = std::max(worst, rc[i]);
+    }
+    return err ? err : worst;
+    GUARD_END
+}
+
 int topo_opt_step_host(topo_ctx* ctx, const double* x_in, double* x_out, double* xphys_out, double* fx) {
     if (!ctx || !x_in || !x_out || !xphys_out) { set_error("null argument"); return TOPO_ERR_ARG; }
     GUARD_BEGIN

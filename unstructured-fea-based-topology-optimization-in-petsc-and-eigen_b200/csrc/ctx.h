@@ -228,10 +228,10 @@ struct Ctx {
     StepGraphs graphs;          // captured Arnoldi steps of the single-load FGMRES
     DBuf<double> red;           // reduction partials
     DBuf<double> dsc;           // device scalars
+    DBuf<int> di;               // device integers (DiSlot)
     PinnedScalars hsc;          // pinned host mirror for readbacks
 
-    // ---- MMA (MMA.cpp state)
-    int mma_k = 0;
+    // ---- MMA (MMA.cpp state; the outer iteration k lives in di[DI_MMA_K])
     // bounds of the device-side waits (grid barrier spins, bulk-copy wait
     // cycles) and the test form that makes them run out (topo_test_wait_limits)
     struct WaitLimits {
@@ -255,6 +255,43 @@ struct Ctx {
     bool u_valid = false;       // U holds a solution of this optimisation run
 
     BlockState blk;
+
+    // Device-driven design iteration (stepgraph.cu): the main.cpp loop body
+    // captured as CUDA graphs, with the FGMRES and filter-CG loops run as
+    // conditional graph nodes whose conditions are set on the device.
+    struct StepGraph {
+        bool dd = false;                 // capturing: stages take their device-driven form
+        cudaStream_t cap = nullptr;      // top-level capture stream
+        cudaStream_t body[4] = {};       // capture streams of nested conditional bodies
+        int depth = 0;
+        // three graphs: [0] solve, sensitivities, filtered sensitivities, move
+        // limits; [1] the MMA update (its cooperative dual solve) and the design
+        // change; [2] filter, projection, results.  A batch of instances
+        // orders the instances' part-1 graphs one after another (the dual
+        // solve's grid barrier wants its blocks resident together).
+        cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+        long launches[3] = {0, 0, 0};    // kernels per replay (for the launch counter)
+        cudaEvent_t mma_done = nullptr;  // recorded after part 1 (batch ordering)
+        uint64_t sig = 0;                // options and buffers the graphs were captured with
+        bool disabled = false;           // capture failed: direct launches from then on
+        bool state_dirty = true;         // host itr/beta changed since the device copies
+        DBuf<double> out;                // collected per-step results (read once per step)
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        void drop() {
+            for (auto& e : exec) {
+                if (e) cudaGraphExecDestroy(e);
+                e = nullptr;
+            }
+        }
+        ~StepGraph() {
+            drop();
+            if (cap) cudaStreamDestroy(cap);
+            for (auto b : body)
+                if (b) cudaStreamDestroy(b);
+            for (auto e : {e0, e1, mma_done})
+                if (e) cudaEventDestroy(e);
+        }
+    } sg;
 
     // launch shapes (autotuned at the first solve, see autotune.cu)
     struct Tune {
@@ -348,9 +385,21 @@ int autotune_single(Ctx& c);                                       // autotune.c
 int autotune_block(Ctx& c);
 int fem_solve(Ctx& c, const double* xphys, double* u);             // solver.cu
 int fem_solve_block(Ctx& c, const double* xphys, double* u);       // block_solve.cu
-int filter_cg(Ctx& c, const double* b, double* x, int* its);
+int filter_cg(Ctx& c, const double* b, double* x, int* its, int slot = 0);
 int dev_dot(Ctx& c, const double* a, const double* b, long n, double* out_dev);
 int finalize_sum(Ctx& c, const double* partials, int nparts, int nv, double* out_dev);
+
+// conditional graph nodes (stepgraph.cu): the body is captured on a private
+// stream (c.s is switched to it) until cond_end
+int cond_begin(Ctx& c, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type);
+int cond_end(Ctx& c);
+int cond_handle(Ctx& c, cudaGraphConditionalHandle* h);  // handle on the graph being captured on c.s
+// the device-driven step (stepgraph.cu): prepare (capture when needed) and
+// say whether this step can be replayed; launch part p (0..2) on c.s; wait
+// for the step and read its results
+int opt_step_graph_prepare(Ctx& c, bool* ok);
+int opt_step_graph_part(Ctx& c, int part);
+int opt_step_graph_finish(Ctx& c);
 
 int mma_alloc(Ctx& c);                                             // mma.cu
 int mma_movelimit(Ctx& c, double Xmin, double Xmax, double movlim, const double* x, double* xmin, double* xmax);
@@ -367,7 +416,29 @@ enum DscSlot {
     DS_CG = 16,                    // CG scratch (16..31)
     DS_GM = 32,                    // FGMRES column (32..170)
     DS_KKT = 176,
+    DS_TTOL = 180,                 // device-driven step: FGMRES stopping threshold
+    DS_CGTOL = 181,                //   filter CG stopping threshold
+    DS_RELRES = 182,               //   true relative residual of the last solve
+    DS_BETA = 183, DS_BETA_TMP = 184,  // Heaviside beta state (PDEFilter.cpp:260-268)
     DS_COUNT = 200
+};
+
+// MMA scalars in Ctx::mma_scal: lam[4] mu[4] y[4] z b[4] its err
+constexpr int kMmaSlots = 32;
+enum { MS_LAM = 0, MS_MU = 4, MS_Y = 8, MS_Z = 12, MS_B = 13, MS_ITS = 17, MS_ERR = 18 };
+
+// device integer slots in Ctx::di (the device-driven step's loop state, and
+// the counters that live on the device in every form)
+enum DiSlot {
+    DI_ITS = 0, DI_KDONE = 1, DI_CONV = 2, DI_STOP = 3, DI_JMAX = 4,  // FGMRES
+    DI_NAN = 5,                    // a solve met a non-finite residual
+    DI_STATUS = 6,                 // FGMRES: 0 converged, 1 iteration cap
+    DI_CG_ITS = 8,                 // filter CG iterations of solves 0..3
+    DI_CG_STATUS = 12,             // filter CG status of solves 0..3
+    DI_ITR = 16,                   // design iteration counter (main.cpp:72)
+    DI_MMA_K = 17,                 // MMA outer iteration k (MMA.cpp:508)
+    DI_CG_CUR = 18,                // iterations of the running filter CG
+    DI_COUNT = 32
 };
 
 }  // namespace topo

@@ -23,8 +23,6 @@ static std::mutex& coop_mutex() {
     return m;
 }
 
-constexpr int kMmaSlots = 32;  // mma_scal layout: lam[4] mu[4] y[4] z b[4] its err
-enum { MS_LAM = 0, MS_MU = 4, MS_Y = 8, MS_Z = 12, MS_B = 13, MS_ITS = 17, MS_ERR = 18 };
 
 struct MmaConst {
     double a[kMaxM], c[kMaxM], d[kMaxM];
@@ -45,7 +43,7 @@ __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : 
 
 // GenSub (MMA.cpp:506-620): asymptotes, bounds, p0/q0/pij/qij, b partials
 template <int M>
-__global__ void k_gensub(int n, int k, double asyminit, double asymdec, double asyminc, int robust, int conmod,
+__global__ void k_gensub(int n, const int* __restrict__ kdev, double asyminit, double asymdec, double asyminc, int robust, int conmod,
                          const double* __restrict__ xv, const double* __restrict__ x1v, const double* __restrict__ x2v,
                          const double* __restrict__ xminv, const double* __restrict__ xmaxv,
                          const double* __restrict__ dfdx, const double* __restrict__ dgdx, double* __restrict__ Lv,
@@ -53,6 +51,7 @@ __global__ void k_gensub(int n, int k, double asyminit, double asymdec, double a
                          double* __restrict__ p0, double* __restrict__ q0, double* __restrict__ pij,
                          double* __restrict__ qij, double* __restrict__ part) {
     __shared__ double sm[M * 32];
+    const int k = *kdev;  // MMA outer iteration, advanced by k_mma_next before this launch
     double bsum[M];
 #pragma unroll
     for (int j = 0; j < M; j++) bsum[j] = 0.0;
@@ -422,6 +421,11 @@ __global__ void k_kkt_final(int nb, const double* __restrict__ part, double* __r
     if (threadIdx.x == 0) { out[0] = v[0]; out[1] = mx; }
 }
 
+// k++ of MMA::GenSub (MMA.cpp:508), on the device so that a replayed graph advances it
+__global__ void k_mma_next(int* __restrict__ k) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *k += 1;
+}
+
 // ---------------------------------------------------------------- host side
 constexpr int kMmaBlocks = 296;
 
@@ -457,8 +461,9 @@ static int update_m(Ctx& c, double* x, const double* dfdx, const double* gx_dev,
     const int n = c.ne;
     double* ms = c.mma_scal.p;
     double* part = ms + kMmaSlots;
-    c.mma_k++;
-    k_gensub<M><<<kMmaBlocks, 256, 0, c.s>>>(n, c.mma_k, c.asyminit, c.asymdec, c.asyminc, c.robust_type,
+    int* kdev = c.di.p + DI_MMA_K;
+    k_mma_next<<<1, 32, 0, c.s>>>(kdev), note_launch();
+    k_gensub<M><<<kMmaBlocks, 256, 0, c.s>>>(n, kdev, c.asyminit, c.asymdec, c.asyminc, c.robust_type,
                                             c.constraint_mod, x, c.xo1.p, c.xo2.p, xmin, xmax, dfdx, dgdx, c.L.p,
                                             c.Uas.p, c.alpha.p, c.beta.p, c.p0.p, c.q0.p, c.pij.p, c.qij.p, part), note_launch();
     k_gensub_final<<<1, 256, 0, c.s>>>(kMmaBlocks, M, part, gx_dev, ms), note_launch();
@@ -472,7 +477,14 @@ static int update_m(Ctx& c, double* x, const double* dfdx, const double* gx_dev,
     TCK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, dev));
     int occ = 0;
     TCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solvedip<M>, 256, 0));
-    int blocks = std::max(1, std::min(dev_sms * std::max(occ, 1), std::min(2048, (n + 255) / 256)));
+    // Co-residency: the grid barrier needs every block of the grid resident at
+    // once.  A direct launch (one at a time per process, under coop_mutex)
+    // leaves one block slot per SM free, and a launch from a replayed step
+    // graph (stepgraph.cu; one at a time per batch) takes at most one block
+    // per SM, so one of each can run side by side without either waiting on
+    // blocks that cannot start.
+    const int cap = c.sg.dd ? dev_sms : dev_sms * std::max(occ - 1, 1);
+    int blocks = std::max(1, std::min(cap, std::min(2048, (n + 255) / 256)));
     MmaConst kc{};
     for (int j = 0; j < M; j++) { kc.a[j] = c.a[j]; kc.c[j] = c.c[j]; kc.d[j] = c.d[j]; }
     double tol = 1.0e-9 * std::sqrt((double)(M + n));
@@ -485,6 +497,22 @@ static int update_m(Ctx& c, double* x, const double* dfdx, const double* gx_dev,
     const double* Lp = c.L.p; const double* Up = c.Uas.p; const double* al = c.alpha.p; const double* be = c.beta.p;
     int nn = n;
     void* args[] = {&nn, &x, &p0, &q0, &pij, &qij, &Lp, &Up, &al, &be, &ms, &kc, &tol, &part1, &part2, &gb};
+    if (c.sg.dd) {
+        // device-driven step: a cooperative kernel node in the step graph; the
+        // iteration count and the barrier flag are read once the step is done
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(blocks);
+        cfg.blockDim = dim3(256);
+        cfg.stream = c.s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        TCK(cudaLaunchKernelExC(&cfg, (const void*)k_solvedip<M>, args));
+        note_launch();
+        return 0;
+    }
     int* herr = reinterpret_cast<int*>(c.hsc.h + 201);
     *herr = 0;
     {

@@ -124,11 +124,12 @@ __global__ void k_scale_to(long n, const double* __restrict__ w, const double* _
     const double f = invert ? 1.0 / (*s) : (*s);
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) v[i] = w[i] * f;
 }
-// x += sum_k y_k Z_k
+// x += sum_k y_k Z_k (kd from the argument, or from device memory)
 template <class TZ>
-__global__ void k_update(long n, int kd, const TZ* __restrict__ Z, long ld, const double* __restrict__ y,
-                         double* __restrict__ x) {
+__global__ void k_update(long n, int kd, const int* __restrict__ kd_dev, const TZ* __restrict__ Z, long ld,
+                         const double* __restrict__ y, double* __restrict__ x) {
     __shared__ double ys[128];
+    if (kd_dev) kd = *kd_dev;
     if (threadIdx.x < kd) ys[threadIdx.x] = y[threadIdx.x];
     __syncthreads();
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -394,9 +395,11 @@ __global__ void k_gm_givens(GmLayout L, int j, const double* __restrict__ hcol, 
     out[0] = fabs(-s * gj);
     out[1] = hcol[j + 1];
 }
-// y = R^-1 g for the kd completed columns
-__global__ void k_gm_solve(GmLayout L, int kd, double* __restrict__ st) {
+// y = R^-1 g for the kd completed columns (kd from the argument, or from
+// device memory)
+__global__ void k_gm_solve(GmLayout L, int kd, const int* __restrict__ kd_dev, double* __restrict__ st) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (kd_dev) kd = *kd_dev;
     for (int i = kd - 1; i >= 0; i--) {
         double s = st[L.g(i)];
         for (int k = i + 1; k < kd; k++) s -= st[L.H(i, k)] * st[L.y(k)];
@@ -410,7 +413,7 @@ struct StepArgs {
     int j;
     long n;
     GmLayout GL;
-    double *gm, *st, *out, *hs;
+    double *gm, *st, *out, *hs;  // hs: pinned host mirror of out (null: no read-back)
 };
 static int arnoldi_step(Ctx& c, void* p) {
     const StepArgs& a = *static_cast<const StepArgs*>(p);
@@ -429,7 +432,143 @@ static int arnoldi_step(Ctx& c, void* p) {
     k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, a.gm + j + 1, c.V.p + (size_t)(j + 1) * ldv, 1),
         note_launch();
     k_gm_givens<<<1, 32, 0, c.s>>>(a.GL, j, a.gm, a.st, a.out + 2 * j), note_launch();
-    TCK(cudaMemcpyAsync(a.hs + 2 * j, a.out + 2 * j, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    if (a.hs) TCK(cudaMemcpyAsync(a.hs + 2 * j, a.out + 2 * j, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    TCK(cudaGetLastError());
+    return 0;
+}
+
+// ----------------------------------------------------------------- device-driven FGMRES
+// The same FGMRES as fgmres() below, for capture into the step graph
+// (stepgraph.cu): the restart cycles are a conditional WHILE node, each
+// Arnoldi step j of a cycle an IF node, and single-thread kernels take the
+// decisions the host takes in fgmres() (stopping test, restart, iteration
+// cap) and set the nodes' conditions.  Every loop is bounded by fem_maxit.
+// State in c.di (DiSlot), thresholds in c.dsc.
+struct StepHandles {
+    cudaGraphConditionalHandle h[128];
+    int m;
+};
+// ttol = max(rtol ||b||, 1e-50); the loop runs while maxit > 0
+__global__ void k_dd_init(const double* __restrict__ b2, double rtol, int maxit, int* __restrict__ di,
+                          double* __restrict__ ttol, cudaGraphConditionalHandle loop) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    *ttol = fmax(rtol * sqrt(*b2), 1e-50);
+    di[DI_ITS] = 0;
+    di[DI_CONV] = 0;
+    di[DI_STATUS] = 1;
+    cudaGraphSetConditional(loop, maxit > 0 ? 1u : 0u);
+}
+// cycle start: beta = ||b - K x|| already in *beta; converged if beta <= ttol
+__global__ void k_dd_cycle(int* __restrict__ di, const double* __restrict__ beta_p, const double* __restrict__ ttol,
+                           int maxit, int m, cudaGraphConditionalHandle cyc) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double beta = *beta_p;
+    unsigned go = 0;
+    if (!isfinite(beta)) di[DI_NAN] = 1;
+    else if (beta <= *ttol) di[DI_CONV] = 1;
+    else {
+        const int jmax = min(m, maxit - di[DI_ITS]);
+        di[DI_JMAX] = jmax;
+        di[DI_KDONE] = jmax;
+        di[DI_STOP] = 0;
+        go = jmax > 0;
+    }
+    cudaGraphSetConditional(cyc, go);
+}
+// first node of a cycle's body: step 0 runs, steps 1.. wait for their predecessor
+__global__ void k_dd_steps_reset(StepHandles H) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int j = 0; j < H.m; j++) cudaGraphSetConditional(H.h[j], j == 0 ? 1u : 0u);
+}
+// after Arnoldi step j: the check fgmres() does on the host
+__global__ void k_dd_step(int j, int* __restrict__ di, const double* __restrict__ out, const double* __restrict__ ttol,
+                          cudaGraphConditionalHandle next, int has_next) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double res = out[0], hn = out[1];
+    di[DI_ITS] += 1;
+    bool stop = false;
+    if (!isfinite(res)) {
+        di[DI_NAN] = 1;
+        di[DI_KDONE] = j + 1;
+        stop = true;
+    } else if (res <= *ttol || hn == 0.0) {
+        di[DI_CONV] = res <= *ttol;
+        di[DI_KDONE] = j + 1;
+        stop = true;
+    }
+    if (j + 1 >= di[DI_JMAX]) stop = true;  // the cycle's last step: kdone = jmax
+    di[DI_STOP] = stop;
+    if (has_next) cudaGraphSetConditional(next, stop ? 0u : 1u);
+}
+// end of a cycle: restart unless converged, broken down or at the cap
+__global__ void k_dd_cycle_end(int* __restrict__ di, int maxit, cudaGraphConditionalHandle loop) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const bool more = !di[DI_CONV] && !di[DI_NAN] && di[DI_ITS] < maxit;
+    di[DI_STATUS] = di[DI_CONV] ? 0 : 1;
+    cudaGraphSetConditional(loop, more ? 1u : 0u);
+}
+// ||F - K U|| / ||F|| from the two squared norms
+__global__ void k_relres(const double* __restrict__ sq, double* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    *out = sq[1] > 0 ? sqrt(sq[0] / sq[1]) : sqrt(sq[0]);
+}
+
+static int fgmres_dd(Ctx& c, const double* b, double* x) {
+    const long n = c.ndof;
+    const int m = std::max(1, std::min(c.p.fem_restart, 128));
+    const int maxit = c.p.fem_maxit;
+    const GmLayout GL{m};
+    const long ldv = (n + 31) & ~31L;
+    const bool mixed = c.p.precision == TOPO_PREC_MIXED;
+    if (!c.V.p || (long)c.V.n < (long)(m + 1) * ldv || (mixed ? !c.Z32.p : !c.Z64.p) || !c.tune.single_done) {
+        set_error("the device-driven step needs a direct solve of this form first");
+        return TOPO_ERR_ARG;
+    }
+    double* gm = c.dsc.p + DS_GM;
+    double* st = c.wtmp.p;
+    double* out = st + GL.size();
+    double* out_beta = out + 2 * m + 2;
+    double* ttol = c.dsc.p + DS_TTOL;
+    int* di = c.di.p;
+    TRET(dev_dot(c, b, b, n, gm));
+    cudaGraphConditionalHandle hloop, hcyc;
+    TRET(cond_handle(c, &hloop));
+    k_dd_init<<<1, 32, 0, c.s>>>(gm, c.p.fem_rtol, maxit, di, ttol, hloop), note_launch();
+    TRET(cond_begin(c, hloop, cudaGraphCondTypeWhile));
+    {
+        // v0 = (b - K x) / beta
+        TRET(kmatvec64r(c, x, c.w.p, b));
+        TRET(dev_dot(c, c.w.p, c.w.p, n, gm));
+        k_gm_start<<<1, 32, 0, c.s>>>(GL, st, gm, out_beta), note_launch();
+        TRET(cond_handle(c, &hcyc));
+        k_dd_cycle<<<1, 32, 0, c.s>>>(di, out_beta, ttol, maxit, m, hcyc), note_launch();
+        TRET(cond_begin(c, hcyc, cudaGraphCondTypeIf));
+        {
+            StepHandles H{};
+            H.m = m;
+            for (int j = 0; j < m; j++) TRET(cond_handle(c, &H.h[j]));
+            k_dd_steps_reset<<<1, 32, 0, c.s>>>(H), note_launch();
+            k_scale_to<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.w.p, out_beta, c.V.p, 1), note_launch();
+            for (int j = 0; j < m; j++) {
+                TRET(cond_begin(c, H.h[j], cudaGraphCondTypeIf));
+                StepArgs sa{j, n, GL, gm, st, out, nullptr};
+                TRET(arnoldi_step(c, &sa));
+                k_dd_step<<<1, 32, 0, c.s>>>(j, di, out + 2 * j, ttol, j + 1 < m ? H.h[j + 1] : H.h[j], j + 1 < m),
+                    note_launch();
+                TRET(cond_end(c));
+            }
+            k_gm_solve<<<1, 32, 0, c.s>>>(GL, 0, di + DI_KDONE, st), note_launch();
+            if (mixed)
+                k_update<float><<<grid_for(n, 256), 256, 0, c.s>>>(n, 0, di + DI_KDONE, c.Z32.p, n, st + GL.y(0), x),
+                    note_launch();
+            else
+                k_update<double><<<grid_for(n, 256), 256, 0, c.s>>>(n, 0, di + DI_KDONE, c.Z64.p, n, st + GL.y(0),
+                                                                    x), note_launch();
+        }
+        TRET(cond_end(c));
+        k_dd_cycle_end<<<1, 32, 0, c.s>>>(di, maxit, hloop), note_launch();
+    }
+    TRET(cond_end(c));
     TCK(cudaGetLastError());
     return 0;
 }
@@ -529,11 +668,13 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
                 stop = true;
             }
         }
-        k_gm_solve<<<1, 32, 0, c.s>>>(GL, kdone, st), note_launch();
+        k_gm_solve<<<1, 32, 0, c.s>>>(GL, kdone, nullptr, st), note_launch();
         if (c.p.precision == TOPO_PREC_MIXED)
-            k_update<float><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z32.p, n, st + GL.y(0), x), note_launch();
+            k_update<float><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, nullptr, c.Z32.p, n, st + GL.y(0), x),
+                note_launch();
         else
-            k_update<double><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, c.Z64.p, n, st + GL.y(0), x), note_launch();
+            k_update<double><<<grid_for(n, 256), 256, 0, c.s>>>(n, kdone, nullptr, c.Z64.p, n, st + GL.y(0), x),
+                note_launch();
         TCK(cudaGetLastError());
     }
     prof_end(c, PS_SOLVE, esolve);
@@ -560,6 +701,10 @@ int fem_solve(Ctx& c, const double* xphys, double* u) {
 // moduli, AMG numeric setup, U = 0, FGMRES, then the true relative residual
 static int fem_solve_impl(Ctx& c, const double* xphys, double* u) {
     if (c.ncases > 1 && c.p.fem_block) return fem_solve_block(c, xphys, u);
+    if (c.sg.dd && c.ncases != 1) {
+        set_error("the device-driven step supports one load case (or the block solver)");
+        return TOPO_ERR_UNSUPPORTED;
+    }
     c.blk.u_valid = c.blk.u_fresh = false;
     TRET(compute_moduli(c, xphys));
     TRET(amg_numeric(c));
@@ -574,7 +719,8 @@ static int fem_solve_impl(Ctx& c, const double* xphys, double* u) {
         if (!(c.p.fem_warm_start && c.u_valid && uk == c.U.p + (size_t)k * n))
             TCK(cudaMemsetAsync(uk, 0, sizeof(double) * n, c.s));
         int its = 0, st = 0;
-        TRET(fgmres(c, fk, uk, &its, &st));
+        if (c.sg.dd) TRET(fgmres_dd(c, fk, uk));
+        else TRET(fgmres(c, fk, uk, &its, &st));
         its_total += its;
         worst = std::max(worst, st);
         // true residual ||F - K U|| / ||F||
@@ -582,6 +728,11 @@ static int fem_solve_impl(Ctx& c, const double* xphys, double* u) {
         double* gm = c.dsc.p + DS_GM;
         TRET(dev_dot(c, c.w.p, c.w.p, n, gm));
         TRET(dev_dot(c, fk, fk, n, gm + 1));
+        if (c.sg.dd) {  // read with the step's other results
+            k_relres<<<1, 32, 0, c.s>>>(gm, c.dsc.p + DS_RELRES), note_launch();
+            TCK(cudaGetLastError());
+            continue;
+        }
         TCK(cudaMemcpyAsync(c.hsc.h, gm, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
         TCK(cudaStreamSynchronize(c.s));
         double rel = c.hsc.h[1] > 0 ? std::sqrt(c.hsc.h[0] / c.hsc.h[1]) : std::sqrt(c.hsc.h[0]);
@@ -589,6 +740,7 @@ static int fem_solve_impl(Ctx& c, const double* xphys, double* u) {
         if (c.p.verbose) printf("Norm of error %e, Iterations %d\n", rel, its);
     }
     c.u_valid = (u == c.U.p);
+    if (c.sg.dd) return 0;  // counts and status come from the device after the step
     c.info.fem_its = its_total;
     c.info.fem_relres = rel_worst;
     c.info.fem_status = worst;
@@ -612,9 +764,11 @@ __global__ void k_cg_start(long n, const double* __restrict__ b, const double* _
     block_sum<3>(v, sm);
     if (threadIdx.x == 0) for (int k = 0; k < 3; k++) part[3L * blockIdx.x + k] = v[k];
 }
-// p = z (first) or p = z + (beta/betaold) p
+// p = z (first) or p = z + (beta/betaold) p; first from the argument, or
+// (its_dev) when no iteration has been done yet
 __global__ void k_cg_p(long n, const double* __restrict__ z, double* __restrict__ p, const double* __restrict__ sc,
-                       int first) {
+                       int first, const int* __restrict__ its_dev) {
+    if (its_dev) first = *its_dev == 0;
     const double bb = first ? 0.0 : sc[2] / sc[3];
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         p[i] = first ? z[i] : z[i] + bb * p[i];
@@ -653,14 +807,78 @@ __global__ void k_cg_final(int nb, int nv, const double* __restrict__ part, doub
     }
 }
 
+// device-driven CG (for the step graph): the iterations are a conditional
+// WHILE node; these kernels take filter_cg()'s host decisions
+__global__ void k_cgdd_init(const double* __restrict__ sc, double rtol, double atol, int maxit, int* __restrict__ di,
+                            int slot, double* __restrict__ ttol, cudaGraphConditionalHandle loop) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double t = fmax(rtol * sc[0], atol), dp = sc[1];
+    *ttol = t;
+    di[DI_CG_CUR] = 0;
+    di[DI_CG_ITS + slot] = 0;
+    di[DI_CG_STATUS + slot] = 0;
+    unsigned go = 1;
+    if (!isfinite(dp)) { di[DI_NAN] = 1; go = 0; }
+    else if (dp <= t) go = 0;
+    else if (maxit <= 0) { di[DI_CG_STATUS + slot] = 1; go = 0; }
+    else if (sc[2] == 0.0) { di[DI_CG_ITS + slot] = 1; go = 0; }  // beta == 0 before the first step
+    cudaGraphSetConditional(loop, go);
+}
+__global__ void k_cgdd_after(const double* __restrict__ sc, const double* __restrict__ ttol, double dtol, int maxit,
+                             int* __restrict__ di, int slot, cudaGraphConditionalHandle loop) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int i = di[DI_CG_CUR] + 1;
+    di[DI_CG_CUR] = i;
+    di[DI_CG_ITS + slot] = i;
+    const double dp = sc[1];
+    unsigned go = 1;
+    if (!isfinite(dp)) { di[DI_NAN] = 1; go = 0; }
+    else if (dp <= *ttol) go = 0;
+    else if (dp >= dtol * sc[0]) { di[DI_CG_STATUS + slot] = 1; go = 0; }  // diverged
+    else if (i >= maxit) { di[DI_CG_STATUS + slot] = 1; go = 0; }
+    else if (sc[2] == 0.0) { di[DI_CG_ITS + slot] = i + 1; go = 0; }
+    cudaGraphSetConditional(loop, go);
+}
+
+static int filter_cg_dd(Ctx& c, const double* b, double* x, int slot) {
+    const long n = c.nn;
+    double* sc = c.dsc.p + DS_CG;
+    int* di = c.di.p;
+    double* ttol = c.dsc.p + DS_CGTOL;
+    TRET(filter_kf(c, x, c.fw.p));
+    k_cg_start<<<kRedBlocks, 256, 0, c.s>>>(n, b, c.fw.p, c.fdiag_inv.p, c.fr.p, c.fz.p, c.red.p), note_launch();
+    k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 3, c.red.p, sc, 1), note_launch();
+    cudaGraphConditionalHandle h;
+    TRET(cond_handle(c, &h));
+    k_cgdd_init<<<1, 32, 0, c.s>>>(sc, c.p.filter_rtol, c.p.filter_atol, c.p.filter_maxit, di, slot, ttol, h),
+        note_launch();
+    TRET(cond_begin(c, h, cudaGraphCondTypeWhile));
+    k_cg_p<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.fz.p, c.fp.p, sc, 0, di + DI_CG_CUR), note_launch();
+    TRET(filter_kf(c, c.fp.p, c.fw.p));
+    k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.red.p), note_launch();
+    k_final<<<1, 32, 0, c.s>>>(kRedBlocks, 1, c.red.p, sc + 4, -1), note_launch();
+    k_cg_step<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.fdiag_inv.p, x, c.fr.p, c.fz.p, sc, c.red.p),
+        note_launch();
+    k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 2, c.red.p, sc, 0), note_launch();
+    k_cgdd_after<<<1, 32, 0, c.s>>>(sc, ttol, c.p.filter_dtol, c.p.filter_maxit, di, slot, h), note_launch();
+    TRET(cond_end(c));
+    TCK(cudaGetLastError());
+    return 0;
+}
+
 // KSPCG + PCJACOBI with a nonzero initial guess x (PDEFilter.cpp:117-137):
 // preconditioned residual norm, converged when ||D^-1 r|| <= max(rtol
-// ||D^-1 b||, atol), diverged when it exceeds dtol ||D^-1 b||.
-int filter_cg(Ctx& c, const double* b, double* x, int* its_out) {
+// ||D^-1 b||, atol), diverged when it exceeds dtol ||D^-1 b||.  `slot`
+// (0..3) names the solve in the device-driven step's counters.
+int filter_cg(Ctx& c, const double* b, double* x, int* its_out, int slot) {
     const long n = c.nn;
     double* sc = c.dsc.p + DS_CG;
     double* hs = c.hsc.h + 96;
     if ((long)c.red.n < kRedBlocks * 40L) TRET(c.red.alloc(std::max<long>(kRedBlocks * 40L, 4096)));
+    if (c.sg.dd) {
+        *its_out = 0;
+        return filter_cg_dd(c, b, x, slot);
+    }
     TRET(filter_kf(c, x, c.fw.p));
     k_cg_start<<<kRedBlocks, 256, 0, c.s>>>(n, b, c.fw.p, c.fdiag_inv.p, c.fr.p, c.fz.p, c.red.p), note_launch();
     k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 3, c.red.p, sc, 1), note_launch();
@@ -676,7 +894,7 @@ int filter_cg(Ctx& c, const double* b, double* x, int* its_out) {
     do {
         *its_out = i + 1;
         if (hs[2] == 0.0) return 0;  // beta == 0
-        k_cg_p<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.fz.p, c.fp.p, sc, i == 0), note_launch();
+        k_cg_p<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.fz.p, c.fp.p, sc, i == 0, nullptr), note_launch();
         TRET(filter_kf(c, c.fp.p, c.fw.p));
         k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.red.p), note_launch();
         k_final<<<1, 32, 0, c.s>>>(kRedBlocks, 1, c.red.p, sc + 4, -1), note_launch();

@@ -1,0 +1,336 @@
+// stepgraph.cu -- the design iteration (main.cpp:72-112) replayed from CUDA graphs.
+//
+// A direct step (abi.cu opt_step) is driven by the host: it launches every
+// kernel, reads the FGMRES residual after each Arnoldi step, reads the filter
+// CG residual after each CG step and waits for the MMA dual solve.  Here the
+// step is captured once into graphs in which those loops are conditional
+// nodes (CUDA 12.4+): a WHILE node per solve, an IF node per Arnoldi step of
+// an FGMRES cycle, and single-thread kernels that take the host's decisions
+// on the device and set the nodes' conditions (cudaGraphSetConditional).
+// Every loop is bounded by its solver's iteration cap.  A replayed step is
+// three graph launches and one wait for its results; the same kernels run in
+// the same order as in a direct step, so the results agree with a direct
+// step to rounding.
+//
+// Several contexts (independent design instances) are advanced together by
+// topo_opt_step_batch (abi.cu): every instance's graphs are launched on its
+// own stream before the host waits for any of them.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "ctx.h"
+
+namespace topo {
+
+int fem_obj_sens_dev(Ctx& c, const double* xphys, double* dfdx, double* dgdx);
+int filter_sens(Ctx& c, double* df, double* dg, int m);
+int filter_apply(Ctx& c, const double* x, double* xf, double Xmin);
+int heaviside(Ctx& c, const double* xf, double* xp, double x0, double beta0, double betamax, int itr, double Xmin,
+              int proj);
+int projected_sens(Ctx& c, const double* xf, double* df, double* dg, int m, double x0);
+uint64_t sig_mix(uint64_t h, uint64_t v);
+const char* last_error();
+
+// ----------------------------------------------------------------- conditional nodes under stream capture
+static int capture_graph_of(cudaStream_t s, cudaGraph_t* g, const cudaGraphNode_t** deps, size_t* nd) {
+    cudaStreamCaptureStatus st;
+    TCK(cudaStreamGetCaptureInfo(s, &st, nullptr, g, deps, nd));
+    if (st != cudaStreamCaptureStatusActive) {
+        set_error("internal: conditional node outside a stream capture");
+        return TOPO_ERR_CUDA;
+    }
+    return 0;
+}
+
+int cond_handle(Ctx& c, cudaGraphConditionalHandle* h) {
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps;
+    size_t nd;
+    TRET(capture_graph_of(c.s, &g, &deps, &nd));
+    TCK(cudaGraphConditionalHandleCreate(h, g, 0, cudaGraphCondAssignDefault));
+    return 0;
+}
+
+// Adds a conditional node after the work captured so far on c.s, and starts
+// capturing its body on the private stream of the next nesting level (c.s
+// names that stream until cond_end).
+int cond_begin(Ctx& c, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type) {
+    if (c.sg.depth >= 4) {
+        set_error("internal: conditional nodes nested too deeply");
+        return TOPO_ERR_CUDA;
+    }
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps;
+    size_t nd;
+    TRET(capture_graph_of(c.s, &g, &deps, &nd));
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = h;
+    np.conditional.type = type;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    TCK(cudaGraphAddNode(&node, g, deps, nd, &np));
+    TCK(cudaStreamUpdateCaptureDependencies(c.s, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaStream_t bs = c.sg.body[c.sg.depth];
+    TCK(cudaStreamBeginCaptureToGraph(bs, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal));
+    c.sg.depth++;
+    c.s = bs;
+    return 0;
+}
+
+int cond_end(Ctx& c) {
+    if (c.sg.depth < 1) {
+        set_error("internal: cond_end without cond_begin");
+        return TOPO_ERR_CUDA;
+    }
+    cudaGraph_t g = nullptr;
+    TCK(cudaStreamEndCapture(c.s, &g));
+    c.sg.depth--;
+    c.s = c.sg.depth ? c.sg.body[c.sg.depth - 1] : c.sg.cap;
+    return 0;
+}
+
+// ----------------------------------------------------------------- step kernels
+__global__ void k_itr_next(int* __restrict__ di) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        di[DI_ITR] += 1;
+        di[DI_NAN] = 0;
+    }
+}
+
+// The step's results in one place (read with one copy per step):
+// [0] fx  [1..4] gx  [5] ch  [6] true relres  [7] beta  [8] beta_tmp
+// [9] MMA inner iterations  [10] barrier timeout flag  [11] FGMRES its
+// [12] FGMRES status  [13] NaN flag  [14..17] CG its  [18..21] CG status
+// [22] itr
+constexpr int kOut = 24;
+__global__ void k_collect(const double* __restrict__ dsc, const int* __restrict__ di, const double* __restrict__ ms_its,
+                          const int* __restrict__ bar_err, double* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    out[0] = dsc[DS_FX];
+    for (int j = 0; j < 4; j++) out[1 + j] = dsc[DS_GX + j];
+    out[5] = dsc[DS_CH];
+    out[6] = dsc[DS_RELRES];
+    out[7] = dsc[DS_BETA];
+    out[8] = dsc[DS_BETA_TMP];
+    out[9] = *ms_its;
+    out[10] = *bar_err;
+    out[11] = di[DI_ITS];
+    out[12] = di[DI_STATUS];
+    out[13] = di[DI_NAN];
+    for (int j = 0; j < 4; j++) {
+        out[14 + j] = di[DI_CG_ITS + j];
+        out[18 + j] = di[DI_CG_STATUS + j];
+    }
+    out[22] = di[DI_ITR];
+}
+
+// the loop body of main.cpp:72-112 with every stage in its device-driven
+// form, in three parts (Ctx::StepGraph)
+static int step_part(Ctx& c, int part) {
+    const topo_params& p = c.p;
+    if (part == 0) {
+        k_itr_next<<<1, 32, 0, c.s>>>(c.di.p), note_launch();
+        TRET(fem_obj_sens_dev(c, c.XP.p, c.dfdx.p, c.dgdx.p));
+        if (p.proj) TRET(projected_sens(c, c.XF.p, c.dfdx.p, c.dgdx.p, p.m, p.x0));
+        TRET(filter_sens(c, c.dfdx.p, c.dgdx.p, p.m));
+        TRET(mma_movelimit(c, p.Xmin, p.Xmax, p.movlim, c.X.p, c.xmin.p, c.xmax.p));
+    } else if (part == 1) {
+        TRET(mma_update(c, c.X.p, c.dfdx.p, c.dsc.p + DS_GX, c.dgdx.p, c.xmin.p, c.xmax.p));
+        TRET(mma_design_change(c, c.X.p, c.Xold.p, c.dsc.p + DS_CH));
+    } else {
+        TRET(filter_apply(c, c.X.p, c.XF.p, p.Xmin));
+        TRET(heaviside(c, c.XF.p, c.XP.p, p.x0, p.beta0, p.betamax, 0, p.Xmin, p.proj));
+        k_collect<<<1, 32, 0, c.s>>>(c.dsc.p, c.di.p, c.mma_scal.p + MS_ITS, c.bar_err.p, c.sg.out.p),
+            note_launch();
+        TCK(cudaMemcpyAsync(c.hsc.h + 600, c.sg.out.p, kOut * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    }
+    TCK(cudaGetLastError());
+    return 0;
+}
+
+// what the captured graphs depend on: options and the buffers they name
+static uint64_t step_sig(const Ctx& c) {
+    uint64_t h = 0x5e9ab1e57e9ull;
+    const unsigned char* pb = reinterpret_cast<const unsigned char*>(&c.p);
+    for (size_t i = 0; i + 8 <= sizeof(c.p); i += 8) {
+        uint64_t v;
+        std::memcpy(&v, pb + i, 8);
+        h = sig_mix(h, v);
+    }
+    for (const void* q : {(const void*)c.V.p, (const void*)c.Z32.p, (const void*)c.Z64.p, (const void*)c.w.p,
+                          (const void*)c.wtmp.p, (const void*)c.red.p, (const void*)c.U.p, (const void*)c.X.p,
+                          (const void*)c.XP.p, (const void*)c.Ee64.p, (const void*)c.v32.A0s.p,
+                          (const void*)c.v64.A0s.p, (const void*)c.h0.S.p, (const void*)c.mma_scal.p})
+        h = sig_mix(h, (uint64_t)(uintptr_t)q);
+    h = sig_mix(h, (uint64_t)c.robust_type | (uint64_t)c.constraint_mod << 8);
+    const double a[3] = {c.asyminit, c.asymdec, c.asyminc};
+    for (double x : a) {
+        uint64_t v;
+        std::memcpy(&v, &x, 8);
+        h = sig_mix(h, v);
+    }
+    return h;
+}
+
+static int capture_part(Ctx& c, int part) {
+    Ctx::StepGraph& G = c.sg;
+    // the captured work starts after everything queued on the context's stream
+    TCK(cudaEventRecord(G.e0, c.s));
+    TCK(cudaStreamWaitEvent(G.cap, G.e0, 0));
+    cudaStream_t s0 = c.s;
+    const bool prof = c.prof.on;
+    c.prof.on = false;
+    c.s = G.cap;
+    c.sg.dd = true;
+    c.sg.depth = 0;
+    const long l0 = launch_counter();
+    cudaError_t e = cudaStreamBeginCapture(G.cap, cudaStreamCaptureModeThreadLocal);
+    int rc = e == cudaSuccess ? step_part(c, part) : TOPO_ERR_CUDA;
+    // unwind nested captures left open by an error
+    while (c.sg.depth > 0) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(c.sg.body[c.sg.depth - 1], &g);
+        c.sg.depth--;
+    }
+    cudaGraph_t g = nullptr;
+    if (e == cudaSuccess) e = cudaStreamEndCapture(G.cap, &g);
+    c.sg.dd = false;
+    c.s = s0;
+    c.prof.on = prof;
+    const long n = launch_counter() - l0;
+    __atomic_fetch_sub(&launch_counter(), n, __ATOMIC_RELAXED);  // nothing ran yet
+    cudaGraphExec_t ex = nullptr;
+    if (rc >= 0 && e == cudaSuccess && g) e = cudaGraphInstantiate(&ex, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (rc < 0 || e != cudaSuccess || !ex) {
+        const char* why = e != cudaSuccess ? cudaGetErrorString(e) : last_error();
+        cudaGetLastError();
+        set_error("step graph capture failed (%s); direct launches from now on", why);
+        if (c.p.verbose) fprintf(stderr, "%s\n", last_error());
+        return TOPO_ERR_UNSUPPORTED;
+    }
+    G.exec[part] = ex;
+    G.launches[part] = n;
+    return 0;
+}
+
+static int capture_step(Ctx& c) {
+    Ctx::StepGraph& G = c.sg;
+    if (!G.cap) TCK(cudaStreamCreateWithFlags(&G.cap, cudaStreamNonBlocking));
+    for (auto& b : G.body)
+        if (!b) TCK(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
+    if (!G.e0) {
+        TCK(cudaEventCreate(&G.e0));
+        TCK(cudaEventCreate(&G.e1));
+        TCK(cudaEventCreateWithFlags(&G.mma_done, cudaEventDisableTiming));
+    }
+    if (!G.out.p) TRET(G.out.alloc(kOut));
+    for (int part = 0; part < 3; part++) {
+        const int rc = capture_part(c, part);
+        if (rc < 0) {
+            G.drop();
+            G.disabled = true;
+            return rc;
+        }
+    }
+    G.sig = step_sig(c);
+    G.state_dirty = true;
+    return 0;
+}
+
+// ----------------------------------------------------------------- replay
+// everything the graphs refer to exists: a direct step of this form (same
+// precision) has allocated it and the autotuner has run
+static bool graph_ready(const Ctx& c) {
+    const bool mixed = c.p.precision == TOPO_PREC_MIXED;
+    return c.X.p && c.U.p && c.V.p && c.uku.p && c.L.p && c.tune.single_done &&
+           (mixed ? (c.Z32.p && c.v32.allocated) : (c.Z64.p && c.v64.allocated));
+}
+
+// Decides whether this step can be replayed (capturing the graphs when
+// needed): not the first step of a run (it allocates, autotunes and builds
+// the solver state the graphs refer to), not the block solver, not after a
+// failed capture.
+int opt_step_graph_prepare(Ctx& c, bool* ok) {
+    *ok = false;
+    Ctx::StepGraph& G = c.sg;
+    c.info.step_graph = G.disabled ? -1 : 0;
+    if (G.disabled || c.ncases > 1 || c.itr < 1 || !graph_ready(c)) return 0;
+    if (G.exec[0] && G.sig != step_sig(c)) G.drop();
+    if (!G.exec[0] && capture_step(c) < 0) {  // disabled: the caller steps directly
+        c.info.step_graph = -1;
+        return 0;
+    }
+    if (G.state_dirty) {
+        // the device copies of the host-side loop state (after direct steps)
+        c.hsc.h[640] = c.beta_proj;
+        c.hsc.h[641] = c.beta_tmp;
+        TCK(cudaMemcpyAsync(c.dsc.p + DS_BETA, c.hsc.h + 640, 2 * sizeof(double), cudaMemcpyHostToDevice, c.s));
+        int* hi = reinterpret_cast<int*>(c.hsc.h + 642);
+        hi[0] = c.itr;
+        TCK(cudaMemcpyAsync(c.di.p + DI_ITR, hi, sizeof(int), cudaMemcpyHostToDevice, c.s));
+        G.state_dirty = false;
+    }
+    c.info.step_graph = 1;
+    *ok = true;
+    return 0;
+}
+
+// launches part p of a prepared step on the context's stream
+int opt_step_graph_part(Ctx& c, int part) {
+    Ctx::StepGraph& G = c.sg;
+    if (part == 0) TCK(cudaEventRecord(G.e0, c.s));
+    TCK(cudaGraphLaunch(G.exec[part], c.s));
+    __atomic_fetch_add(&launch_counter(), G.launches[part], __ATOMIC_RELAXED);
+    if (part == 1) TCK(cudaEventRecord(G.mma_done, c.s));
+    if (part == 2) {
+        TCK(cudaEventRecord(G.e1, c.s));
+        c.itr++;
+    }
+    return 0;
+}
+
+// Waits for a launched step and reads its results into the context's info.
+int opt_step_graph_finish(Ctx& c) {
+    TCK(cudaEventSynchronize(c.sg.e1));
+    const double* o = c.hsc.h + 600;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c.sg.e0, c.sg.e1) != cudaSuccess) { cudaGetLastError(); ms = 0.f; }
+    c.info.last_fx = o[0];
+    c.info.last_gx0 = o[1];
+    c.ch = c.info.last_ch = o[5];
+    c.info.fem_relres = o[6];
+    c.beta_proj = o[7];
+    c.beta_tmp = o[8];
+    c.info.mma_inner_its = (int)o[9];
+    c.info.fem_its = (int)o[11];
+    c.info.fem_status = (int)o[12];
+    int cg_status = 0;
+    for (int j = 0; j < 4; j++) {
+        c.info.filter_its[j] = (int)o[14 + j];
+        cg_status = std::max(cg_status, (int)o[18 + j]);
+    }
+    c.info.t_fem_ms = ms;  // the whole replayed step
+    c.info.t_filter_ms = c.info.t_mma_ms = 0.0;
+    c.u_valid = true;
+    if (c.p.verbose)
+        printf("It.: %i, fx: %f, gx[0]: %f, ch.: %f, time: %f\n", c.itr, c.info.last_fx, c.info.last_gx0, c.ch,
+               ms * 1e-3);
+    if (o[13] != 0.0 || !std::isfinite(c.info.last_fx)) {
+        c.u_valid = false;
+        amg_reset_warm_start(c);
+        set_error("a solve of the design iteration met a non-finite residual");
+        return TOPO_ERR_NAN;
+    }
+    if (o[10] != 0.0) {
+        set_error("MMA dual solve: grid barrier timed out");
+        return TOPO_ERR_TIMEOUT;
+    }
+    return (c.info.fem_status || cg_status) ? TOPO_NOT_CONVERGED : 0;
+}
+
+}  // namespace topo
