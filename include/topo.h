@@ -307,6 +307,14 @@ int topo_server_submit(topo_server* s, const topo_params* p, int nen, int n_node
                        const int32_t* element, int n_fixed, const int32_t* fixed_dofs, int n_cases,
                        const int32_t* case_ptr, const int32_t* load_dofs, const double* load_vals, int iterations,
                        double arrival_s, int* job_id);
+/* Instance batching (no counterpart in the reference): admitted jobs of at
+ * most max_elems elements and one load case run their first design iteration
+ * on a thread of their own, then join one batch worker that advances all the
+ * jobs it holds by one design iteration per round (topo_opt_step_batch with
+ * device-driven steps: one graph replay per job, all launched before one wait
+ * per round).  Jobs join and leave the batch between rounds.  0 (default)
+ * runs every job on its own thread.  Call before topo_server_run. */
+int topo_server_set_batching(topo_server* s, int max_elems);
 /* runs every submitted job to completion (real-time arrivals); blocks */
 int topo_server_run(topo_server* s);
 /* Cancels a job; safe to call from another thread while topo_server_run is

@@ -21,8 +21,8 @@ def jobs(T):
     return out
 
 
-def run(T, js, max_active, arrivals, iters=8):
-    s = T.Server(hbm_budget_bytes=0, max_active=max_active)
+def run(T, js, max_active, arrivals, iters=8, batch_max_elems=0):
+    s = T.Server(hbm_budget_bytes=0, max_active=max_active, batch_max_elems=batch_max_elems)
     for (v, e, f, ld, lv, kw), a in zip(js, arrivals):
         s.submit(v, e, f, ld, lv, iterations=iters, arrival_s=a, **kw)
     assert s.run() == 0
@@ -80,3 +80,23 @@ def test_footprint_estimate_is_an_upper_bound(T, cuda):
         ctx.close()
         est = T.estimate_job_bytes(8, v.shape[0], e.shape[0], prec)
         assert used <= est, (prec, used, est)
+
+
+def test_batched_instances_equal_alone(T, cuda):
+    """Instance batching: jobs up to 2,000 elements join one batch worker
+    that advances them together (one graph replay per job per round, one
+    wait per round); the largest job runs on its own thread beside them.
+    Every job's result equals its alone run, and the batch holds several
+    jobs at once."""
+    js = jobs(T)
+    alone = [run(T, [j], 1, [0.0])[0][0] for j in js]
+    sizes = [j[1].shape[0] for j in js]
+    limit = sorted(sizes)[-2]  # all but the largest job are batched
+    mixed, st = run(T, js, 4, [0.0, 0.0, 0.05, 0.1], batch_max_elems=limit)
+    assert st["jobs_done"] == 4 and st["jobs_failed"] == 0 and st["max_active"] >= 2
+    for a, m in zip(alone, mixed):
+        assert a["status"] == 0 and m["status"] == 0
+        assert len(m["fx"]) == 8
+        assert np.max(np.abs(a["fx"] - m["fx"]) / np.abs(a["fx"])) < 1e-6
+        assert np.abs(a["xphys"] - m["xphys"]).max() < 1e-5
+    assert st["iterations"] == 4 * 8

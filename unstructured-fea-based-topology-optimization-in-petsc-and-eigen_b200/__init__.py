@@ -127,6 +127,7 @@ _SIGS = {
                             C.POINTER(C.c_int)], C.c_int),
     "topo_server_run": ([C.c_void_p], C.c_int),
     "topo_server_cancel": ([C.c_void_p, C.c_int], C.c_int),
+    "topo_server_set_batching": ([C.c_void_p, C.c_int], C.c_int),
     "topo_test_wait_limits": ([C.c_void_p, C.c_uint, C.c_ulonglong, C.c_int], C.c_int),
     "topo_server_job": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)] + [C.c_void_p] * 3 +
                         [_dp, _dp], C.c_int),
@@ -564,11 +565,13 @@ def estimate_job_bytes(nen, n_nodes, n_elems, precision=PREC_FP64):
 class Server:
     """Continuous-batching job server (topo_server_*)."""
 
-    def __init__(self, hbm_budget_bytes=0, max_active=8):
+    def __init__(self, hbm_budget_bytes=0, max_active=8, batch_max_elems=0):
         h = C.c_void_p()
         _check(lib().topo_server_create(hbm_budget_bytes, max_active, C.byref(h)), "server_create")
         self.h = h
         self.jobs = []
+        if batch_max_elems:
+            _check(lib().topo_server_set_batching(h, batch_max_elems), "server_set_batching")
 
     def submit(self, vertex, element, fixed, load_dofs, load_vals, iterations, arrival_s=0.0, case_ptr=None,
                params=None, **kw):

@@ -9,6 +9,15 @@
 // the next ones: no step barrier couples the jobs.  Each job's state
 // (densities, displacements, filter warm start, MMA history) stays resident
 // in its context from admission to completion.
+//
+// Instance batching (topo_server_set_batching): admitted jobs up to a size
+// limit run their first design iteration on a thread of their own (it
+// allocates and tunes their context) and then join one batch worker, which
+// advances every job it holds by one design iteration per round with
+// topo_opt_step_batch: each job's iteration replayed from its step graph
+// (conditional nodes decide the solver loops on the device), all of them
+// launched before the worker waits once for the round.  Jobs join and leave
+// the batch between rounds.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -58,6 +67,10 @@ struct Job {
 struct topo_server {
     size_t budget = 0;
     int max_active = 1;
+    int batch_max_elems = 0;      // batching: jobs of at most this many elements (0: off)
+    std::vector<std::pair<Job*, topo_ctx*>> ready;  // prepared jobs waiting to join the batch
+    int preparing = 0;            // batched jobs still in their first iteration
+    bool batch_quit = false;
     std::vector<Job> jobs;
     std::mutex mu;
     std::condition_variable cv;
@@ -157,6 +170,17 @@ int topo_server_submit(topo_server* s, const topo_params* p, int nen, int n_node
     }
 }
 
+// a finished, failed or cancelled job gives back its slot and memory
+static void retire(topo_server* s, Job* j, int rc, Clock::time_point t0) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    j->status = rc;
+    j->state = rc == TOPO_ERR_CANCELLED ? 4 : rc < 0 ? 3 : 2;
+    j->finish_s = std::chrono::duration<double>(Clock::now() - t0).count();
+    s->reserved -= j->est_bytes;
+    s->active--;
+    s->cv.notify_all();
+}
+
 static void run_job(topo_server* s, Job* j, Clock::time_point t0) {
     topo_ctx* ctx = nullptr;
     int rc = topo_create(&j->p, j->nen, j->nn, j->vertex.data(), j->ne, j->element.data(), (int)j->fixed.size(),
@@ -194,13 +218,130 @@ static void run_job(topo_server* s, Job* j, Clock::time_point t0) {
         j->error = "host allocation failed";
     }
     if (ctx) topo_destroy(ctx);
-    std::lock_guard<std::mutex> lk(s->mu);
-    j->status = rc;
-    j->state = rc == TOPO_ERR_CANCELLED ? 4 : rc < 0 ? 3 : 2;
-    j->finish_s = std::chrono::duration<double>(Clock::now() - t0).count();
-    s->reserved -= j->est_bytes;
-    s->active--;
-    s->cv.notify_all();
+    retire(s, j, rc, t0);
+}
+
+// final design of a job, then its context goes
+static int finish_ctx(Job* j, topo_ctx* ctx, int rc) {
+    if (rc >= 0) {
+        double* xp = nullptr;
+        try {
+            j->xphys.resize(j->ne);
+        } catch (...) {
+            j->error = "host allocation failed";
+            topo_destroy(ctx);
+            return TOPO_ERR_OOM;
+        }
+        rc = topo_opt_vector(ctx, 1, &xp);
+        if (rc >= 0) rc = topo_memcpy_d2h(j->xphys.data(), xp, sizeof(double) * j->ne, ctx);
+        if (rc < 0) j->error = topo::last_error();
+    }
+    topo_destroy(ctx);
+    return rc;
+}
+
+// Batched job, first part: context, first design iteration (direct: it
+// allocates and tunes), then the hand-over to the batch worker.
+static void prepare_job(topo_server* s, Job* j, Clock::time_point t0) {
+    topo_ctx* ctx = nullptr;
+    j->p.step_graph = 1;
+    int rc = topo_create(&j->p, j->nen, j->nn, j->vertex.data(), j->ne, j->element.data(), (int)j->fixed.size(),
+                         j->fixed.data(), j->ncases, j->case_ptr.data(), j->load_dofs.data(), j->load_vals.data(),
+                         nullptr, &ctx);
+    try {
+        j->iter_ms.reserve(j->iterations);
+        j->fx_hist.reserve(j->iterations);
+        if (rc >= 0) rc = topo_opt_init(ctx);
+        if (rc >= 0 && j->cancel->load()) {
+            rc = TOPO_ERR_CANCELLED;
+            j->error = "cancelled";
+        }
+        if (rc >= 0) {
+            auto a = Clock::now();
+            double fx = 0.0;
+            rc = topo_opt_step(ctx, nullptr, &fx, nullptr, nullptr);
+            j->iter_ms.push_back(std::chrono::duration<double, std::milli>(Clock::now() - a).count());
+            j->fx_hist.push_back(fx);
+        }
+        if (rc < 0 && rc != TOPO_ERR_CANCELLED) j->error = topo::last_error();
+    } catch (...) {
+        rc = TOPO_ERR_OOM;
+        j->error = "host allocation failed";
+    }
+    if (rc >= 0 && (int)j->iter_ms.size() < j->iterations) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->ready.push_back({j, ctx});
+        s->preparing--;
+        s->cv.notify_all();
+        return;
+    }
+    if (ctx) rc = finish_ctx(j, ctx, rc);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->preparing--;
+    }
+    retire(s, j, rc, t0);
+}
+
+// Batched jobs, the rest: one design iteration of every held job per round.
+static void batch_worker(topo_server* s, Clock::time_point t0) {
+    std::vector<std::pair<Job*, topo_ctx*>> held;
+    std::vector<topo_ctx*> ctxs;
+    std::vector<int> st;
+    std::vector<double> fx;
+    while (true) {
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            while (s->ready.empty() && held.empty() && !(s->batch_quit && s->preparing == 0))
+                s->cv.wait_for(lk, std::chrono::milliseconds(50));
+            for (auto& r : s->ready) held.push_back(r);
+            s->ready.clear();
+            if (held.empty() && s->batch_quit && s->preparing == 0) return;
+        }
+        // cancellations take effect between rounds
+        for (size_t i = 0; i < held.size();) {
+            Job* j = held[i].first;
+            if (j->cancel->load()) {
+                j->error = "cancelled";
+                topo_destroy(held[i].second);
+                retire(s, j, TOPO_ERR_CANCELLED, t0);
+                held.erase(held.begin() + i);
+            } else {
+                i++;
+            }
+        }
+        if (held.empty()) continue;
+        ctxs.clear();
+        for (auto& h : held) ctxs.push_back(h.second);
+        st.assign(held.size(), 0);
+        fx.assign(held.size(), 0.0);
+        auto a = Clock::now();
+        topo_opt_step_batch(ctxs.data(), (int)ctxs.size(), st.data(), fx.data());
+        const double ms = std::chrono::duration<double, std::milli>(Clock::now() - a).count();
+        for (size_t i = 0; i < held.size();) {
+            Job* j = held[i].first;
+            j->iter_ms.push_back(ms);
+            j->fx_hist.push_back(fx[i]);
+            const bool done = (int)j->iter_ms.size() >= j->iterations;
+            if (st[i] < 0 || done) {
+                if (st[i] < 0) j->error = topo::last_error();
+                const int rc = finish_ctx(j, held[i].second, st[i]);
+                retire(s, j, rc, t0);
+                held.erase(held.begin() + i);
+                st.erase(st.begin() + i);
+                fx.erase(fx.begin() + i);
+            } else {
+                i++;
+            }
+        }
+    }
+}
+
+int topo_server_set_batching(topo_server* s, int max_elems) {
+    if (!s || max_elems < 0) { set_error("bad argument"); return TOPO_ERR_ARG; }
+    if (s->ran) { set_error("the server already ran"); return TOPO_ERR_ARG; }
+    s->batch_max_elems = max_elems;
+    return 0;
 }
 
 int topo_server_run(topo_server* s) {
@@ -221,6 +362,14 @@ int topo_server_run(topo_server* s) {
                      [&](int a, int b) { return s->jobs[a].arrival_s < s->jobs[b].arrival_s; });
     const auto t0 = Clock::now();
     size_t next = 0;
+    std::thread batcher;
+    if (s->batch_max_elems > 0) {
+        try {
+            batcher = std::thread(batch_worker, s, t0);
+        } catch (...) {
+            s->batch_max_elems = 0;  // no worker thread: every job runs on its own thread
+        }
+    }
     {
         std::unique_lock<std::mutex> lk(s->mu);
         while (true) {
@@ -244,9 +393,16 @@ int topo_server_run(topo_server* s) {
                 s->peak_reserved = std::max(s->peak_reserved, s->reserved);
                 s->active++;
                 s->max_seen = std::max(s->max_seen, s->active);
+                const bool batched = s->batch_max_elems > 0 && j.ne <= s->batch_max_elems && j.ncases == 1;
                 try {
-                    workers.emplace_back(run_job, s, &j, t0);
+                    if (batched) {
+                        s->preparing++;
+                        workers.emplace_back(prepare_job, s, &j, t0);
+                    } else {
+                        workers.emplace_back(run_job, s, &j, t0);
+                    }
                 } catch (...) {
+                    if (batched) s->preparing--;
                     // no host thread for this job: it fails, the others go on
                     j.status = TOPO_ERR_OOM;
                     j.error = "could not start a host thread for the job";
@@ -267,6 +423,14 @@ int topo_server_run(topo_server* s) {
         }
     }
     for (auto& t : workers) t.join();
+    if (batcher.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->batch_quit = true;
+            s->cv.notify_all();
+        }
+        batcher.join();
+    }
     s->makespan = std::chrono::duration<double>(Clock::now() - t0).count();
     int failed = 0;
     for (auto& j : s->jobs) failed += j.state == 3;
