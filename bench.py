@@ -280,20 +280,29 @@ def run_multiload(T, torch, steps, warmup, stream, forms=("block_mixed", "block_
     return out
 
 
-def run_serving(T, n_jobs, seed=7, rate=4.0, iters=30):
+BATCH_MAX_ELEMS = 150_000  # serving: jobs up to this size are advanced together by the batch worker
+
+
+def run_serving(T, n_jobs, seed=7, rate=4.0, iters=30, batch_max_elems=0):
     """Serving stream: Poisson arrivals (mean `rate` jobs/s, seeded) of hex8 /
-    tet4 cantilever jobs, sizes log-uniform in [20k, 1.2M] elements, volfrac
-    U(0.1, 0.3), filter radius U(1.2, 2.0) h, `iters` design iterations each,
-    mixed precision; HBM-budget admission, up to 8 jobs in flight."""
+    tet4 cantilever jobs, sizes log-uniform in [20k, 1.2M] elements (and the
+    middle job of the stream at the top of that range, 1.2M hex8 elements, so
+    that every stream holds the largest size), volfrac U(0.1, 0.3), filter
+    radius U(1.2, 2.0) h, `iters` design iterations each, mixed precision;
+    HBM-budget admission, up to 8 jobs in flight; with batch_max_elems > 0
+    the jobs up to that size are advanced together by the batch worker
+    (device-driven steps, one wait per round)."""
     import numpy as np
     rng = np.random.default_rng(seed)
-    s = T.Server(hbm_budget_bytes=0, max_active=8)
+    s = T.Server(hbm_budget_bytes=0, max_active=8, batch_max_elems=batch_max_elems)
     t = 0.0
     sizes = []
-    for _ in range(n_jobs):
+    for k in range(n_jobs):
         t += rng.exponential(1.0 / rate)
         ne = float(np.exp(rng.uniform(np.log(2e4), np.log(1.2e6))))
         nen = 8 if rng.uniform() < 0.5 else 4
+        if k == n_jobs // 2:
+            ne, nen = 1.2e6, 8
         a = max(2, int(round((ne / (2.0 if nen == 8 else 12.0)) ** (1.0 / 3.0))))
         v, e, f, ld, lv = T.gen_cantilever(2 * a, a, a, nen, seed=int(rng.integers(1, 2 ** 31)))
         kw = dict(PARAMS, volfrac=float(rng.uniform(0.1, 0.3)), rmin=float(rng.uniform(1.2, 2.0)),
@@ -302,10 +311,53 @@ def run_serving(T, n_jobs, seed=7, rate=4.0, iters=30):
         sizes.append(e.shape[0])
     rc = s.run()
     st = s.stats()
+    batched = sum(1 for n in sizes if n <= batch_max_elems) if batch_max_elems else 0
     s.close()
     st.update({"jobs": n_jobs, "arrival_rate_per_s": rate, "iterations_per_job": iters,
-               "elements_min": int(min(sizes)), "elements_max": int(max(sizes)), "rc": rc})
+               "elements_min": int(min(sizes)), "elements_max": int(max(sizes)), "rc": rc,
+               "batch_max_elems": batch_max_elems, "jobs_batched": batched})
     return st
+
+
+def run_tet4(T, torch, stream, steps, warmup, cpu_steps):
+    """The unstructured tet4 configuration: the 140 x 70 x 40 box with every
+    hex split into 6 tets (2,352,000 tet4, interior nodes jittered +-0.2 h),
+    same SIMP / filter / MMA settings; mixed and FP64 forms (zero start),
+    the element operator's roofline, and the CPU port on the same design
+    iterations (warm-up W, then K timed)."""
+    wl = WORKLOADS["tet4-2.35M"]
+    v, e, f, ld, lv = T.gen_cantilever(wl["nx"], wl["ny"], wl["nz"], 4)
+    ctx = T.Context(v, e, f, ld, lv, precision=T.PREC_MIXED, **PARAMS)
+    out = {"workload": f"tet4 {wl['nx']}x{wl['ny']}x{wl['nz']} x6 ({e.shape[0]} tets, {v.shape[0]} nodes)",
+           "steps": steps, "warmup": warmup}
+    ms, launches, _, its = run_device(ctx, T, torch, steps, warmup, stream, None, profile=False)
+    out["mixed"] = {"value": steps / (ms / 1e3), "ms_per_step": ms / steps, "fgmres_its": its,
+                    "gpu_launches": launches}
+    ctx.set_params(precision=T.PREC_FP64)
+    ms64, _, _, its64 = run_device(ctx, T, torch, steps, warmup, stream, None, profile=False)
+    out["fp64"] = {"value": steps / (ms64 / 1e3), "ms_per_step": ms64 / steps, "fgmres_its": its64}
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    # the FP64 element operator K(x) u for tet4 (k_kmv<4>): algorithmic bytes
+    # N_e (4 ids + mask + E + 78 packed Ke) + N_n 3 (u read + y write)
+    ctx.set_params(precision=T.PREC_FP64)
+    _, _, prof, _ = run_device(ctx, T, torch, min(steps, 2), 1, stream, None, profile=True)
+    n_kmv, t_kmv = prof.get("kmv", (0, 0.0))
+    if n_kmv:
+        b = kmv_bytes(ctx, 8)
+        peak, kind = peaks()
+        avg = t_kmv / n_kmv * 1e-3
+        out["kmv_tet4_fp64"] = {"kernel": "k_kmv<4, double>", "launches": n_kmv, "avg_us": avg * 1e6,
+                                "algorithmic_bytes": b, "gbs": b / avg / 1e9, "frac_hbm": b / avg / 1e9 / peak,
+                                "peak_kind": kind}
+    ctx.set_params(precision=T.PREC_MIXED)
+    out["compliance_error"] = compliance_errors(ctx, T, torch)
+    ctx.close()
+    if cpu_steps > 0:
+        done, dt, cores = cpu_run(wl, cpu_steps, 600.0, warmup=warmup)
+        out["cpu_port"] = {"value": done / dt, "unit": "design iters/s", "cores": cores, "kind": "port",
+                           "sample": f"design iterations {warmup + 1}..{warmup + done} (the GPU forms' first "
+                                     f"{done} timed ones) after {warmup} untimed"}
+    return out
 
 
 def kmv_bytes(ctx, u_bytes):
@@ -335,11 +387,14 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving stream (p50/p99 latency)")
     ap.add_argument("--serve-jobs", type=int, default=12)
-    ap.add_argument("--only", choices=["mixed", "fp64", "multiload"], default=None,
+    ap.add_argument("--only", choices=["mixed", "fp64", "multiload", "tet4", "serve"], default=None,
                     help="time one form only (used for short profiling runs)")
     ap.add_argument("--no-multiload", action="store_true", help="skip the k=8 multi-load configuration")
     ap.add_argument("--multiload-steps", type=int, default=6)
     ap.add_argument("--multiload-forms", default="block_mixed,block_fp64,one_by_one_mixed")
+    ap.add_argument("--no-tet4", action="store_true", help="skip the tet4 2.35M configuration")
+    ap.add_argument("--tet4-steps", type=int, default=4)
+    ap.add_argument("--tet4-cpu-steps", type=int, default=1)
     ap.add_argument("--param", action="append", default=[],
                     help="override a solver option for this run, e.g. --param fem_graphs=0")
     args = ap.parse_args()
@@ -387,6 +442,18 @@ def main():
         dist = dist_mod
     T = _pkg()
     stream = torch.cuda.current_stream()
+    if args.only == "tet4":
+        if rank == 0:
+            print(json.dumps({"only": "tet4", **run_tet4(T, torch, stream, args.tet4_steps, min(args.warmup, 2),
+                                                         0 if args.no_cpu_baseline else args.tet4_cpu_steps)}),
+                  flush=True)
+        return
+    if args.only == "serve":
+        if rank == 0:
+            print(json.dumps({"only": "serve",
+                              "serve": run_serving(T, args.serve_jobs, seed=7, batch_max_elems=BATCH_MAX_ELEMS),
+                              "serve_unbatched": run_serving(T, args.serve_jobs, seed=7)}), flush=True)
+        return
     if args.only == "multiload":
         if rank == 0:
             print(json.dumps({"only": "multiload",
@@ -484,9 +551,13 @@ def main():
     multi = None
     if not args.no_multiload and rank == 0 and world == 1:
         multi = run_multiload(T, torch, args.multiload_steps, 3, stream)
-    serve = None
+    serve = serve_unbatched = None
     if not args.no_serve:
-        serve = run_serving(T, args.serve_jobs, seed=7)
+        serve = run_serving(T, args.serve_jobs, seed=7, batch_max_elems=BATCH_MAX_ELEMS)
+        serve_unbatched = run_serving(T, args.serve_jobs, seed=7, batch_max_elems=0)
+    tet4 = None
+    if not args.no_tet4 and rank == 0 and world == 1:
+        tet4 = run_tet4(T, torch, stream, args.tet4_steps, 2, 0 if args.no_cpu_baseline else args.tet4_cpu_steps)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         done, dt, cores = cpu_run(wl, args.cpu_steps, 60.0, warmup=1)
@@ -507,7 +578,7 @@ def main():
             "e2e": {"value": e2e_val, "unit": "design iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "clocks": clocks, "cpu_baseline": cpu,
             "fgmres_initial_guess": "previous design iteration's U (warm start); stopping rule unchanged",
-            "multiload": multi, "serve": serve, "kernels": kern,
+            "multiload": multi, "tet4": tet4, "serve_unbatched": serve_unbatched, "serve": serve, "kernels": kern,
             "fgmres_its_per_step": {"mixed_warm": its, "mixed_zero_start": itsz, "fp64": its64, "fp64_warm": its64w,
                                     "mixed_fp16_fine": its16},
             "setup_s": setup_s, "fgmres_breakdown": breakdown,

@@ -83,7 +83,7 @@ def test_footprint_estimate_is_an_upper_bound(T, cuda):
 
 
 def test_batched_instances_equal_alone(T, cuda):
-    """Instance batching: jobs up to 2,000 elements join one batch worker
+    """Instance batching: every job but the largest joins one batch worker
     that advances them together (one graph replay per job per round, one
     wait per round); the largest job runs on its own thread beside them.
     Every job's result equals its alone run, and the batch holds several
