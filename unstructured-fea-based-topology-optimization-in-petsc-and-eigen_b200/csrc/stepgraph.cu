@@ -253,13 +253,14 @@ static bool graph_ready(const Ctx& c) {
 
 // Decides whether this step can be replayed (capturing the graphs when
 // needed): not the first step of a run (it allocates, autotunes and builds
-// the solver state the graphs refer to), not the block solver, not after a
-// failed capture.
+// the solver state the graphs refer to), not the block solver, not while
+// per-kernel timing is on, not after a failed capture.
 int opt_step_graph_prepare(Ctx& c, bool* ok) {
     *ok = false;
     Ctx::StepGraph& G = c.sg;
     c.info.step_graph = G.disabled ? -1 : 0;
-    if (G.disabled || c.ncases > 1 || c.itr < 1 || !graph_ready(c)) return 0;
+    // per-kernel event timing (topo_profile_enable) needs the direct launches
+    if (G.disabled || c.ncases > 1 || c.itr < 1 || c.prof.on || !graph_ready(c)) return 0;
     if (G.exec[0] && G.sig != step_sig(c)) G.drop();
     if (!G.exec[0] && capture_step(c) < 0) {  // disabled: the caller steps directly
         c.info.step_graph = -1;
