@@ -100,6 +100,8 @@ typedef struct topo_params {
                               loops as conditional graph nodes decided on the device (no host
                               round trip inside an iteration); 0 (default): host-driven iterations.
                               One load case (the block solver always steps directly). */
+    int blk_stages;        /* block operator: element-matrix copies in flight per warp, 2 or 3;
+                              0 (default): the autotuner times both */
 } topo_params;
 
 typedef struct topo_solve_info {
@@ -113,7 +115,8 @@ typedef struct topo_solve_info {
     double last_fx, last_gx0, last_ch;
     double t_fem_ms, t_filter_ms, t_mma_ms, t_setup_ms; /* stage times (CUDA events) */
     int tuned[4];          /* launch shapes picked by the autotuner: element-operator block,
-                              level-0 smoother block, reduction grid, block-operator CTAs/SM */
+                              level-0 smoother block, reduction grid, block operator (10 x Ke
+                              copies in flight per warp + CTAs per SM, 0: occupancy limit) */
     int tuned_lanes[8];    /* lanes per block row picked for the smoothing and residual products
                               of AMG level l >= 1 (0: not tuned) */
     int step_graph;        /* last design iteration: 1 replayed from the step graph, 0 stepped

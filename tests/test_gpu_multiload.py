@@ -38,12 +38,14 @@ def mesh(T, nen, k):
     return v, e, f, ld, lv, cp
 
 
+@pytest.mark.parametrize("stages", [2, 3])
 @pytest.mark.parametrize("nen,k", [(8, 3), (8, 8), (8, 11), (4, 3), (4, 8)])
-def test_block_operator_matches_oracle(T, O, cuda, nen, k):
-    """K(x) [u_1..u_k] by the tensor-core block kernel against the oracle's
-    assembled K applied case by case (Dirichlet rows/columns identity)."""
+def test_block_operator_matches_oracle(T, O, cuda, nen, k, stages):
+    """K(x) [u_1..u_k] by the tensor-core block kernel (2 and 3 element-matrix
+    copies in flight per warp) against the oracle's assembled K applied case
+    by case (Dirichlet rows/columns identity)."""
     v, e, f, ld, lv, cp = mesh(T, nen, k)
-    ctx = T.Context(v, e, f, ld, lv, case_ptr=cp, **KW)
+    ctx = T.Context(v, e, f, ld, lv, case_ptr=cp, blk_stages=stages, **KW)
     orc = O.Oracle(v, e, f, ld[:3], lv[:3], **KW)
     rng = np.random.default_rng(11 + k)
     x = rng.uniform(0.01, 1.0, e.shape[0])

@@ -378,6 +378,10 @@ static int check_params(const topo_params* p) {
         set_error("cheb_degree_post and cheb_degree_coarse must be in [0,15] (0: as cheb_degree)");
         return TOPO_ERR_ARG;
     }
+    if (p->blk_stages != 0 && p->blk_stages != 2 && p->blk_stages != 3) {
+        set_error("blk_stages must be 0 (tuned), 2 or 3");
+        return TOPO_ERR_ARG;
+    }
     if (p->amg_rho_its < 0 || p->amg_rho_its > 1000) { set_error("amg_rho_its must be in [0,1000]"); return TOPO_ERR_ARG; }
     if (!(p->cheb_safety >= 0.0 && p->cheb_safety <= 10.0)) {
         set_error("cheb_safety must be in [0,10] (0: 1)");

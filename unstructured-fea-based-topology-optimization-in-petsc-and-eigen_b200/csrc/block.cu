@@ -11,7 +11,8 @@
 // tcgen05 instruction family has no FP64 kind).  One warp owns one element at
 // a time: its packed Ke (300 doubles) is brought into shared memory by the
 // TMA engine (cp.async.bulk, completion on a per-warp mbarrier, a ring of
-// kStages copies in flight per warp), the U_e fragments are gathered from
+// ST copies in flight per warp, 2 or 3 picked by the autotuner: 2 leaves room
+// for a third CTA per SM), the U_e fragments are gathered from
 // global memory one phase ahead, and the outputs accumulate in a
 // shared-memory image of the chunk's nodes.  Elements are grouped (host
 // side, once per mesh) into chunks of <= 64 spatially close elements (Morton
@@ -31,7 +32,6 @@
 namespace topo {
 
 constexpr int kWarps = 8;      // warps (= elements per phase) per CTA
-constexpr int kStages = 3;     // Ke copies in flight per warp
 constexpr int kChunkElems = 64;
 
 // ----------------------------------------------------------------- host: chunks and phases
@@ -273,22 +273,22 @@ struct BlkArgs {
 //         columns masked on input, Dirichlet rows not written (the caller
 //         sets them).
 // MODE 1: uku[e] = sum_case u_e' Ke_e u_e (E = 1, unmasked u).
-template <int NEN, int KB, int MODE, class TU>
+template <int NEN, int KB, int MODE, class TU, int ST>
 __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __restrict__ u, double* __restrict__ y,
                                                        double alpha, double* __restrict__ uku) {
     constexpr int ND = 3 * NEN, NPK = ND * (ND + 1) / 2;
     constexpr int MT = (ND + 7) / 8, KT = (ND + 3) / 4, NT = (KB + 7) / 8;
     constexpr int NVL = 3 * KB;  // values per node in the shared image
     extern __shared__ __align__(128) unsigned char smraw[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);                        // [kWarps][kStages]
-    double* kes = reinterpret_cast<double*>(smraw + 128 * ((kWarps * kStages * 8 + 127) / 128));
-    double* yl = kes + kWarps * kStages * NPK;                                  // [max_nodes][3][KB]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);                        // [kWarps][ST]
+    double* kes = reinterpret_cast<double*>(smraw + 128 * ((kWarps * ST * 8 + 127) / 128));
+    double* yl = kes + kWarps * ST * NPK;                                  // [max_nodes][3][KB]
     __shared__ int s_abort;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nch = a.nchunks;
     if (threadIdx.x == 0) s_abort = 0;
     if (lane == 0)
-        for (int s = 0; s < kStages; s++) mbar_init(&bar[warp * kStages + s], 1);
+        for (int s = 0; s < ST; s++) mbar_init(&bar[warp * ST + s], 1);
     fence_mbar_init();
     // per-lane A-fragment offsets into the packed Ke
     int aoff[MT][KT];
@@ -309,13 +309,13 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
     uint32_t parity = 0, pending = 0;
     auto issue = [&]() {
         const int s0 = a.ph_sl[pp], cnt = a.ph_sl[pp + 1] - s0;
-        const int st = pq % kStages;
+        const int st = pq % ST;
         if (warp < cnt && !a.hold) {
             if (lane == 0) {
                 fence_proxy_async();
-                mbar_expect_tx(&bar[warp * kStages + st], NPK * 8);
-                bulk_g2s(kes + (warp * kStages + st) * NPK, a.keb + (size_t)(s0 + warp) * NPK, NPK * 8,
-                         &bar[warp * kStages + st]);
+                mbar_expect_tx(&bar[warp * ST + st], NPK * 8);
+                bulk_g2s(kes + (warp * ST + st) * NPK, a.keb + (size_t)(s0 + warp) * NPK, NPK * 8,
+                         &bar[warp * ST + st]);
             }
             pending |= 1u << st;
         }
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
             pp = pc < nch ? a.ch_ph[pc] : 0;
         }
     };
-    for (int i = 0; i < kStages - 1 && pc < nch; i++) issue();
+    for (int i = 0; i < ST - 1 && pc < nch; i++) issue();
 
     // Per-element data of the elements this warp owns in the next phases,
     // fetched ahead so that no dependent global load sits on the critical
@@ -400,18 +400,18 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
     bool ok = true;
     while (cc < nch) {
         if (pc < nch) issue();
-        const int st = cq % kStages;
+        const int st = cq % ST;
         load_meta(c2, p2, mnn);
         load_b(mn, bnxt);
         if (mc.has) {
-            if (mbar_wait(&bar[warp * kStages + st], (parity >> st) & 1u, a.wait_cycles)) {
+            if (mbar_wait(&bar[warp * ST + st], (parity >> st) & 1u, a.wait_cycles)) {
                 parity ^= 1u << st;
                 pending &= ~(1u << st);
             } else {
                 ok = false;
                 if (lane == 0) { s_abort = 1; atomicExch(a.err, 1); }
             }
-            const double* ks = kes + (warp * kStages + st) * NPK;
+            const double* ks = kes + (warp * ST + st) * NPK;
             const double sc = MODE == 0 ? alpha * mc.E : 1.0;
             double q = 0.0;
 #pragma unroll
@@ -482,8 +482,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
     }
     // on an abort, let this warp's copies in flight land before the CTA exits
     if (lane == 0 && pending) {
-        for (int s = 0; s < kStages; s++)
-            if ((pending >> s) & 1u) mbar_wait(&bar[warp * kStages + s], (parity >> s) & 1u, a.wait_cycles);
+        for (int s = 0; s < ST; s++)
+            if ((pending >> s) & 1u) mbar_wait(&bar[warp * ST + s], (parity >> s) & 1u, a.wait_cycles);
     }
 }
 
@@ -520,18 +520,18 @@ __global__ void k_blk_init(long n, double* __restrict__ y, const double* __restr
 }
 
 // ----------------------------------------------------------------- host entry points
-static size_t blk_smem(int npk, int kb, int nodes) {
-    return 128 * ((kWarps * kStages * 8 + 127) / 128) +
-           sizeof(double) * ((size_t)kWarps * kStages * npk + (size_t)nodes * 3 * kb);
+static size_t blk_smem(int npk, int kb, int nodes, int stages) {
+    return 128 * ((kWarps * stages * 8 + 127) / 128) +
+           sizeof(double) * ((size_t)kWarps * stages * npk + (size_t)nodes * 3 * kb);
 }
 
 int blk_width(int ncases) { return ncases <= 4 ? 4 : ncases <= 8 ? 8 : 16; }
 
-template <int NEN, int KB, int MODE, class TU>
-static int launch_blk(Ctx& c, const TU* u, double* y, double alpha, double* uku) {
+template <int NEN, int KB, int MODE, class TU, int ST>
+static int launch_blk_st(Ctx& c, const TU* u, double* y, double alpha, double* uku) {
     BlockState& B = c.blk;
-    auto kern = k_blk_kmv<NEN, KB, MODE, TU>;
-    const size_t smem = blk_smem(c.npk, KB, B.max_nodes);
+    auto kern = k_blk_kmv<NEN, KB, MODE, TU, ST>;
+    const size_t smem = blk_smem(c.npk, KB, B.max_nodes, ST);
     TCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
     TCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kWarps * 32, smem));
@@ -545,6 +545,13 @@ static int launch_blk(Ctx& c, const TU* u, double* y, double alpha, double* uku)
     kern<<<grid, kWarps * 32, smem, c.s>>>(a, u, y, alpha, uku), note_launch();
     TCK(cudaGetLastError());
     return 0;
+}
+
+template <int NEN, int KB, int MODE, class TU>
+static int launch_blk(Ctx& c, const TU* u, double* y, double alpha, double* uku) {
+    const int st = c.p.blk_stages ? c.p.blk_stages : c.tune.blk_stages;
+    if (st == 2) return launch_blk_st<NEN, KB, MODE, TU, 2>(c, u, y, alpha, uku);
+    return launch_blk_st<NEN, KB, MODE, TU, 3>(c, u, y, alpha, uku);
 }
 
 template <int MODE, class TU>

@@ -695,9 +695,12 @@ int autotune_block(Ctx& c) {
     TCK(cudaEventCreate(&e0));
     TCK(cudaEventCreate(&e1));
     double best = 1e30;
-    int pick = 0;
-    for (int ctas : {1, 0}) {
+    int pick = 0, pick_st = 3;
+    for (int cand : {31, 30, 21, 20}) {  // Ke copies in flight per warp x 10 + CTAs per SM (0: occupancy)
+        if (c.p.blk_stages && cand / 10 != c.p.blk_stages) continue;  // forced by the options
+        const int ctas = cand % 10;
         c.tune.blk_ctas = ctas;
+        c.tune.blk_stages = cand / 10;
         double t = 1e30;
         for (int rep = 0; rep < 3; rep++) {
             TCK(cudaEventRecord(e0, c.s));
@@ -708,13 +711,14 @@ int autotune_block(Ctx& c) {
             TCK(cudaEventElapsedTime(&ms, e0, e1));
             t = std::min(t, (double)ms);
         }
-        if (t < best) { best = t; pick = ctas; }
+        if (t < best) { best = t; pick = ctas; pick_st = cand / 10; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c.tune.blk_ctas = pick;
+    c.tune.blk_stages = pick_st;
     c.prof.on = prof;
-    c.info.tuned[3] = pick;
+    c.info.tuned[3] = 10 * pick_st + pick;
     return 0;
 }
 
@@ -796,7 +800,7 @@ static int fgmres_blk(Ctx& c, const double* b, double* x, int* its_out, int* sta
                        (uint64_t)(uintptr_t)B.bv32.x[0].p, (uint64_t)(uintptr_t)B.bv64.x[0].p,
                        (uint64_t)(uintptr_t)c.v32.A0s.p, (uint64_t)(uintptr_t)c.v64.A0s.p,
                        (uint64_t)(uintptr_t)c.cinv.p, (uint64_t)(uintptr_t)c.rho.p, (uint64_t)c.p.precision,
-                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.tune.blk_ctas, (uint64_t)KB, (uint64_t)nf})
+                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.tune.blk_ctas, (uint64_t)c.tune.blk_stages, (uint64_t)KB, (uint64_t)nf})
         sig = sig_mix(sig, v);
     StepGraphs& G = B.graphs;
     if (G.sig != sig) {
