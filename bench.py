@@ -286,7 +286,7 @@ def run_multiload(T, torch, steps, warmup, stream, forms=("block_mixed", "block_
 BATCH_MAX_ELEMS = 150_000  # serving: jobs up to this size are advanced together by the batch worker
 
 
-def run_serving(T, n_jobs, seed=7, rate=4.0, iters=30, batch_max_elems=0):
+def run_serving(T, n_jobs, seed=7, rate=4.0, iters=30, batch_max_elems=0, size_range=(2e4, 1.2e6), top_job=True):
     """Serving stream: Poisson arrivals (mean `rate` jobs/s, seeded) of hex8 /
     tet4 cantilever jobs, sizes log-uniform in [20k, 1.2M] elements (and the
     middle job of the stream at the top of that range, 1.2M hex8 elements, so
@@ -302,10 +302,10 @@ def run_serving(T, n_jobs, seed=7, rate=4.0, iters=30, batch_max_elems=0):
     sizes = []
     for k in range(n_jobs):
         t += rng.exponential(1.0 / rate)
-        ne = float(np.exp(rng.uniform(np.log(2e4), np.log(1.2e6))))
+        ne = float(np.exp(rng.uniform(np.log(size_range[0]), np.log(size_range[1]))))
         nen = 8 if rng.uniform() < 0.5 else 4
-        if k == n_jobs // 2:
-            ne, nen = 1.2e6, 8
+        if top_job and k == n_jobs // 2:
+            ne, nen = size_range[1], 8
         a = max(2, int(round((ne / (2.0 if nen == 8 else 12.0)) ** (1.0 / 3.0))))
         v, e, f, ld, lv = T.gen_cantilever(2 * a, a, a, nen, seed=int(rng.integers(1, 2 ** 31)))
         kw = dict(PARAMS, volfrac=float(rng.uniform(0.1, 0.3)), rmin=float(rng.uniform(1.2, 2.0)),
@@ -320,6 +320,21 @@ def run_serving(T, n_jobs, seed=7, rate=4.0, iters=30, batch_max_elems=0):
                "elements_min": int(min(sizes)), "elements_max": int(max(sizes)), "rc": rc,
                "batch_max_elems": batch_max_elems, "jobs_batched": batched})
     return st
+
+
+def serve_small_jobs(T, n_jobs=16):
+    """A stream of small jobs only (sizes log-uniform in [20k, 150k] elements,
+    Poisson 8 jobs/s, otherwise the serving configuration's settings), with
+    and without instance batching: where per-job host round trips and kernel
+    launches, not HBM, bound an iteration."""
+    kw = dict(n_jobs=n_jobs, seed=11, rate=8.0, size_range=(2e4, 1.5e5), top_job=False)
+    keys = ("p50_iter_ms", "p99_iter_ms", "mean_iter_ms", "jobs_per_hour", "iters_per_s", "makespan_s", "jobs_done",
+            "jobs_batched", "elements_min", "elements_max", "max_active")
+    out = {"stream": "16 jobs, 20k-150k elements log-uniform, Poisson 8 jobs/s, 30 iterations each"}
+    for name, lim in (("batched", BATCH_MAX_ELEMS), ("unbatched", 0)):
+        st = run_serving(T, batch_max_elems=lim, **kw)
+        out[name] = {k: st[k] for k in keys}
+    return out
 
 
 def run_tet4(T, torch, stream, steps, warmup, cpu_steps):
@@ -455,7 +470,8 @@ def main():
         if rank == 0:
             print(json.dumps({"only": "serve",
                               "serve": run_serving(T, args.serve_jobs, seed=7, batch_max_elems=BATCH_MAX_ELEMS),
-                              "serve_unbatched": run_serving(T, args.serve_jobs, seed=7)}), flush=True)
+                              "serve_unbatched": run_serving(T, args.serve_jobs, seed=7),
+                              "serve_small_jobs": serve_small_jobs(T)}), flush=True)
         return
     if args.only == "multiload":
         if rank == 0:
@@ -554,10 +570,11 @@ def main():
     multi = None
     if not args.no_multiload and rank == 0 and world == 1:
         multi = run_multiload(T, torch, args.multiload_steps, 3, stream)
-    serve = serve_unbatched = None
+    serve = serve_unbatched = serve_small = None
     if not args.no_serve:
         serve = run_serving(T, args.serve_jobs, seed=7, batch_max_elems=BATCH_MAX_ELEMS)
         serve_unbatched = run_serving(T, args.serve_jobs, seed=7, batch_max_elems=0)
+        serve_small = serve_small_jobs(T)
     tet4 = None
     if not args.no_tet4 and rank == 0 and world == 1:
         tet4 = run_tet4(T, torch, stream, args.tet4_steps, 2, 0 if args.no_cpu_baseline else args.tet4_cpu_steps)
@@ -581,7 +598,8 @@ def main():
             "e2e": {"value": e2e_val, "unit": "design iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "clocks": clocks, "cpu_baseline": cpu,
             "fgmres_initial_guess": "previous design iteration's U (warm start); stopping rule unchanged",
-            "multiload": multi, "tet4": tet4, "serve_unbatched": serve_unbatched, "serve": serve, "kernels": kern,
+            "multiload": multi, "tet4": tet4, "serve_small_jobs": serve_small, "serve_unbatched": serve_unbatched,
+            "serve": serve, "kernels": kern,
             "fgmres_its_per_step": {"mixed_warm": its, "mixed_zero_start": itsz, "fp64": its64, "fp64_warm": its64w,
                                     "mixed_fp16_fine": its16},
             "setup_s": setup_s, "fgmres_breakdown": breakdown,
