@@ -52,6 +52,7 @@ def test_struct_mirrors_match_the_library(T):
     assert (p.cheb_degree, p.cheb_degree_post, p.cheb_degree_coarse) == (2, 0, 4)
     assert (p.fem_restart, p.fem_block, p.fem_graphs, p.autotune, p.pdl) == (30, 1, 1, 1, 1)
     assert (p.amg_coarse_cta, p.amg_half_fine, p.fem_warm_start) == (0, 0, 0)
+    assert (p.step_graph, p.blk_stages) == (0, 0)
 
 
 @pytest.mark.parametrize("nen", [8, 4])
@@ -206,7 +207,8 @@ def test_driver_program_fails_loudly_without_a_gpu(tmp_path):
 @pytest.mark.parametrize("field,value", [("cheb_degree_coarse", 16), ("cheb_degree_post", -1), ("amg_max_levels", 0),
                                          ("amg_max_levels", 9), ("amg_rho_its", -2), ("cheb_safety", -0.5),
                                          ("pdl", 2), ("fem_graphs", -1), ("autotune", 3), ("amg_half_fine", 2),
-                                         ("fem_block", 5), ("proj", 2), ("amg_coarse_max", 5), ("cheb_degree", 0)])
+                                         ("fem_block", 5), ("proj", 2), ("amg_coarse_max", 5), ("cheb_degree", 0),
+                                         ("step_graph", 2), ("blk_stages", 1), ("blk_stages", 4)])
 def test_invalid_solver_options_rejected_before_any_device_work(T, field, value):
     """Out-of-range solver options are refused at creation with the option's
     name in the message (no silent clamping), before any device call."""
@@ -227,3 +229,15 @@ def test_job_footprint_estimate_is_monotone(T):
         assert T.estimate_job_bytes(nen, 400_000, 390_000, T.PREC_FP64) > big
         more_elems = T.estimate_job_bytes(nen, 400_000, 780_000, T.PREC_MIXED)
         assert more_elems - big >= 390_000 * 9 * nen * nen * 4
+
+
+def test_batch_and_server_arguments_checked_on_the_host(T):
+    """topo_opt_step_batch and the server's batching switch reject bad
+    arguments before any device work."""
+    import ctypes as C
+    L = T.lib()
+    assert L.topo_opt_step_batch(None, 1, None, None) == T.TOPO_ERR_ARG
+    arr = (C.c_void_p * 2)(None, None)
+    assert L.topo_opt_step_batch(arr, 2, None, None) == T.TOPO_ERR_ARG and "null context" in T.last_error()
+    assert L.topo_opt_step_batch(arr, 0, None, None) == 0  # nothing to do
+    assert L.topo_server_set_batching(None, 10) == T.TOPO_ERR_ARG
