@@ -270,12 +270,26 @@ int topo_opt_run(topo_ctx* ctx, int max_itr, double* hist, int* iterations);
  * Instances whose options select step_graph = 1 and that have done their first
  * iteration are replayed from their step graphs: all of them are launched,
  * each on its own context stream, before the host waits for any, so their
- * iterations overlap on the device (the cooperative MMA dual solves run one
- * after another); the other instances step directly, after those launches.
+ * iterations overlap on the device (the cooperative MMA dual solves of a
+ * process run one after another on a device); the other instances step
+ * directly, after those launches.
  * status[i] (may be NULL) receives each instance's status, fx[i] (may be NULL)
  * its compliance.  Returns the most severe status: the first error (< 0)
  * met, else the largest warning.  Contexts that share a stream serialise. */
 int topo_opt_step_batch(topo_ctx* const* ctxs, int n, int* status, double* fx);
+/* One design iteration without waiting for it (no counterpart in the
+ * reference).  With step_graph = 1 and a replayable step, topo_opt_step_async
+ * launches the iteration's solve and returns at once; topo_opt_step_query
+ * never blocks: it launches the rest of the iteration once the solve has
+ * finished, and when the iteration is done sets *done = 1, fills itr, fx, gx0
+ * and ch (host, may be NULL) and returns the iteration's status (as
+ * topo_opt_step).  Otherwise (the first iteration of a run, the block solver,
+ * step_graph = 0) the iteration runs directly inside topo_opt_step_async and
+ * the next query reports it.  One host thread can keep many contexts going
+ * this way; while an iteration is in flight its context accepts no other
+ * optimisation call. */
+int topo_opt_step_async(topo_ctx* ctx);
+int topo_opt_step_query(topo_ctx* ctx, int* done, int* itr, double* fx, double* gx0, double* ch);
 /* Host-buffer form used end to end: uploads the design X (host, n_elems),
  * runs one iteration, downloads the updated X and XPhys (host) and fx. */
 int topo_opt_step_host(topo_ctx* ctx, const double* x_in, double* x_out, double* xphys_out, double* fx);
@@ -312,11 +326,11 @@ int topo_server_submit(topo_server* s, const topo_params* p, int nen, int n_node
                        double arrival_s, int* job_id);
 /* Instance batching (no counterpart in the reference): admitted jobs of at
  * most max_elems elements and one load case run their first design iteration
- * on a thread of their own, then join one batch worker that advances all the
- * jobs it holds by one design iteration per round (topo_opt_step_batch with
- * device-driven steps: one graph replay per job, all launched before one wait
- * per round).  Jobs join and leave the batch between rounds.  0 (default)
- * runs every job on its own thread.  Call before topo_server_run. */
+ * on a thread of their own, then join one batch worker that keeps all of them
+ * going from one host thread: each job's iterations are replayed from its
+ * step graphs (topo_opt_step_async / topo_opt_step_query) and relaunched as
+ * soon as they are done.  0 (default) runs every job on its own thread.  Call
+ * before topo_server_run. */
 int topo_server_set_batching(topo_server* s, int max_elems);
 /* runs every submitted job to completion (real-time arrivals); blocks */
 int topo_server_run(topo_server* s);

@@ -125,3 +125,43 @@ def test_batch_of_instances_equals_solo_runs(T, cuda):
         assert ctxs[k].info().fem_its > 0 and ctxs[k].info().step_graph == 1
     for c in ctxs:
         c.close()
+
+
+def test_async_steps_from_one_thread_equal_solo_runs(T, cuda):
+    """topo_opt_step_async / topo_opt_step_query: three instances kept going
+    from one host thread, each relaunched as soon as its iteration is done,
+    equal their solo host-driven runs; a context with an iteration in flight
+    refuses other optimisation calls."""
+    specs = [((20, 10, 6, 8), dict(volfrac=0.12)), ((12, 6, 6, 4), dict(volfrac=0.2, rmin=1.3)),
+             ((16, 8, 8, 8), dict(volfrac=0.25, precision=1))]
+    n = 8
+    solo = [run(T, T.gen_cantilever(*d), n, step_graph=0, **kw)[0][:, 0] for d, kw in specs]
+    ctxs = [T.Context(*T.gen_cantilever(*d), stream="own", step_graph=1, **dict(KW, **kw)) for d, kw in specs]
+    for c in ctxs:
+        c.opt_init()
+    hist = [[] for _ in ctxs]
+    running = [False] * len(ctxs)
+    checked = False
+    while min(len(h) for h in hist) < n:
+        for k, c in enumerate(ctxs):
+            if len(hist[k]) >= n:
+                continue
+            if not running[k]:
+                c.opt_step_async()
+                running[k] = True
+                if len(hist[k]) >= 2 and not checked:  # a replayed iteration is in flight
+                    with pytest.raises(T.TopoError):
+                        c.opt_step()
+                    checked = True
+                continue
+            r = c.opt_step_query()
+            if r is not None:
+                rc, it, fx, gx, ch = r
+                assert rc == 0 and it == len(hist[k]) + 1
+                hist[k].append(fx)
+                running[k] = False
+    assert checked
+    for k, c in enumerate(ctxs):
+        assert rel(np.array(hist[k]), solo[k]) < 1e-6, k
+        assert c.info().step_graph == 1
+        c.close()

@@ -118,6 +118,8 @@ _SIGS = {
     "topo_opt_run": ([C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)], C.c_int),
     "topo_opt_step_host": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _dp], C.c_int),
     "topo_opt_step_batch": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+    "topo_opt_step_async": ([C.c_void_p], C.c_int),
+    "topo_opt_step_query": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp, _dp], C.c_int),
     "topo_fem_sensitivities_noalloc": ([C.c_int, C.c_int] + [C.c_void_p] * 5 + [C.c_double] * 5 +
                                        [C.c_void_p] * 4, C.c_int),
     "topo_estimate_job_bytes": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_size_t),
@@ -469,6 +471,17 @@ class Context:
         it, fx, gx, ch = C.c_int(), C.c_double(), C.c_double(), C.c_double()
         rc = _check(lib().topo_opt_step(self.h, C.byref(it), C.byref(fx), C.byref(gx), C.byref(ch)), "opt_step")
         return it.value, fx.value, gx.value, ch.value
+
+    def opt_step_async(self):
+        """Start one design iteration without waiting for it."""
+        _check(lib().topo_opt_step_async(self.h), "opt_step_async")
+
+    def opt_step_query(self):
+        """None while the started iteration runs, else (status, itr, fx, gx0, ch)."""
+        done, it, fx, gx, ch = C.c_int(), C.c_int(), C.c_double(), C.c_double(), C.c_double()
+        rc = _check(lib().topo_opt_step_query(self.h, C.byref(done), C.byref(it), C.byref(fx), C.byref(gx),
+                                              C.byref(ch)), "opt_step_query")
+        return (rc, it.value, fx.value, gx.value, ch.value) if done.value else None
 
     def opt_run(self, max_itr):
         hist = np.zeros(3 * max_itr)

@@ -751,6 +751,7 @@ int topo_opt_step(topo_ctx* ctx, int* itr, double* fx, double* gx0, double* ch) 
     if (!ctx) { set_error("null context"); return TOPO_ERR_ARG; }
     GUARD_BEGIN
     Ctx& c = ctx->c;
+    if (c.sg.stage) { set_error("a design iteration of this context is still in flight"); return TOPO_ERR_ARG; }
     if (!c.opt_ready) TRET(opt_init(c));
     int rc = opt_step(c);
     TRET(rc);
@@ -765,6 +766,7 @@ int topo_opt_run(topo_ctx* ctx, int max_itr, double* hist, int* iterations) {
     if (!ctx) { set_error("null context"); return TOPO_ERR_ARG; }
     GUARD_BEGIN
     Ctx& c = ctx->c;
+    if (c.sg.stage) { set_error("a design iteration of this context is still in flight"); return TOPO_ERR_ARG; }
     if (!c.opt_ready) TRET(opt_init(c));
     int worst = 0, done = 0;
     const double tol = c.p.ch_tol;
@@ -792,26 +794,21 @@ int topo_opt_step_batch(topo_ctx* const* ctxs, int n, int* status, double* fx) {
     std::vector<char> replay(n, 0);
     for (int i = 0; i < n; i++) {
         Ctx& c = ctxs[i]->c;
+        if (c.sg.stage) {
+            set_error("a design iteration of context %d is still in flight", i);
+            rc[i] = TOPO_ERR_ARG;
+            continue;
+        }
         if (!c.opt_ready) rc[i] = opt_init(c);
         bool ok = false;
         if (rc[i] >= 0 && c.p.step_graph) rc[i] = opt_step_graph_prepare(c, &ok);
         replay[i] = rc[i] >= 0 && ok;
     }
-    // every replayed instance's three parts, with the cooperative dual solves
-    // (part 1) one after another across the instances
-    for (int part = 0; part < 3; part++) {
-        Ctx* prev = nullptr;
-        for (int i = 0; i < n; i++) {
-            if (!replay[i] || rc[i] < 0) continue;
-            Ctx& c = ctxs[i]->c;
-            if (part == 1 && prev) {
-                cudaError_t e = cudaStreamWaitEvent(c.s, prev->sg.mma_done, 0);
-                if (e != cudaSuccess) { rc[i] = cuda_fail(e, __FILE__, __LINE__); continue; }
-            }
-            rc[i] = opt_step_graph_part(c, part);
-            if (part == 1) prev = &c;
-        }
-    }
+    // every replayed instance's three parts (the cooperative dual solves of
+    // part 1 run one after another, opt_step_graph_part)
+    for (int part = 0; part < 3; part++)
+        for (int i = 0; i < n; i++)
+            if (replay[i] && rc[i] >= 0) rc[i] = opt_step_graph_part(ctxs[i]->c, part);
     for (int i = 0; i < n; i++)
         if (!replay[i] && rc[i] >= 0) rc[i] = opt_step(ctxs[i]->c);
     for (int i = 0; i < n; i++)
@@ -827,10 +824,71 @@ int topo_opt_step_batch(topo_ctx* const* ctxs, int n, int* status, double* fx) {
     GUARD_END
 }
 
+int topo_opt_step_async(topo_ctx* ctx) {
+    if (!ctx) { set_error("null context"); return TOPO_ERR_ARG; }
+    GUARD_BEGIN
+    Ctx& c = ctx->c;
+    if (c.sg.stage != 0) { set_error("a design iteration of this context is still in flight"); return TOPO_ERR_ARG; }
+    if (!c.opt_ready) TRET(opt_init(c));
+    bool ok = false;
+    if (c.p.step_graph) TRET(opt_step_graph_prepare(c, &ok));
+    if (ok) {
+        TRET(opt_step_graph_part(c, 0));
+        c.sg.stage = 1;
+        return 0;
+    }
+    const int rc = opt_step(c);  // a direct step: done when this returns
+    TRET(rc);
+    c.sg.direct_rc = rc;
+    c.sg.stage = 3;
+    return 0;
+    GUARD_END
+}
+
+int topo_opt_step_query(topo_ctx* ctx, int* done, int* itr, double* fx, double* gx0, double* ch) {
+    if (!ctx || !done) { set_error("null argument"); return TOPO_ERR_ARG; }
+    GUARD_BEGIN
+    Ctx& c = ctx->c;
+    *done = 0;
+    int rc = 0;
+    switch (c.sg.stage) {
+        case 0: set_error("no design iteration of this context was started"); return TOPO_ERR_ARG;
+        case 1: {  // the solve part: once it is done, the MMA update and the filter go
+            const cudaError_t e = cudaEventQuery(c.sg.p0_done);
+            if (e == cudaErrorNotReady) return 0;
+            if (e != cudaSuccess) { c.sg.stage = 0; return cuda_fail(e, __FILE__, __LINE__); }
+            rc = opt_step_graph_part(c, 1);
+            if (rc >= 0) rc = opt_step_graph_part(c, 2);
+            if (rc < 0) { c.sg.stage = 0; return rc; }
+            c.sg.stage = 2;
+            return 0;
+        }
+        case 2: {
+            const cudaError_t e = cudaEventQuery(c.sg.e1);
+            if (e == cudaErrorNotReady) return 0;
+            c.sg.stage = 0;
+            if (e != cudaSuccess) return cuda_fail(e, __FILE__, __LINE__);
+            rc = opt_step_graph_finish(c);
+            break;
+        }
+        default:
+            c.sg.stage = 0;
+            rc = c.sg.direct_rc;
+    }
+    *done = 1;
+    if (itr) *itr = c.itr;
+    if (fx) *fx = c.info.last_fx;
+    if (gx0) *gx0 = c.info.last_gx0;
+    if (ch) *ch = c.info.last_ch;
+    return rc;
+    GUARD_END
+}
+
 int topo_opt_step_host(topo_ctx* ctx, const double* x_in, double* x_out, double* xphys_out, double* fx) {
     if (!ctx || !x_in || !x_out || !xphys_out) { set_error("null argument"); return TOPO_ERR_ARG; }
     GUARD_BEGIN
     Ctx& c = ctx->c;
+    if (c.sg.stage) { set_error("a design iteration of this context is still in flight"); return TOPO_ERR_ARG; }
     if (!c.opt_ready) TRET(opt_init(c));
     TCK(cudaMemcpyAsync(c.X.p, x_in, sizeof(double) * c.ne, cudaMemcpyHostToDevice, c.s));
     int rc = opt_step(c);

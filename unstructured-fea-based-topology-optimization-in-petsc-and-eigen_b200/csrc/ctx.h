@@ -266,12 +266,15 @@ struct Ctx {
         int depth = 0;
         // three graphs: [0] solve, sensitivities, filtered sensitivities, move
         // limits; [1] the MMA update (its cooperative dual solve) and the design
-        // change; [2] filter, projection, results.  A batch of instances
-        // orders the instances' part-1 graphs one after another (the dual
-        // solve's grid barrier wants its blocks resident together).
+        // change; [2] filter, projection, results.  The part-1 graphs of all
+        // contexts of a process run one after another on each device (the
+        // dual solve's grid barrier wants its blocks resident together).
         cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
         long launches[3] = {0, 0, 0};    // kernels per replay (for the launch counter)
-        cudaEvent_t mma_done = nullptr;  // recorded after part 1 (batch ordering)
+        cudaEvent_t p0_done = nullptr;   // recorded after part 0
+        int stage = 0;                   // topo_opt_step_async: 0 idle, 1 part 0 in flight,
+                                         // 2 parts 1-2 in flight, 3 a direct step finished
+        int direct_rc = 0;               // its status
         uint64_t sig = 0;                // options and buffers the graphs were captured with
         bool disabled = false;           // capture failed: direct launches from then on
         bool state_dirty = true;         // host itr/beta changed since the device copies
@@ -288,7 +291,7 @@ struct Ctx {
             if (cap) cudaStreamDestroy(cap);
             for (auto b : body)
                 if (b) cudaStreamDestroy(b);
-            for (auto e : {e0, e1, mma_done})
+            for (auto e : {e0, e1, p0_done})
                 if (e) cudaEventDestroy(e);
         }
     } sg;

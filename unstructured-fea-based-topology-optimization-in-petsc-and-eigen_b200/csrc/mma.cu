@@ -480,9 +480,9 @@ static int update_m(Ctx& c, double* x, const double* dfdx, const double* gx_dev,
     // Co-residency: the grid barrier needs every block of the grid resident at
     // once.  A direct launch (one at a time per process, under coop_mutex)
     // leaves one block slot per SM free, and a launch from a replayed step
-    // graph (stepgraph.cu; one at a time per batch) takes at most one block
-    // per SM, so one of each can run side by side without either waiting on
-    // blocks that cannot start.
+    // graph (stepgraph.cu: one at a time per device and process, chained on an
+    // event) takes at most one block per SM, so one of each can run side by
+    // side without either waiting on blocks that cannot start.
     const int cap = c.sg.dd ? dev_sms : dev_sms * std::max(occ - 1, 1);
     int blocks = std::max(1, std::min(cap, std::min(2048, (n + 255) / 256)));
     MmaConst kc{};

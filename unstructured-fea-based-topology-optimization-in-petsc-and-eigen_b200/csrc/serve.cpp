@@ -13,11 +13,10 @@
 // Instance batching (topo_server_set_batching): admitted jobs up to a size
 // limit run their first design iteration on a thread of their own (it
 // allocates and tunes their context) and then join one batch worker, which
-// advances every job it holds by one design iteration per round with
-// topo_opt_step_batch: each job's iteration replayed from its step graph
-// (conditional nodes decide the solver loops on the device), all of them
-// launched before the worker waits once for the round.  Jobs join and leave
-// the batch between rounds.
+// keeps every job it holds going: each job's iterations are replayed from its
+// step graphs (conditional nodes decide the solver loops on the device) and
+// relaunched as soon as they are done, with no host thread per job and no
+// host round trip inside an iteration.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -283,57 +282,73 @@ static void prepare_job(topo_server* s, Job* j, Clock::time_point t0) {
     retire(s, j, rc, t0);
 }
 
-// Batched jobs, the rest: one design iteration of every held job per round.
+// Batched jobs, the rest: one host thread keeps every held job going.  Each
+// job's next design iteration is launched (topo_opt_step_async) as soon as its
+// previous one is done; the thread polls (topo_opt_step_query, which never
+// blocks and launches the second half of an iteration once its solve is
+// done), so no job waits for another and the host never waits on the device.
 static void batch_worker(topo_server* s, Clock::time_point t0) {
-    std::vector<std::pair<Job*, topo_ctx*>> held;
-    std::vector<topo_ctx*> ctxs;
-    std::vector<int> st;
-    std::vector<double> fx;
+    struct Held {
+        Job* j;
+        topo_ctx* ctx;
+        Clock::time_point start;
+        bool running;
+    };
+    std::vector<Held> held;
     while (true) {
         {
             std::unique_lock<std::mutex> lk(s->mu);
             while (s->ready.empty() && held.empty() && !(s->batch_quit && s->preparing == 0))
                 s->cv.wait_for(lk, std::chrono::milliseconds(50));
-            for (auto& r : s->ready) held.push_back(r);
+            for (auto& r : s->ready) held.push_back({r.first, r.second, Clock::now(), false});
             s->ready.clear();
             if (held.empty() && s->batch_quit && s->preparing == 0) return;
         }
-        // cancellations take effect between rounds
+        bool progressed = false;
         for (size_t i = 0; i < held.size();) {
-            Job* j = held[i].first;
-            if (j->cancel->load()) {
-                j->error = "cancelled";
-                topo_destroy(held[i].second);
-                retire(s, j, TOPO_ERR_CANCELLED, t0);
+            Held& h = held[i];
+            Job* j = h.j;
+            int rc = 0;
+            bool retire_now = false;
+            if (!h.running) {
+                if (j->cancel->load()) {  // cancellations take effect between iterations
+                    j->error = "cancelled";
+                    topo_destroy(h.ctx);
+                    retire(s, j, TOPO_ERR_CANCELLED, t0);
+                    held.erase(held.begin() + i);
+                    continue;
+                }
+                h.start = Clock::now();
+                rc = topo_opt_step_async(h.ctx);
+                if (rc < 0) {
+                    j->error = topo::last_error();
+                    retire_now = true;
+                } else {
+                    h.running = true;
+                }
+                progressed = true;
+            } else {
+                int done = 0;
+                double fx = 0.0;
+                rc = topo_opt_step_query(h.ctx, &done, nullptr, &fx, nullptr, nullptr);
+                if (rc < 0 || done) {
+                    j->iter_ms.push_back(std::chrono::duration<double, std::milli>(Clock::now() - h.start).count());
+                    j->fx_hist.push_back(fx);
+                    h.running = false;
+                    progressed = true;
+                    if (rc < 0) j->error = topo::last_error();
+                    retire_now = rc < 0 || (int)j->iter_ms.size() >= j->iterations;
+                }
+            }
+            if (retire_now) {
+                const int frc = finish_ctx(j, h.ctx, rc);
+                retire(s, j, frc, t0);
                 held.erase(held.begin() + i);
             } else {
                 i++;
             }
         }
-        if (held.empty()) continue;
-        ctxs.clear();
-        for (auto& h : held) ctxs.push_back(h.second);
-        st.assign(held.size(), 0);
-        fx.assign(held.size(), 0.0);
-        auto a = Clock::now();
-        topo_opt_step_batch(ctxs.data(), (int)ctxs.size(), st.data(), fx.data());
-        const double ms = std::chrono::duration<double, std::milli>(Clock::now() - a).count();
-        for (size_t i = 0; i < held.size();) {
-            Job* j = held[i].first;
-            j->iter_ms.push_back(ms);
-            j->fx_hist.push_back(fx[i]);
-            const bool done = (int)j->iter_ms.size() >= j->iterations;
-            if (st[i] < 0 || done) {
-                if (st[i] < 0) j->error = topo::last_error();
-                const int rc = finish_ctx(j, held[i].second, st[i]);
-                retire(s, j, rc, t0);
-                held.erase(held.begin() + i);
-                st.erase(st.begin() + i);
-                fx.erase(fx.begin() + i);
-            } else {
-                i++;
-            }
-        }
+        if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
 }
 

@@ -14,12 +14,15 @@
 //
 // Several contexts (independent design instances) are advanced together by
 // topo_opt_step_batch (abi.cu): every instance's graphs are launched on its
-// own stream before the host waits for any of them.
+// own stream before the host waits for any of them; topo_opt_step_async and
+// topo_opt_step_query let one host thread keep many instances going without
+// waiting on any.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "ctx.h"
 
@@ -226,7 +229,7 @@ static int capture_step(Ctx& c) {
     if (!G.e0) {
         TCK(cudaEventCreate(&G.e0));
         TCK(cudaEventCreate(&G.e1));
-        TCK(cudaEventCreateWithFlags(&G.mma_done, cudaEventDisableTiming));
+        TCK(cudaEventCreateWithFlags(&G.p0_done, cudaEventDisableTiming));
     }
     if (!G.out.p) TRET(G.out.alloc(kOut));
     for (int part = 0; part < 3; part++) {
@@ -281,13 +284,41 @@ int opt_step_graph_prepare(Ctx& c, bool* ok) {
     return 0;
 }
 
+// One event per device, recorded after every replayed part 1 (the MMA update
+// with its cooperative dual solve) of any context of this process: the next
+// part 1 waits on it, so at most one replayed dual solve runs on a device at a
+// time.  With its grid of one block per SM it fits beside the one direct
+// dual solve a process runs at a time (mma.cu), whatever the other kernels.
+constexpr int kMaxDevices = 64;
+static std::mutex& mma_chain_mutex() {
+    static std::mutex m;
+    return m;
+}
+static cudaEvent_t mma_chain_event[kMaxDevices];
+
 // launches part p of a prepared step on the context's stream
 int opt_step_graph_part(Ctx& c, int part) {
     Ctx::StepGraph& G = c.sg;
+    if (part == 1) {
+        int dev = 0;
+        TCK(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kMaxDevices) {
+            set_error("device index %d out of range", dev);
+            return TOPO_ERR_UNSUPPORTED;
+        }
+        std::lock_guard<std::mutex> lk(mma_chain_mutex());
+        cudaEvent_t& ev = mma_chain_event[dev];
+        if (!ev) TCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        TCK(cudaStreamWaitEvent(c.s, ev, 0));
+        TCK(cudaGraphLaunch(G.exec[1], c.s));
+        TCK(cudaEventRecord(ev, c.s));
+        __atomic_fetch_add(&launch_counter(), G.launches[1], __ATOMIC_RELAXED);
+        return 0;
+    }
     if (part == 0) TCK(cudaEventRecord(G.e0, c.s));
     TCK(cudaGraphLaunch(G.exec[part], c.s));
     __atomic_fetch_add(&launch_counter(), G.launches[part], __ATOMIC_RELAXED);
-    if (part == 1) TCK(cudaEventRecord(G.mma_done, c.s));
+    if (part == 0) TCK(cudaEventRecord(G.p0_done, c.s));
     if (part == 2) {
         TCK(cudaEventRecord(G.e1, c.s));
         c.itr++;
