@@ -239,8 +239,10 @@ static int finish_ctx(Job* j, topo_ctx* ctx, int rc) {
     return rc;
 }
 
-// Batched job, first part: context, first design iteration (direct: it
-// allocates and tunes), then the hand-over to the batch worker.
+// Batched job, first part: context, the first design iteration (direct: it
+// allocates and tunes) and the second (it captures the step graphs), then
+// the hand-over to the batch worker, so that no capture holds up the jobs
+// the worker is running.
 static void prepare_job(topo_server* s, Job* j, Clock::time_point t0) {
     topo_ctx* ctx = nullptr;
     j->p.step_graph = 1;
@@ -255,7 +257,7 @@ static void prepare_job(topo_server* s, Job* j, Clock::time_point t0) {
             rc = TOPO_ERR_CANCELLED;
             j->error = "cancelled";
         }
-        if (rc >= 0) {
+        for (int it = 0; rc >= 0 && it < 2 && it < j->iterations; it++) {
             auto a = Clock::now();
             double fx = 0.0;
             rc = topo_opt_step(ctx, nullptr, &fx, nullptr, nullptr);
