@@ -33,7 +33,12 @@ void cheb_coeffs(int deg, double* cr, double* cq);  // amg.cu
 // the row's matrix blocks are read once per thread group (broadcast).
 // MODE 0: y = A x; 1: y = b - A x; 2: Chebyshev step with x = d_old:
 // t = A d_old; r -= t; d_new = c1 d_old + c2 Dinv r; xo += d_new.
-template <class T, int KB, int MODE>
+// The slots of a row are taken in groups of U: the column ids of the next
+// group are fetched while the current group's values and neighbour runs are
+// gathered (one memory round trip per group instead of two), and with U > 1
+// all of a group's loads are issued before its arithmetic.  U (1 or 3) is
+// picked by the autotuner: U = 3 holds more registers.
+template <class T, int KB, int MODE, int U>
 __global__ void __launch_bounds__(256) k_sell_blk(int nrows, const int* __restrict__ sp, const int* __restrict__ sci,
                                                   const T* __restrict__ S, const T* __restrict__ x, T* __restrict__ y,
                                                   const T* __restrict__ b, T* __restrict__ r, T* __restrict__ xo,
@@ -54,22 +59,42 @@ __global__ void __launch_bounds__(256) k_sell_blk(int nrows, const int* __restri
     for (int q = 0; q < 3; q++)
 #pragma unroll
         for (int c = 0; c < CPT; c++) acc[q][c] = T(0);
-#pragma unroll 3
-    for (int k = 0; k < w; k++) {
-        const int j = __ldg(cp + 32 * k);
-        T xv[3][CPT];
+    int jn[U];
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            const uint4 t = __ldg(reinterpret_cast<const uint4*>(x + (3L * j + d) * KB + c0));
-            memcpy(xv[d], &t, 16);
+    for (int u = 0; u < U; u++) jn[u] = u < w ? __ldg(cp + 32 * u) : 0;
+    for (int k = 0; k < w; k += U) {
+        int jc[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) jc[u] = jn[u];
+#pragma unroll
+        for (int u = 0; u < U; u++) jn[u] = k + U + u < w ? __ldg(cp + 32 * (k + U + u)) : 0;
+        T xv[U][3][CPT], av[U][9];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (k + u < w) {
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const uint4 t = __ldg(reinterpret_cast<const uint4*>(x + (3L * jc[u] + d) * KB + c0));
+                    memcpy(xv[u][d], &t, 16);
+                }
+                sell_load9<T>(S, sb + k + u, lane, av[u]);
+            } else {
+#pragma unroll
+                for (int d = 0; d < 3; d++)
+#pragma unroll
+                    for (int c = 0; c < CPT; c++) xv[u][d][c] = T(0);
+#pragma unroll
+                for (int e = 0; e < 9; e++) av[u][e] = T(0);
+            }
         }
-        T av[9];
-        sell_load9<T>(S, sb + k, lane, av);
 #pragma unroll
-        for (int q = 0; q < 3; q++)
+        for (int u = 0; u < U; u++)
 #pragma unroll
-            for (int c = 0; c < CPT; c++)
-                acc[q][c] += av[3 * q] * xv[0][c] + av[3 * q + 1] * xv[1][c] + av[3 * q + 2] * xv[2][c];
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int c = 0; c < CPT; c++)
+                    acc[q][c] += av[u][3 * q] * xv[u][0][c] + av[u][3 * q + 1] * xv[u][1][c] +
+                                 av[u][3 * q + 2] * xv[u][2][c];
     }
 #pragma unroll
     for (int q = 0; q < 3; q++) {
@@ -289,6 +314,22 @@ static int sell_grid(int nrows) {
     return (int)((nt + 255) / 256);
 }
 
+// level-0 block sweep in the slot-group form picked by the autotuner
+template <class T, int KB, int MODE>
+static void launch_sell_blk(Ctx& c, const T* x, T* y, const T* b, T* r, T* xo, const T* dinv, const double* rho,
+                            double cr, double cq) {
+    const AmgDevLevel& D = c.dl[0];
+    const T* S = avals<T>(c).A0s.p;
+    const int grid = sell_grid<T, KB>(D.nnode);
+    if (c.tune.blk_sell_u == 3)
+        k_sell_blk<T, KB, MODE, 3><<<grid, 256, 0, c.s>>>(D.nnode, D.sell_ptr.p, D.sell_ci.p, S, x, y, b, r, xo,
+                                                          dinv, rho, cr, cq);
+    else
+        k_sell_blk<T, KB, MODE, 1><<<grid, 256, 0, c.s>>>(D.nnode, D.sell_ptr.p, D.sell_ci.p, S, x, y, b, r, xo,
+                                                          dinv, rho, cr, cq);
+    note_launch();
+}
+
 // level operator on block vectors: mode 0 y = A x, 1 y = b - A x
 template <class T, int KB>
 static int level_apply(Ctx& c, int l, const T* x, T* y, const T* b, int mode) {
@@ -298,14 +339,8 @@ static int level_apply(Ctx& c, int l, const T* x, T* y, const T* b, int mode) {
         cudaEvent_t e0;
         const bool rec = mode == 1;
         if (rec) prof_begin(c, PS_RES0, &e0);
-        const int grid = sell_grid<T, KB>(D.nnode);
-        if (mode == 0)
-            k_sell_blk<T, KB, 0><<<grid, 256, 0, c.s>>>(D.nnode, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, x, y, b, nullptr,
-                                                        nullptr, nullptr, nullptr, 0, 0);
-        else
-            k_sell_blk<T, KB, 1><<<grid, 256, 0, c.s>>>(D.nnode, D.sell_ptr.p, D.sell_ci.p, v.A0s.p, x, y, b, nullptr,
-                                                        nullptr, nullptr, nullptr, 0, 0);
-        note_launch();
+        if (mode == 0) launch_sell_blk<T, KB, 0>(c, x, y, b, nullptr, nullptr, nullptr, nullptr, 0, 0);
+        else launch_sell_blk<T, KB, 1>(c, x, y, b, nullptr, nullptr, nullptr, nullptr, 0, 0);
         if (rec) prof_end(c, PS_RES0, e0);
         TCK(cudaGetLastError());
         return 0;
@@ -334,10 +369,7 @@ static int smooth_blk(Ctx& c, int l, const T* b, T* x, bool zero_init) {
         if (l == 0) {
             cudaEvent_t e0;
             prof_begin(c, PS_CHEB0, &e0);
-            k_sell_blk<T, KB, 2><<<sell_grid<T, KB>(D.nnode), 256, 0, c.s>>>(D.nnode, D.sell_ptr.p, D.sell_ci.p,
-                                                                            v.A0s.p, dcur, dnxt, nullptr, w.r[l].p,
-                                                                            x, v.dinv[l].p, rho, cr[k], cq[k]),
-                note_launch();
+            launch_sell_blk<T, KB, 2>(c, dcur, dnxt, nullptr, w.r[l].p, x, v.dinv[l].p, rho, cr[k], cq[k]);
             prof_end(c, PS_CHEB0, e0);
         } else {
             TRET((level_apply<T, KB>(c, l, dcur, w.t[l].p, nullptr, 0)));
@@ -681,6 +713,40 @@ static int norms_blk(Ctx& c, const double* w, double* out) {
 
 // Autotuning of the block operator's CTAs per SM (1 or the occupancy
 // limit), timed on this context's operator at its first block solve.
+// the level-0 block sweep's slot-group form (1 or 3 slots per load group),
+// timed on the context's own operator (MODE 0 on scratch rows of the basis)
+template <class T, int KB>
+static int tune_sell_u(Ctx& c, cudaEvent_t e0, cudaEvent_t e1) {
+    if (!avals<T>(c).A0s.p) return 0;
+    const long nf = (long)c.ndof * KB;
+    const T* x = reinterpret_cast<const T*>(c.blk.V.p);
+    T* y = reinterpret_cast<T*>(c.blk.V.p + nf);
+    double best = 1e30;
+    int pick = 1;
+    for (int u : {1, 3}) {
+        c.tune.blk_sell_u = u;
+        double t = 1e30;
+        for (int rep = 0; rep < 3; rep++) {
+            TCK(cudaEventRecord(e0, c.s));
+            launch_sell_blk<T, KB, 0>(c, x, y, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0);
+            TCK(cudaEventRecord(e1, c.s));
+            TCK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            TCK(cudaEventElapsedTime(&ms, e0, e1));
+            t = std::min(t, (double)ms);
+        }
+        if (t < best) { best = t; pick = u; }
+    }
+    c.tune.blk_sell_u = pick;
+    return 0;
+}
+template <class T>
+static int tune_sell_u_kb(Ctx& c, cudaEvent_t e0, cudaEvent_t e1) {
+    if (c.blk.kb == 4) return tune_sell_u<T, 4>(c, e0, e1);
+    if (c.blk.kb == 8) return tune_sell_u<T, 8>(c, e0, e1);
+    return tune_sell_u<T, 16>(c, e0, e1);
+}
+
 int autotune_block(Ctx& c) {
     BlockState& B = c.blk;
     if (!c.p.autotune || c.tune.block_done || !B.V.p) return 0;
@@ -713,8 +779,10 @@ int autotune_block(Ctx& c) {
         }
         if (t < best) { best = t; pick = ctas; pick_st = cand / 10; }
     }
+    const int rc = c.p.precision == TOPO_PREC_MIXED ? tune_sell_u_kb<float>(c, e0, e1) : tune_sell_u_kb<double>(c, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    TRET(rc);
     c.tune.blk_ctas = pick;
     c.tune.blk_stages = pick_st;
     c.prof.on = prof;
@@ -800,7 +868,7 @@ static int fgmres_blk(Ctx& c, const double* b, double* x, int* its_out, int* sta
                        (uint64_t)(uintptr_t)B.bv32.x[0].p, (uint64_t)(uintptr_t)B.bv64.x[0].p,
                        (uint64_t)(uintptr_t)c.v32.A0s.p, (uint64_t)(uintptr_t)c.v64.A0s.p,
                        (uint64_t)(uintptr_t)c.cinv.p, (uint64_t)(uintptr_t)c.rho.p, (uint64_t)c.p.precision,
-                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.tune.blk_ctas, (uint64_t)c.tune.blk_stages, (uint64_t)KB, (uint64_t)nf})
+                       (uint64_t)m, (uint64_t)c.nlev, (uint64_t)c.p.cheb_degree, (uint64_t)c.p.cheb_degree_post, (uint64_t)c.p.cheb_degree_coarse, (uint64_t)c.tune.blk_ctas, (uint64_t)c.tune.blk_stages, (uint64_t)c.tune.blk_sell_u, (uint64_t)KB, (uint64_t)nf})
         sig = sig_mix(sig, v);
     StepGraphs& G = B.graphs;
     if (G.sig != sig) {

@@ -304,6 +304,7 @@ struct Ctx {
         int red_blocks = 1184;      // grid of the vector reductions / Gram-Schmidt sweeps
         int blk_ctas = 0;           // block operator CTAs per SM (0: occupancy limit)
         int blk_stages = 3;         // block operator Ke copies in flight per warp (2 or 3)
+        int blk_sell_u = 1;         // block level-0 sweep: slots per load group (1 or 3)
         int bsr_g[kMaxLevels] = {}; // lanes per block row of the level-l (>= 1) smoother/residual (0: by row length)
         bool single_done = false, block_done = false;
     } tune;
