@@ -435,7 +435,7 @@ def main():
         # the same design-iteration window as the GPU arm: W untimed warm-up
         # iterations, then K timed ones (iterations W+1 .. W+K); the cap only
         # guards against a much slower host than the one this was sized on
-        cap = float(os.environ.get("TOPO_REFERENCE_CAP_S", "1500"))
+        cap = float(os.environ.get("TOPO_REFERENCE_CAP_S", "600"))
         done, dt, cores = cpu_run(wl, args.steps, cap, warmup=args.warmup)
         val = done / dt
         line = {"metric": METRIC, "value": val, "unit": "design iters/s", "n_gpus": args.gpus, "steps": done,
