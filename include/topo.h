@@ -121,6 +121,8 @@ typedef struct topo_solve_info {
                               of AMG level l >= 1 (0: not tuned) */
     int step_graph;        /* last design iteration: 1 replayed from the step graph, 0 stepped
                               directly, -1 the capture failed (direct steps from then on) */
+    double t_capture_ms;   /* host time of the last capture of the step graphs (capture and
+                              instantiation; 0 before the first) */
 } topo_solve_info;
 
 /* ---------------------------------------------------------------- basics */

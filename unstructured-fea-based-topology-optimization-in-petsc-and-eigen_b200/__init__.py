@@ -62,7 +62,7 @@ class SolveInfo(C.Structure):
                 ("mma_inner_its", C.c_int), ("last_fx", C.c_double), ("last_gx0", C.c_double),
                 ("last_ch", C.c_double), ("t_fem_ms", C.c_double), ("t_filter_ms", C.c_double),
                 ("t_mma_ms", C.c_double), ("t_setup_ms", C.c_double), ("tuned", C.c_int * 4),
-                ("tuned_lanes", C.c_int * 8), ("step_graph", C.c_int)]
+                ("tuned_lanes", C.c_int * 8), ("step_graph", C.c_int), ("t_capture_ms", C.c_double)]
 
 
 class TopoError(RuntimeError):

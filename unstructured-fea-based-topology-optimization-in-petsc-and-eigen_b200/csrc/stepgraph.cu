@@ -19,6 +19,7 @@
 // waiting on any.
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -222,6 +223,7 @@ static int capture_part(Ctx& c, int part) {
 }
 
 static int capture_step(Ctx& c) {
+    const auto t0 = std::chrono::steady_clock::now();
     Ctx::StepGraph& G = c.sg;
     if (!G.cap) TCK(cudaStreamCreateWithFlags(&G.cap, cudaStreamNonBlocking));
     for (auto& b : G.body)
@@ -242,6 +244,7 @@ static int capture_step(Ctx& c) {
     }
     G.sig = step_sig(c);
     G.state_dirty = true;
+    c.info.t_capture_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return 0;
 }
 
