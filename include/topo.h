@@ -331,8 +331,9 @@ int topo_server_submit(topo_server* s, const topo_params* p, int nen, int n_node
  * on a thread of their own, then join one batch worker that keeps all of them
  * going from one host thread: each job's iterations are replayed from its
  * step graphs (topo_opt_step_async / topo_opt_step_query) and relaunched as
- * soon as they are done.  0 (default) runs every job on its own thread.  Call
- * before topo_server_run. */
+ * soon as they are done.  Batched jobs use the default launch shapes (no
+ * autotuning on the shared device).  0 (default) runs every job on its own
+ * thread.  Call before topo_server_run. */
 int topo_server_set_batching(topo_server* s, int max_elems);
 /* runs every submitted job to completion (real-time arrivals); blocks */
 int topo_server_run(topo_server* s);

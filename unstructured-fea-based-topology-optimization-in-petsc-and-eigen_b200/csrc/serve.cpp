@@ -246,6 +246,9 @@ static int finish_ctx(Job* j, topo_ctx* ctx, int rc) {
 static void prepare_job(topo_server* s, Job* j, Clock::time_point t0) {
     topo_ctx* ctx = nullptr;
     j->p.step_graph = 1;
+    // default launch shapes: timing candidate shapes on a device shared with
+    // the batch would measure the neighbours, and hold them up
+    j->p.autotune = 0;
     int rc = topo_create(&j->p, j->nen, j->nn, j->vertex.data(), j->ne, j->element.data(), (int)j->fixed.size(),
                          j->fixed.data(), j->ncases, j->case_ptr.data(), j->load_dofs.data(), j->load_vals.data(),
                          nullptr, &ctx);
