@@ -33,12 +33,12 @@ def run(T, mesh, n, **kw):
     return h, xp, its
 
 
-@pytest.mark.parametrize("prec,nen", [("fp64", 8), ("mixed", 8), ("mixed", 4)])
-def test_graph_step_matches_direct_step(T, cuda, prec, nen):
+@pytest.mark.parametrize("prec,nen,tune", [("fp64", 8, 1), ("mixed", 8, 1), ("mixed", 4, 1), ("mixed", 8, 0)])
+def test_graph_step_matches_direct_step(T, cuda, prec, nen, tune):
     mesh = T.gen_cantilever(40, 20, 10, 8) if nen == 8 else T.gen_cantilever(12, 6, 6, 4)
     pr = T.PREC_MIXED if prec == "mixed" else T.PREC_FP64
-    hd, xd, _ = run(T, mesh, 12, precision=pr, step_graph=0)
-    hg, xg, its = run(T, mesh, 12, precision=pr, step_graph=1)
+    hd, xd, _ = run(T, mesh, 12, precision=pr, step_graph=0, autotune=tune)
+    hg, xg, its = run(T, mesh, 12, precision=pr, step_graph=1, autotune=tune)
     assert its > 0
     assert rel(hg[:, 0], hd[:, 0]) < 1e-6
     assert np.abs(hg[:, 1] - hd[:, 1]).max() < 1e-9

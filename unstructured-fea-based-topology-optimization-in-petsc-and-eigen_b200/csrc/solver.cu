@@ -520,7 +520,8 @@ static int fgmres_dd(Ctx& c, const double* b, double* x) {
     const GmLayout GL{m};
     const long ldv = (n + 31) & ~31L;
     const bool mixed = c.p.precision == TOPO_PREC_MIXED;
-    if (!c.V.p || (long)c.V.n < (long)(m + 1) * ldv || (mixed ? !c.Z32.p : !c.Z64.p) || !c.tune.single_done) {
+    if (!c.V.p || (long)c.V.n < (long)(m + 1) * ldv || (mixed ? !c.Z32.p : !c.Z64.p) ||
+        (c.p.autotune && !c.tune.single_done)) {
         set_error("the device-driven step needs a direct solve of this form first");
         return TOPO_ERR_ARG;
     }
