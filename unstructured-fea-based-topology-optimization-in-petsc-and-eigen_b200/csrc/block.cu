@@ -436,10 +436,17 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
                     if (dof < ND) {
                         const int comp = dof / NEN;
                         if (MODE == 0) {
-                            double* yp = yl + (size_t)mc.dn[mt] * NVL + comp * KB;
-#pragma unroll
-                            for (int i = 0; i < 2; i++)
-                                if (n0 + i < KB) yp[n0 + i] += sc * acc[mt][i];
+                            // the lane's two cases are one aligned 16-byte pair: n0 is even, the
+                            // node and component offsets are multiples of KB >= 4 doubles, and
+                            // the image starts 8 * ST * NPK doubles (a multiple of 16 bytes)
+                            // after the 128-byte aligned element-matrix ring
+                            if (n0 < KB) {
+                                double2* yp = reinterpret_cast<double2*>(yl + (size_t)mc.dn[mt] * NVL + comp * KB + n0);
+                                double2 cur = *yp;
+                                cur.x += sc * acc[mt][0];
+                                cur.y += sc * acc[mt][1];
+                                *yp = cur;
+                            }
                         } else {
 #pragma unroll
                             for (int i = 0; i < 2; i++)
