@@ -287,12 +287,32 @@ static void prepare_job(topo_server* s, Job* j, Clock::time_point t0) {
     retire(s, j, rc, t0);
 }
 
+// A batched job that is done: its final design is read back and its context
+// destroyed on a thread of its own, so that the frees (each of which waits
+// for the device) hold up no job the batch worker is running.
+static void finish_batched(topo_server* s, Job* j, topo_ctx* ctx, int rc, Clock::time_point t0) {
+    if (rc == TOPO_ERR_CANCELLED) {
+        topo_destroy(ctx);
+    } else {
+        rc = finish_ctx(j, ctx, rc);
+    }
+    retire(s, j, rc, t0);
+}
+
 // Batched jobs, the rest: one host thread keeps every held job going.  Each
 // job's next design iteration is launched (topo_opt_step_async) as soon as its
 // previous one is done; the thread polls (topo_opt_step_query, which never
 // blocks and launches the second half of an iteration once its solve is
 // done), so no job waits for another and the host never waits on the device.
 static void batch_worker(topo_server* s, Clock::time_point t0) {
+    std::vector<std::thread> reapers;
+    auto finish = [&](Job* j, topo_ctx* ctx, int rc) {
+        try {
+            reapers.emplace_back(finish_batched, s, j, ctx, rc, t0);
+        } catch (...) {
+            finish_batched(s, j, ctx, rc, t0);  // no thread: finish here
+        }
+    };
     struct Held {
         Job* j;
         topo_ctx* ctx;
@@ -307,7 +327,7 @@ static void batch_worker(topo_server* s, Clock::time_point t0) {
                 s->cv.wait_for(lk, std::chrono::milliseconds(50));
             for (auto& r : s->ready) held.push_back({r.first, r.second, Clock::now(), false});
             s->ready.clear();
-            if (held.empty() && s->batch_quit && s->preparing == 0) return;
+            if (held.empty() && s->batch_quit && s->preparing == 0) break;
         }
         bool progressed = false;
         for (size_t i = 0; i < held.size();) {
@@ -318,8 +338,7 @@ static void batch_worker(topo_server* s, Clock::time_point t0) {
             if (!h.running) {
                 if (j->cancel->load()) {  // cancellations take effect between iterations
                     j->error = "cancelled";
-                    topo_destroy(h.ctx);
-                    retire(s, j, TOPO_ERR_CANCELLED, t0);
+                    finish(j, h.ctx, TOPO_ERR_CANCELLED);
                     held.erase(held.begin() + i);
                     continue;
                 }
@@ -346,8 +365,7 @@ static void batch_worker(topo_server* s, Clock::time_point t0) {
                 }
             }
             if (retire_now) {
-                const int frc = finish_ctx(j, h.ctx, rc);
-                retire(s, j, frc, t0);
+                finish(j, h.ctx, rc);
                 held.erase(held.begin() + i);
             } else {
                 i++;
@@ -355,6 +373,7 @@ static void batch_worker(topo_server* s, Clock::time_point t0) {
         }
         if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
+    for (auto& t : reapers) t.join();
 }
 
 int topo_server_set_batching(topo_server* s, int max_elems) {
