@@ -378,6 +378,71 @@ def run_tet4(T, torch, stream, steps, warmup, cpu_steps):
     return out
 
 
+def run_instances(T, steps=10, warmup=3, specs=None):
+    """Independent design instances advanced together: eight hex8 cantilevers
+    of 12k to 48k elements (mixed and FP64, volume fractions 0.12 to 0.3).
+    Three ways to step them, each W untimed + K timed iterations of every
+    instance from a fresh start (host wall clock around each iteration of
+    all instances, which ends with their results on the host):
+    - batch_graph: topo_opt_step_batch, all iterations one graph launch;
+    - async_streams: topo_opt_step_async / _query from one thread, every
+      instance's own graphs on its own stream;
+    - one_by_one: topo_opt_step on each instance in turn (its own graphs).
+    The metric is instance design iterations per second."""
+    import time
+    import numpy as np
+    specs = specs or [((40, 20, 15), 0.12, 1), ((48, 24, 16), 0.2, 1), ((30, 20, 20), 0.15, 0),
+                      ((60, 20, 10), 0.3, 1), ((36, 18, 18), 0.25, 1), ((32, 16, 24), 0.12, 0),
+                      ((44, 22, 12), 0.18, 1), ((50, 25, 8), 0.22, 1)]
+    meshes = [T.gen_cantilever(*d, 8) for d, _, _ in specs]
+    out = {"workload": f"{len(specs)} hex8 cantilever instances, "
+                       f"{min(m[1].shape[0] for m in meshes)}-{max(m[1].shape[0] for m in meshes)} elements",
+           "steps": steps, "warmup": warmup, "timing": "host wall clock per iteration of all instances"}
+    hist = {}
+    for form in ("batch_graph", "async_streams", "one_by_one"):
+        ctxs = [T.Context(*m, stream="own", **dict(PARAMS, volfrac=vf, precision=pr))
+                for m, (_, vf, pr) in zip(meshes, specs)]
+        for c in ctxs:
+            c.opt_init()
+        fx_all, t = [], 0.0
+        launches0 = 0
+        for it in range(warmup + steps):
+            if it == warmup:
+                launches0 = T.kernel_launches()
+            t0 = time.perf_counter()
+            if form == "batch_graph":
+                st, fx = T.opt_step_batch(ctxs)
+                assert np.all(st >= 0), st
+            elif form == "one_by_one":
+                fx = [c.opt_step()[1] for c in ctxs]
+            else:
+                for c in ctxs:
+                    c.opt_step_async()
+                fx, left = [None] * len(ctxs), set(range(len(ctxs)))
+                while left:
+                    for k in list(left):
+                        r = ctxs[k].opt_step_query()
+                        if r is not None:
+                            fx[k] = r[2]
+                            left.discard(k)
+            dt = time.perf_counter() - t0
+            if it >= warmup:
+                t += dt
+            fx_all.append(list(fx))
+        out[form] = {"value": len(ctxs) * steps / t, "unit": "instance design iters/s",
+                     "ms_per_iteration_of_all": 1e3 * t / steps,
+                     "gpu_launches": T.kernel_launches() - launches0,
+                     "step_graph": ctxs[0].info().step_graph}
+        hist[form] = np.array(fx_all)
+        for c in ctxs:
+            c.close()
+    out["batch_over_one_by_one"] = out["batch_graph"]["value"] / out["one_by_one"]["value"]
+    out["batch_over_async_streams"] = out["batch_graph"]["value"] / out["async_streams"]["value"]
+    out["max_rel_compliance_diff_vs_one_by_one"] = float(
+        np.max(np.abs(hist["batch_graph"] - hist["one_by_one"]) / np.abs(hist["one_by_one"])))
+    return out
+
+
 def kmv_bytes(ctx, u_bytes):
     """Algorithmic bytes of one element-operator launch: per element the 8
     connectivity ids, the fixed mask, E_e and the 300 packed FP64 Ke entries;
@@ -405,12 +470,13 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving stream (p50/p99 latency)")
     ap.add_argument("--serve-jobs", type=int, default=12)
-    ap.add_argument("--only", choices=["mixed", "fp64", "multiload", "tet4", "serve"], default=None,
+    ap.add_argument("--only", choices=["mixed", "fp64", "multiload", "tet4", "serve", "instances"], default=None,
                     help="time one form only (used for short profiling runs)")
     ap.add_argument("--no-multiload", action="store_true", help="skip the k=8 multi-load configuration")
     ap.add_argument("--multiload-steps", type=int, default=6)
     ap.add_argument("--multiload-forms", default="block_mixed,block_fp64,one_by_one_mixed")
     ap.add_argument("--no-tet4", action="store_true", help="skip the tet4 2.35M configuration")
+    ap.add_argument("--no-instances", action="store_true", help="skip the batch of design instances")
     ap.add_argument("--tet4-steps", type=int, default=4)
     ap.add_argument("--tet4-cpu-steps", type=int, default=1)
     ap.add_argument("--param", action="append", default=[],
@@ -472,6 +538,11 @@ def main():
                               "serve": run_serving(T, args.serve_jobs, seed=7, batch_max_elems=BATCH_MAX_ELEMS),
                               "serve_unbatched": run_serving(T, args.serve_jobs, seed=7),
                               "serve_small_jobs": serve_small_jobs(T)}), flush=True)
+        return
+    if args.only == "instances":
+        if rank == 0:
+            print(json.dumps({"only": "instances", **run_instances(T, max(args.steps, 3), max(args.warmup, 3))}),
+                  flush=True)
         return
     if args.only == "multiload":
         if rank == 0:
@@ -575,6 +646,9 @@ def main():
         serve = run_serving(T, args.serve_jobs, seed=7, batch_max_elems=BATCH_MAX_ELEMS)
         serve_unbatched = run_serving(T, args.serve_jobs, seed=7, batch_max_elems=0)
         serve_small = serve_small_jobs(T)
+    inst = None
+    if not args.no_instances and rank == 0 and world == 1:
+        inst = run_instances(T)
     tet4 = None
     if not args.no_tet4 and rank == 0 and world == 1:
         tet4 = run_tet4(T, torch, stream, args.tet4_steps, 2, 0 if args.no_cpu_baseline else args.tet4_cpu_steps)
@@ -598,7 +672,7 @@ def main():
             "e2e": {"value": e2e_val, "unit": "design iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "clocks": clocks, "cpu_baseline": cpu,
             "fgmres_initial_guess": "previous design iteration's U (warm start); stopping rule unchanged",
-            "multiload": multi, "tet4": tet4, "serve_small_jobs": serve_small, "serve_unbatched": serve_unbatched,
+            "multiload": multi, "tet4": tet4, "instances": inst, "serve_small_jobs": serve_small, "serve_unbatched": serve_unbatched,
             "serve": serve, "kernels": kern,
             "fgmres_its_per_step": {"mixed_warm": its, "mixed_zero_start": itsz, "fp64": its64, "fp64_warm": its64w,
                                     "mixed_fp16_fine": its16},

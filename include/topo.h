@@ -119,10 +119,12 @@ typedef struct topo_solve_info {
                               copies in flight per warp + CTAs per SM, 0: occupancy limit) */
     int tuned_lanes[8];    /* lanes per block row picked for the smoothing and residual products
                               of AMG level l >= 1 (0: not tuned) */
-    int step_graph;        /* last design iteration: 1 replayed from the step graph, 0 stepped
+    int step_graph;        /* last design iteration: 1 replayed from the step graph, 2 replayed as
+                              a branch of a batch graph (topo_opt_step_batch), 0 stepped
                               directly, -1 the capture failed (direct steps from then on) */
     double t_capture_ms;   /* host time of the last capture of the step graphs (capture and
-                              instantiation; 0 before the first) */
+                              instantiation; 0 before the first); of the whole batch graph when
+                              that was captured last */
 } topo_solve_info;
 
 /* ---------------------------------------------------------------- basics */
@@ -270,14 +272,17 @@ int topo_opt_run(topo_ctx* ctx, int max_itr, double* hist, int* iterations);
 /* Advances n independent contexts (design instances) by one design iteration
  * each (no counterpart in the reference, which runs one design per MPI job).
  * Instances whose options select step_graph = 1 and that have done their first
- * iteration are replayed from their step graphs: all of them are launched,
- * each on its own context stream, before the host waits for any, so their
- * iterations overlap on the device (the cooperative MMA dual solves of a
- * process run one after another on a device); the other instances step
- * directly, after those launches.
+ * iteration are replayed: two or more of them as ONE graph launch in which
+ * each instance's iteration is a branch of its own, so their iterations
+ * overlap on the device (the cooperative MMA dual solves run one after
+ * another).  That batch graph is captured at the first call with a given
+ * ordered set of instances and reused while the set and the instances'
+ * options and buffers stay the same (the last few sets are kept).  Should its
+ * capture fail, every instance's own step graphs are launched on its stream
+ * instead.  The other instances step directly, after that launch.
  * status[i] (may be NULL) receives each instance's status, fx[i] (may be NULL)
  * its compliance.  Returns the most severe status: the first error (< 0)
- * met, else the largest warning.  Contexts that share a stream serialise. */
+ * met, else the largest warning. */
 int topo_opt_step_batch(topo_ctx* const* ctxs, int n, int* status, double* fx);
 /* One design iteration without waiting for it (no counterpart in the
  * reference).  With step_graph = 1 and a replayable step, topo_opt_step_async

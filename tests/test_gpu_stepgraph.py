@@ -116,14 +116,64 @@ def test_batch_of_instances_equals_solo_runs(T, cuda):
         c.opt_init()
         ctxs.append(c)
     hist = np.zeros((n, len(ctxs)))
+    caps = []
     for it in range(n):
         st, fx = T.opt_step_batch(ctxs)
         assert np.all(st == 0), st
         hist[it] = fx
+        caps.append(ctxs[0].info().t_capture_ms)
     for k in range(len(ctxs)):
         assert rel(hist[:, k], solo[k]) < 1e-6, k
-        assert ctxs[k].info().fem_its > 0 and ctxs[k].info().step_graph == 1
+        # replayed as a branch of the one batch graph
+        assert ctxs[k].info().fem_its > 0 and ctxs[k].info().step_graph == 2
+    # the batch graph is captured once (second call) and then reused
+    assert caps[1] > 0 and all(c == caps[1] for c in caps[2:])
     for c in ctxs:
+        c.close()
+
+
+def test_batch_graph_follows_set_and_options(T, cuda):
+    """The batch graph is keyed by the ordered set of instances and by their
+    own captures: a smaller set, an instance with new options (an iteration
+    cap) and a destroyed instance each lead to a graph of their own, and the
+    trajectories still equal the solo runs."""
+    specs = [((20, 10, 6, 8), dict(volfrac=0.12)), ((12, 6, 6, 4), dict(volfrac=0.2, rmin=1.3)),
+             ((16, 8, 8, 8), dict(volfrac=0.25, precision=1))]
+    n = 9
+    solo = [run(T, T.gen_cantilever(*d), n, step_graph=0, **kw)[0][:, 0] for d, kw in specs]
+    ctxs = [T.Context(*T.gen_cantilever(*d), stream="own", step_graph=1, **dict(KW, **kw)) for d, kw in specs]
+    for c in ctxs:
+        c.opt_init()
+    hist = [[] for _ in ctxs]
+
+    def step(ks):
+        st, fx = T.opt_step_batch([ctxs[k] for k in ks])
+        for j, k in enumerate(ks):
+            hist[k].append(fx[j])
+        return st
+
+    for _ in range(3):
+        assert np.all(step([0, 1, 2]) == 0)
+    for _ in range(2):                      # a subset, in another order
+        assert np.all(step([2, 0]) == 0)
+    assert ctxs[0].info().step_graph == 2
+    step([1])                               # alone: its own graphs
+    step([1])
+    assert ctxs[1].info().step_graph == 1
+    # an iteration cap on one instance: its graphs and the batch graph are
+    # captured again; the cap shows in its status only
+    ctxs[2].set_params(fem_maxit=2)
+    st = step([0, 1, 2])
+    assert st[2] == T.TOPO_NOT_CONVERGED and st[0] == 0 and st[1] == 0
+    assert ctxs[2].info().fem_its == 2 and ctxs[2].info().step_graph == 2
+    ctxs[2].close()                         # destroyed: batch graphs naming it go
+    for _ in range(2):
+        assert np.all(step([0, 1]) == 0)
+    assert len(hist[0]) == n - 1 and len(hist[1]) == n - 1
+    for k in (0, 1):
+        assert rel(np.array(hist[k]), solo[k][: n - 1]) < 1e-6, k
+    assert rel(np.array(hist[2][:5]), solo[2][:5]) < 1e-6
+    for c in ctxs[:2]:
         c.close()
 
 

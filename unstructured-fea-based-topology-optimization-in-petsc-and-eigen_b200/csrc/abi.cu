@@ -463,6 +463,7 @@ int topo_create(const topo_params* p, int nen, int n_nodes, const double* vertex
 int topo_destroy(topo_ctx* ctx) {
     if (!ctx) return 0;
     cudaStreamSynchronize(ctx->c.s);
+    step_batch_forget(&ctx->c);
     cudaGetLastError();
     for (int i = 0; i < 4; i++)
         if (ctx->c.ev[i]) cudaEventDestroy(ctx->c.ev[i]);
@@ -804,11 +805,22 @@ int topo_opt_step_batch(topo_ctx* const* ctxs, int n, int* status, double* fx) {
         if (rc[i] >= 0 && c.p.step_graph) rc[i] = opt_step_graph_prepare(c, &ok);
         replay[i] = rc[i] >= 0 && ok;
     }
-    // every replayed instance's three parts (the cooperative dual solves of
-    // part 1 run one after another, opt_step_graph_part)
-    for (int part = 0; part < 3; part++)
+    // the replayed instances' iterations as one graph launch, or, without a
+    // batch graph, every instance's own three graphs on its own stream (the
+    // cooperative dual solves of part 1 run one after another either way)
+    std::vector<Ctx*> rs;
+    for (int i = 0; i < n; i++)
+        if (replay[i] && rc[i] >= 0) rs.push_back(&ctxs[i]->c);
+    bool one = false;
+    const int brc = opt_step_graph_batch(rs.data(), (int)rs.size(), &one);
+    if (brc < 0) {
         for (int i = 0; i < n; i++)
-            if (replay[i] && rc[i] >= 0) rc[i] = opt_step_graph_part(ctxs[i]->c, part);
+            if (replay[i] && rc[i] >= 0) rc[i] = brc;
+    }
+    if (!one)
+        for (int part = 0; part < 3; part++)
+            for (int i = 0; i < n; i++)
+                if (replay[i] && rc[i] >= 0) rc[i] = opt_step_graph_part(ctxs[i]->c, part);
     for (int i = 0; i < n; i++)
         if (!replay[i] && rc[i] >= 0) rc[i] = opt_step(ctxs[i]->c);
     for (int i = 0; i < n; i++)

@@ -264,6 +264,7 @@ struct Ctx {
         cudaStream_t cap = nullptr;      // top-level capture stream
         cudaStream_t body[4] = {};       // capture streams of nested conditional bodies
         int depth = 0;
+        int coop_blocks = 0;             // capturing: cap on the dual solve's grid (0: one block per SM)
         // three graphs: [0] solve, sensitivities, filtered sensitivities, move
         // limits; [1] the MMA update (its cooperative dual solve) and the design
         // change; [2] filter, projection, results.  The part-1 graphs of all
@@ -276,6 +277,7 @@ struct Ctx {
                                          // 2 parts 1-2 in flight, 3 a direct step finished
         int direct_rc = 0;               // its status
         uint64_t sig = 0;                // options and buffers the graphs were captured with
+        uint64_t gen = 0;                // capture number (process-wide; batch graphs follow it)
         bool disabled = false;           // capture failed: direct launches from then on
         bool state_dirty = true;         // host itr/beta changed since the device copies
         DBuf<double> out;                // collected per-step results (read once per step)
@@ -405,6 +407,8 @@ int cond_handle(Ctx& c, cudaGraphConditionalHandle* h);  // handle on the graph 
 int opt_step_graph_prepare(Ctx& c, bool* ok);
 int opt_step_graph_part(Ctx& c, int part);
 int opt_step_graph_finish(Ctx& c);
+int opt_step_graph_batch(Ctx* const* cs, int n, bool* launched);
+void step_batch_forget(const Ctx* c);
 
 int mma_alloc(Ctx& c);                                             // mma.cu
 int mma_movelimit(Ctx& c, double Xmin, double Xmax, double movlim, const double* x, double* xmin, double* xmax);

@@ -479,11 +479,15 @@ static int update_m(Ctx& c, double* x, const double* dfdx, const double* gx_dev,
     TCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solvedip<M>, 256, 0));
     // Co-residency: the grid barrier needs every block of the grid resident at
     // once.  A direct launch (one at a time per process, under coop_mutex)
-    // leaves one block slot per SM free, and a launch from a replayed step
-    // graph (stepgraph.cu: one at a time per device and process, chained on an
-    // event) takes at most one block per SM, so one of each can run side by
-    // side without either waiting on blocks that cannot start.
-    const int cap = c.sg.dd ? dev_sms : dev_sms * std::max(occ - 1, 1);
+    // leaves one block slot per SM free, and the launches from replayed step
+    // graphs that can run at once take at most one block per SM together
+    // (stepgraph.cu: a context's own part-1 graphs run one at a time per device
+    // and process, chained on an event; inside a batch graph every instance's
+    // grid is capped at its share, coop_blocks), so the direct and the graph
+    // grids can run side by side without any waiting on blocks that cannot
+    // start.
+    const int cap = c.sg.dd ? (c.sg.coop_blocks > 0 ? std::min(c.sg.coop_blocks, dev_sms) : dev_sms)
+                            : dev_sms * std::max(occ - 1, 1);
     int blocks = std::max(1, std::min(cap, std::min(2048, (n + 255) / 256)));
     MmaConst kc{};
     for (int j = 0; j < M; j++) { kc.a[j] = c.a[j]; kc.c[j] = c.c[j]; kc.d[j] = c.d[j]; }

@@ -13,17 +13,21 @@
 // step to rounding.
 //
 // Several contexts (independent design instances) are advanced together by
-// topo_opt_step_batch (abi.cu): every instance's graphs are launched on its
-// own stream before the host waits for any of them; topo_opt_step_async and
-// topo_opt_step_query let one host thread keep many instances going without
-// waiting on any.
+// topo_opt_step_batch (abi.cu): the iterations of all replayable instances
+// are one graph launch (opt_step_graph_batch below), each instance a branch
+// of that graph; topo_opt_step_async and topo_opt_step_query let one host
+// thread keep many instances going without waiting on any.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
+#include <vector>
 
 #include "ctx.h"
 
@@ -242,7 +246,9 @@ static int capture_step(Ctx& c) {
             return rc;
         }
     }
+    static std::atomic<uint64_t> n_captures{0};
     G.sig = step_sig(c);
+    G.gen = ++n_captures;
     G.state_dirty = true;
     c.info.t_capture_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return 0;
@@ -366,6 +372,208 @@ int opt_step_graph_finish(Ctx& c) {
         return TOPO_ERR_TIMEOUT;
     }
     return (c.info.fem_status || cg_status) ? TOPO_NOT_CONVERGED : 0;
+}
+
+// ----------------------------------------------------------------- one graph for a batch of instances
+// topo_opt_step_batch with two or more replayable instances launches a single
+// graph for all of them.  Each instance's three parts are captured as a branch
+// of their own (the branches' kernels overlap on the device), and every
+// branch ends with its instance's result copy.  The cooperative dual solves
+// (part 1) share one block per SM, as a single replayed part 1 would take:
+// with S = min(n, SMs) slots, each instance's grid is capped at SMs / S blocks
+// and instance i's part 1 waits for instance i - S's (no waits while n <= SMs).
+// The batch graph itself waits on, and records, the per-device part-1 event,
+// so no other replayed dual solve runs beside it.  A batch graph is captured
+// once per ordered set of instances and kept while none of them recaptures
+// its own graphs (StepGraph::gen) or is destroyed.
+struct BatchGraph {
+    std::vector<Ctx*> ctxs;
+    std::vector<uint64_t> gens;
+    cudaGraphExec_t exec = nullptr;
+    bool failed = false;              // capture failed: these instances use their own graphs
+    long launches = 0;                // kernels per replay
+    cudaStream_t s = nullptr;         // launch (and capture origin) stream
+    cudaEvent_t ev = nullptr;
+    std::vector<cudaEvent_t> slot;    // part-1 slots (instances beyond the SM count)
+    void drop() {
+        if (s) cudaStreamSynchronize(s);
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+    }
+    ~BatchGraph() {
+        drop();
+        if (s) cudaStreamDestroy(s);
+        if (ev) cudaEventDestroy(ev);
+        for (auto e : slot) cudaEventDestroy(e);
+    }
+};
+constexpr size_t kMaxBatchGraphs = 4;  // sets of instances kept at once (least recently used goes)
+static std::mutex& batch_mutex() {
+    static std::mutex m;
+    return m;
+}
+// never destroyed: CUDA objects must not be released after the runtime shut down
+static std::vector<std::unique_ptr<BatchGraph>>& batch_cache() {
+    static auto* v = new std::vector<std::unique_ptr<BatchGraph>>();
+    return *v;
+}
+
+static int capture_batch(BatchGraph& B) {
+    const auto t0 = std::chrono::steady_clock::now();
+    if (!B.s) TCK(cudaStreamCreateWithFlags(&B.s, cudaStreamNonBlocking));
+    if (!B.ev) TCK(cudaEventCreateWithFlags(&B.ev, cudaEventDisableTiming));
+    int dev = 0, nsm = 0;
+    TCK(cudaGetDevice(&dev));
+    TCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int n_inst = (int)B.ctxs.size();
+    const int n_slot = std::max(1, std::min(n_inst, nsm));
+    const int share = std::max(1, nsm / n_slot);  // dual-solve blocks per instance
+    while ((int)B.slot.size() < n_slot && n_inst > n_slot) {
+        cudaEvent_t e;
+        TCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        B.slot.push_back(e);
+    }
+    const long l0 = launch_counter();
+    int rc = 0;
+    cudaError_t e = cudaStreamBeginCapture(B.s, cudaStreamCaptureModeThreadLocal);
+    const bool begun = e == cudaSuccess;
+    if (begun) e = cudaEventRecord(B.ev, B.s);
+    size_t joined = 0;  // branches whose capture stream joined this capture
+    for (size_t i = 0; i < B.ctxs.size() && e == cudaSuccess && rc >= 0; i++) {
+        Ctx& c = *B.ctxs[i];
+        const cudaStream_t s0 = c.s;
+        const bool prof = c.prof.on;
+        c.prof.on = false;
+        c.s = c.sg.cap;
+        c.sg.dd = true;
+        c.sg.depth = 0;
+        c.sg.coop_blocks = share;
+        const bool slotted = n_inst > n_slot;
+        cudaEvent_t slot_ev = slotted ? B.slot[i % n_slot] : nullptr;
+        e = cudaStreamWaitEvent(c.s, B.ev, 0);  // the branch forks off the origin stream
+        if (e == cudaSuccess) {
+            joined++;
+            rc = step_part(c, 0);
+            if (rc >= 0 && slotted && (int)i >= n_slot) e = cudaStreamWaitEvent(c.s, slot_ev, 0);
+            if (rc >= 0 && e == cudaSuccess) rc = step_part(c, 1);
+            if (rc >= 0 && e == cudaSuccess && slotted) e = cudaEventRecord(slot_ev, c.s);
+            if (rc >= 0 && e == cudaSuccess) rc = step_part(c, 2);
+        }
+        while (c.sg.depth > 0) {  // nested captures left open by an error
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(c.sg.body[c.sg.depth - 1], &g);
+            c.sg.depth--;
+        }
+        c.sg.dd = false;
+        c.sg.coop_blocks = 0;
+        c.s = s0;
+        c.prof.on = prof;
+    }
+    // every branch joins the origin stream again (also after an error, so that
+    // the capture ends cleanly)
+    for (size_t i = 0; i < joined; i++) {
+        const cudaError_t r1 = cudaEventRecord(B.ev, B.ctxs[i]->sg.cap);
+        const cudaError_t r2 = cudaStreamWaitEvent(B.s, B.ev, 0);
+        if (e == cudaSuccess) e = r1 != cudaSuccess ? r1 : r2;
+    }
+    cudaGraph_t g = nullptr;
+    if (begun) {
+        const cudaError_t r = cudaStreamEndCapture(B.s, &g);
+        if (e == cudaSuccess) e = r;
+    }
+    const long n = launch_counter() - l0;
+    __atomic_fetch_sub(&launch_counter(), n, __ATOMIC_RELAXED);  // nothing ran yet
+    if (rc >= 0 && e == cudaSuccess && g) e = cudaGraphInstantiate(&B.exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (rc < 0 || e != cudaSuccess || !B.exec) {
+        const char* why = e != cudaSuccess ? cudaGetErrorString(e) : last_error();
+        cudaGetLastError();
+        set_error("batch graph capture failed (%s); the instances' own graphs from now on", why);
+        if (B.ctxs[0]->p.verbose) fprintf(stderr, "%s\n", last_error());
+        B.exec = nullptr;
+        B.failed = true;
+        return TOPO_ERR_UNSUPPORTED;
+    }
+    B.launches = n;
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    for (Ctx* c : B.ctxs) c->info.t_capture_ms = ms;
+    return 0;
+}
+
+// Launches one iteration of each of the n contexts (every one prepared for
+// replay by opt_step_graph_prepare, none in flight) as one graph launch, or
+// sets *launched = false when no batch graph can be had (fewer than two
+// contexts, a failed capture): the caller then launches the contexts' own
+// graphs.  Results are read per context with opt_step_graph_finish.
+int opt_step_graph_batch(Ctx* const* cs, int n, bool* launched) {
+    *launched = false;
+    if (n < 2) return 0;
+    std::lock_guard<std::mutex> lk(batch_mutex());
+    auto& cache = batch_cache();
+    size_t at = cache.size();
+    for (size_t k = 0; k < cache.size(); k++)
+        if (cache[k]->ctxs.size() == (size_t)n && std::equal(cs, cs + n, cache[k]->ctxs.begin())) at = k;
+    if (at == cache.size()) {
+        if (cache.size() >= kMaxBatchGraphs) cache.erase(cache.begin());
+        auto b = std::make_unique<BatchGraph>();
+        b->ctxs.assign(cs, cs + n);
+        cache.push_back(std::move(b));
+        at = cache.size() - 1;
+    } else if (at + 1 != cache.size()) {  // most recently used last
+        std::unique_ptr<BatchGraph> b = std::move(cache[at]);
+        cache.erase(cache.begin() + at);
+        cache.push_back(std::move(b));
+        at = cache.size() - 1;
+    }
+    BatchGraph& B = *cache[at];
+    std::vector<uint64_t> gens(n);
+    for (int i = 0; i < n; i++) gens[i] = cs[i]->sg.gen;
+    if (gens != B.gens) {  // an instance recaptured its graphs: its buffers or options changed
+        B.drop();
+        B.failed = false;
+        B.gens = gens;
+    }
+    if (B.failed) return 0;
+    if (!B.exec && capture_batch(B) < 0) return 0;
+    // the graph starts after everything queued on every instance's stream
+    for (int i = 0; i < n; i++) {
+        TCK(cudaEventRecord(cs[i]->sg.e0, cs[i]->s));
+        TCK(cudaStreamWaitEvent(B.s, cs[i]->sg.e0, 0));
+    }
+    int dev = 0;
+    TCK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("device index %d out of range", dev);
+        return TOPO_ERR_UNSUPPORTED;
+    }
+    {
+        std::lock_guard<std::mutex> lk2(mma_chain_mutex());
+        cudaEvent_t& ev = mma_chain_event[dev];
+        if (!ev) TCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        TCK(cudaStreamWaitEvent(B.s, ev, 0));
+        TCK(cudaGraphLaunch(B.exec, B.s));
+        TCK(cudaEventRecord(ev, B.s));
+    }
+    __atomic_fetch_add(&launch_counter(), B.launches, __ATOMIC_RELAXED);
+    // each instance's stream continues after the batch
+    for (int i = 0; i < n; i++) {
+        Ctx& c = *cs[i];
+        TCK(cudaEventRecord(c.sg.e1, B.s));
+        TCK(cudaStreamWaitEvent(c.s, c.sg.e1, 0));
+        c.itr++;
+        c.info.step_graph = 2;
+    }
+    *launched = true;
+    return 0;
+}
+
+// Drops every batch graph that names context c (it is being destroyed).
+void step_batch_forget(const Ctx* c) {
+    std::lock_guard<std::mutex> lk(batch_mutex());
+    auto& cache = batch_cache();
+    for (size_t k = cache.size(); k-- > 0;)
+        if (std::find(cache[k]->ctxs.begin(), cache[k]->ctxs.end(), c) != cache[k]->ctxs.end())
+            cache.erase(cache.begin() + k);
 }
 
 }  // namespace topo
