@@ -332,9 +332,20 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
     // path: the slot record (global and chunk-local node ids, Dirichlet mask,
     // modulus) two phases ahead, the U_e fragments (B operand: DOF
     // 4kt + lane%4, case lane/4 + 8nt) one phase ahead.
+    // Lane-level view of one element's fragments (fixed by the mma layout):
+    // - B row d = 4 kt + lane%4 is DOF (comp, node) with node = d % NEN and
+    //   comp = d / NEN: for hex8 node 4 (kt & 1) + lane%4 and comp kt / 2,
+    //   for tet4 node lane%4 and comp kt, so a lane's six B rows touch NBN
+    //   element nodes (2 or 1);
+    // - D row 8 mt + lane/4 is node lane/4 (hex8; comp mt) or (lane/4) % 4
+    //   (tet4; comp 2 mt + lane/16), one element node per lane.
+    // The per-element record a lane loads is therefore NBN global node ids,
+    // one D-row node id, the Dirichlet mask and the modulus.
+    constexpr int NBN = NEN == 8 ? 2 : 1;
+    const int lD = NEN == 8 ? (lane >> 2) : ((lane >> 2) & 3);
     struct Meta {
-        int gn[KT];     // global node of this lane's B rows
-        int dn[MT];     // MODE 0: chunk-local node of this lane's D rows; MODE 1: global node
+        int gb[NBN];    // global nodes of this lane's B rows
+        int dn;         // MODE 0: chunk-local node of this lane's D rows; MODE 1: global node
         uint32_t msk;
         int e;
         double E;
@@ -347,32 +358,29 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
         if (warp >= a.ph_sl[ph + 1] - s0) return;
         const int slot = s0 + warp;
         m.has = true;
+        const int* gns = a.sl_gn + (size_t)slot * NEN;
 #pragma unroll
-        for (int kt = 0; kt < KT; kt++) {
-            const int d = 4 * kt + (lane & 3);
-            m.gn[kt] = d < ND ? a.sl_gn[(size_t)slot * NEN + d % NEN] : 0;
-        }
-#pragma unroll
-        for (int mt = 0; mt < MT; mt++) {
-            const int dof = 8 * mt + (lane >> 2);
-            const int l = (dof < ND ? dof : 0) % NEN;
-            m.dn[mt] = MODE == 0 ? (int)a.sl_lc[(size_t)slot * NEN + l] : a.sl_gn[(size_t)slot * NEN + l];
-        }
+        for (int h = 0; h < NBN; h++) m.gb[h] = gns[4 * h + (lane & 3)];
+        m.dn = MODE == 0 ? (int)a.sl_lc[(size_t)slot * NEN + lD] : gns[lD];
         m.msk = MODE == 0 ? a.sl_mask[slot] : 0u;
-        m.e = a.sl_elem[slot];
+        if (MODE == 1) m.e = a.sl_elem[slot];
         m.E = MODE == 0 ? a.Es[slot] : 1.0;
     };
     auto load_b = [&](const Meta& m, double (&bf)[KT][NT]) {
         if (!m.has) return;
+        const uint32_t lm = m.msk >> (lane & 3);  // bit 4 kt: B row d = 4 kt + lane%4 is fixed
+        long base[NBN];
+#pragma unroll
+        for (int h = 0; h < NBN; h++) base[h] = (long)m.gb[h] * (3 * KB) + (lane >> 2);
 #pragma unroll
         for (int kt = 0; kt < KT; kt++) {
-            const int d = 4 * kt + (lane & 3);
-            const int comp = d / NEN;
+            const int h = NEN == 8 ? (kt & 1) : 0;
+            const int comp = NEN == 8 ? (kt >> 1) : kt;
+            const bool fixed = (lm >> (4 * kt)) & 1u;
 #pragma unroll
             for (int nt = 0; nt < NT; nt++) {
                 const int n = (lane >> 2) + 8 * nt;
-                bf[kt][nt] = (d < ND && n < KB && !((m.msk >> d) & 1u)) ? (double)u[(3L * m.gn[kt] + comp) * KB + n]
-                                                                        : 0.0;
+                bf[kt][nt] = (n < KB && !fixed) ? (double)u[base[h] + comp * KB + 8 * nt] : 0.0;
             }
         }
     };
@@ -425,23 +433,26 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
                     for (int kt = 0; kt < KT; kt++)
 #pragma unroll
                         for (int mt = 0; mt < MT; mt++) {
-                            const double av = aoff[mt][kt] >= 0 ? ks[aoff[mt][kt]] : 0.0;
+                            // hex8: 24 = 3 x 8 rows and 6 x 4 columns, every index valid
+                            const double av = (ND % 8 == 0 || aoff[mt][kt] >= 0) ? ks[aoff[mt][kt]] : 0.0;
                             dmma(acc[mt], av, bcur[kt][nt]);
                         }
                 }
+                const int n0 = 2 * (lane & 3) + 8 * nt;
+                // this lane's D rows: one element node, component comp(mt)
+                const long dbase = MODE == 0 ? (long)mc.dn * NVL + n0 : (long)mc.dn * (3 * KB) + n0;
 #pragma unroll
                 for (int mt = 0; mt < MT; mt++) {
                     const int dof = 8 * mt + (lane >> 2);
-                    const int n0 = 2 * (lane & 3) + 8 * nt;
                     if (dof < ND) {
-                        const int comp = dof / NEN;
+                        const int comp = NEN == 8 ? mt : 2 * mt + (lane >> 4);
                         if (MODE == 0) {
                             // the lane's two cases are one aligned 16-byte pair: n0 is even, the
                             // node and component offsets are multiples of KB >= 4 doubles, and
                             // the image starts 8 * ST * NPK doubles (a multiple of 16 bytes)
                             // after the 128-byte aligned element-matrix ring
                             if (n0 < KB) {
-                                double2* yp = reinterpret_cast<double2*>(yl + (size_t)mc.dn[mt] * NVL + comp * KB + n0);
+                                double2* yp = reinterpret_cast<double2*>(yl + dbase + comp * KB);
                                 double2 cur = *yp;
                                 cur.x += sc * acc[mt][0];
                                 cur.y += sc * acc[mt][1];
@@ -450,7 +461,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
                         } else {
 #pragma unroll
                             for (int i = 0; i < 2; i++)
-                                if (n0 + i < KB) q += acc[mt][i] * (double)u[(3L * mc.dn[mt] + comp) * KB + n0 + i];
+                                if (n0 + i < KB) q += acc[mt][i] * (double)u[dbase + comp * KB + i];
                         }
                     }
                 }
