@@ -102,6 +102,13 @@ typedef struct topo_params {
                               One load case (the block solver always steps directly). */
     int blk_stages;        /* block operator: element-matrix copies in flight per warp, 2 or 3;
                               0 (default): the autotuner times both */
+    int deterministic;     /* 1: bitwise-reproducible runs (same inputs, options and GPU give the
+                              same bits): the element operators add each node's element
+                              contributions in a fixed order (a per-element pass into scratch, then
+                              a gather over the node-to-element map) instead of with atomics, no
+                              launch shape is autotuned, and several load cases are solved one by
+                              one; fixed at creation.  0 (default): atomic scatters (runs agree to
+                              rounding) */
 } topo_params;
 
 typedef struct topo_solve_info {

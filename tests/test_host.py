@@ -52,7 +52,7 @@ def test_struct_mirrors_match_the_library(T):
     assert (p.cheb_degree, p.cheb_degree_post, p.cheb_degree_coarse) == (2, 0, 4)
     assert (p.fem_restart, p.fem_block, p.fem_graphs, p.autotune, p.pdl) == (30, 1, 1, 1, 1)
     assert (p.amg_coarse_cta, p.amg_half_fine, p.fem_warm_start) == (0, 0, 0)
-    assert (p.step_graph, p.blk_stages) == (0, 0)
+    assert (p.step_graph, p.blk_stages, p.deterministic) == (0, 0, 0)
 
 
 @pytest.mark.parametrize("nen", [8, 4])
@@ -208,7 +208,8 @@ def test_driver_program_fails_loudly_without_a_gpu(tmp_path):
                                          ("amg_max_levels", 9), ("amg_rho_its", -2), ("cheb_safety", -0.5),
                                          ("pdl", 2), ("fem_graphs", -1), ("autotune", 3), ("amg_half_fine", 2),
                                          ("fem_block", 5), ("proj", 2), ("amg_coarse_max", 5), ("cheb_degree", 0),
-                                         ("step_graph", 2), ("blk_stages", 1), ("blk_stages", 4)])
+                                         ("step_graph", 2), ("blk_stages", 1), ("blk_stages", 4),
+                                         ("deterministic", 2)])
 def test_invalid_solver_options_rejected_before_any_device_work(T, field, value):
     """Out-of-range solver options are refused at creation with the option's
     name in the message (no silent clamping), before any device call."""

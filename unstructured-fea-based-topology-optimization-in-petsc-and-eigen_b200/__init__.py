@@ -53,7 +53,8 @@ class Params(C.Structure):
         ("amg_half_fine", C.c_int),
         ("pdl", C.c_int),
         ("step_graph", C.c_int),
-        ("blk_stages", C.c_int)]
+        ("blk_stages", C.c_int),
+        ("deterministic", C.c_int)]
 
 
 class SolveInfo(C.Structure):

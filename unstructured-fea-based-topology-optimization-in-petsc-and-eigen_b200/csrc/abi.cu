@@ -247,6 +247,7 @@ int create(Ctx& c, int nen, int n_nodes, const double* vertex, int n_elems, cons
     for (DBuf<double>* b : {&c.RX, &c.TX, &c.fr, &c.fz, &c.fp, &c.fw}) { TRET(b->alloc(c.nn)); TRET(b->zero(c.s)); }
     TRET(build_amg_host(c));
     TRET(amg_alloc(c));
+    if (c.p.deterministic) TRET(c.det_scr.alloc((size_t)c.ntiles * 32 * c.nde));  // per-element contributions
     TRET(mma_alloc(c));
     TCK(cudaStreamSynchronize(c.s));
     return 0;
@@ -328,6 +329,7 @@ void topo_params_default(topo_params* p) {
     p->autotune = 1;
     p->pdl = 1;
     p->step_graph = 0;
+    p->deterministic = 0;
 }
 
 int topo_device_alloc(size_t bytes, void** ptr) {
@@ -391,7 +393,7 @@ static int check_params(const topo_params* p) {
         {p->proj, "proj"}, {p->amg_smooth_p, "amg_smooth_p"}, {p->fine_smoother_matfree, "fine_smoother_matfree"},
         {p->fem_warm_start, "fem_warm_start"}, {p->fem_block, "fem_block"}, {p->fem_graphs, "fem_graphs"},
         {p->autotune, "autotune"}, {p->amg_coarse_cta, "amg_coarse_cta"}, {p->amg_half_fine, "amg_half_fine"},
-        {p->pdl, "pdl"}, {p->step_graph, "step_graph"}};
+        {p->pdl, "pdl"}, {p->step_graph, "step_graph"}, {p->deterministic, "deterministic"}};
     for (const auto& f : flags)
         if (f.v != 0 && f.v != 1) { set_error("%s must be 0 or 1", f.name); return TOPO_ERR_ARG; }
     return 0;
@@ -488,8 +490,9 @@ int topo_set_params(topo_ctx* ctx, const topo_params* p) {
     TRET(check_params(p));
     const topo_params& o = ctx->c.p;
     if (p->nu != o.nu || p->rmin != o.rmin || p->m != o.m || p->amg_max_levels != o.amg_max_levels ||
-        p->amg_coarse_max != o.amg_coarse_max || p->amg_smooth_p != o.amg_smooth_p || p->fem_restart != o.fem_restart) {
-        set_error("nu, rmin, m, restart and AMG structure options are fixed at creation");
+        p->amg_coarse_max != o.amg_coarse_max || p->amg_smooth_p != o.amg_smooth_p || p->fem_restart != o.fem_restart ||
+        p->deterministic != o.deterministic) {
+        set_error("nu, rmin, m, restart, AMG structure options and deterministic are fixed at creation");
         return TOPO_ERR_ARG;
     }
     ctx->c.p = *p;

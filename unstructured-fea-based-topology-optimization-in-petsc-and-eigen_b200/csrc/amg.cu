@@ -1206,7 +1206,7 @@ static int prolong(Ctx& c, int l, const T* xc, T* xf, int mode, const T* dinv) {
 // level 0 of the mixed form runs on the FP16 scaled operator (single load case)
 static bool use_half0(const Ctx& c) {
     return c.p.precision == TOPO_PREC_MIXED && c.p.amg_half_fine && !c.p.fine_smoother_matfree &&
-           !(c.ncases > 1 && c.p.fem_block);
+           !block_cases(c);
 }
 template <class T>
 static bool half_level(const Ctx& c, int l) {

@@ -749,7 +749,7 @@ static int tune_sell_u_kb(Ctx& c, cudaEvent_t e0, cudaEvent_t e1) {
 
 int autotune_block(Ctx& c) {
     BlockState& B = c.blk;
-    if (!c.p.autotune || c.tune.block_done || !B.V.p) return 0;
+    if (!tuning_on(c) || c.tune.block_done || !B.V.p) return 0;
     c.tune.block_done = true;
     const long nf = (long)c.ndof * B.kb;
     double* u = B.V.p;

@@ -194,6 +194,7 @@ struct Ctx {
     double TV = 0.0;
     DBuf<double> F;             // [ncases][ndof]
     DBuf<int> n2e_ptr, n2e;     // node -> element*nen + local
+    DBuf<double> det_scr;       // deterministic form: per-element operator contributions [tile][nde][32]
     DBuf<uint16_t> bpos;        // [ne][nen][nen] slot of node q in node p's row
     int maxdeg = 0;
 
@@ -322,6 +323,14 @@ struct Ctx {
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rec[12];
     } prof;
 };
+
+// launch shapes are timed on the context's data unless the run must be
+// bitwise reproducible (a shape can change the order of a sum)
+inline bool tuning_on(const Ctx& c) { return c.p.autotune && !c.p.deterministic; }
+// several load cases share the block operator and block V-cycle, unless the
+// run must be bitwise reproducible (the block operator adds chunk images
+// with atomics): then they are solved one by one
+inline bool block_cases(const Ctx& c) { return c.ncases > 1 && c.p.fem_block && !c.p.deterministic; }
 
 // profiler slots
 enum ProfSlot {

@@ -299,7 +299,11 @@ int compute_moduli(Ctx& c, const double* xphys) {
 // nodes of a face: the lane-pair combine folds lane i+1's left-face
 // contribution into lane i's right-face one when the node ids agree
 // (checked, so any mesh stays correct), halving the atomics on such meshes.
-template <int NEN, class TK, class TU, class TY>
+//
+// STORE (the deterministic form): instead of adding into y, the element's
+// 3*NEN outputs go to the scratch y in the AoSoA layout [tile][3 NEN][32],
+// and k_node_gather3 adds them node by node in a fixed order.
+template <int NEN, class TK, class TU, class TY, bool STORE>
 __global__ void __launch_bounds__(128) k_kmv(int ne, const int* __restrict__ conn, const uint32_t* __restrict__ emask,
                                              const TK* __restrict__ ke, const TK* __restrict__ Ee,
                                              const TU* __restrict__ u, TY* __restrict__ y, TK alpha) {
@@ -344,6 +348,12 @@ __global__ void __launch_bounds__(128) k_kmv(int ne, const int* __restrict__ con
     }
 #pragma unroll
     for (int i = 0; i < ND; i++) ye[i] *= E;
+    if constexpr (STORE) {
+        if (active)
+#pragma unroll
+            for (int i = 0; i < ND; i++) y[((size_t)tile * ND + i) * 32 + lane] = TY(ye[i]);
+        return;
+    }
     if constexpr (NEN == 8) {
         // lane-pair combine across the shared x-face: my local nodes 1,3,5,7
         // against the next lane's local nodes 0,2,4,6
@@ -380,6 +390,43 @@ __global__ void __launch_bounds__(128) k_kmv(int ne, const int* __restrict__ con
     }
 }
 
+// Deterministic scatter, second pass: node n adds, in the fixed order of the
+// node-to-element map (entries e * NEN + l, ascending), the contributions its
+// elements stored in the first pass: y[3n + c] += sum scr[e][c NEN + l].
+template <int NEN, class TY>
+__global__ void k_node_gather3(int nn, const int* __restrict__ n2e_ptr, const int* __restrict__ n2e,
+                               const TY* __restrict__ scr, TY* __restrict__ y) {
+    constexpr int ND = 3 * NEN;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nn) return;
+    TY s0 = TY(0), s1 = TY(0), s2 = TY(0);
+    const int p1 = n2e_ptr[n + 1];
+    for (int p = n2e_ptr[n]; p < p1; p++) {
+        const int q = n2e[p], e = q / NEN, l = q - e * NEN;
+        const TY* b = scr + ((size_t)(e >> 5) * ND + l) * 32 + (e & 31);
+        s0 += b[0];
+        s1 += b[NEN * 32];
+        s2 += b[2 * NEN * 32];
+    }
+    y[3L * n] += s0;
+    y[3L * n + 1] += s1;
+    y[3L * n + 2] += s2;
+}
+// the same for one value per node (the Helmholtz filter operator)
+template <int NEN>
+__global__ void k_node_gather1(int nn, const int* __restrict__ n2e_ptr, const int* __restrict__ n2e,
+                               const double* __restrict__ scr, double* __restrict__ y) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nn) return;
+    double s = 0.0;
+    const int p1 = n2e_ptr[n + 1];
+    for (int p = n2e_ptr[n]; p < p1; p++) {
+        const int q = n2e[p], e = q / NEN, l = q - e * NEN;
+        s += scr[((size_t)(e >> 5) * NEN + l) * 32 + (e & 31)];
+    }
+    y[n] += s;
+}
+
 // y = beta*b (or 0 if b == null) before the element scatter
 template <class TY>
 __global__ void k_init_y(long n, TY* __restrict__ y, const TY* __restrict__ b, TY beta) {
@@ -399,10 +446,25 @@ __global__ void k_fix_rows(int nf, const int* __restrict__ fixed, const TU* __re
 template <class TK, class TU, class TY>
 static int launch_kmv(Ctx& c, const TK* ke, const TK* Ee, const TU* u, TY* y, TK alpha) {
     const int block = c.tune.kmv_block, grid = c.ntiles * 32 / block + 1;
+    if (c.p.deterministic) {
+        // per-element outputs into scratch, then a fixed-order node gather
+        TY* scr = reinterpret_cast<TY*>(c.det_scr.p);
+        if (!scr) { set_error("deterministic form: no scratch (the option is fixed at creation)"); return TOPO_ERR_ARG; }
+        const int gn = (c.nn + 255) / 256;
+        if (c.nen == 8) {
+            k_kmv<8, TK, TU, TY, true><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, scr, alpha), note_launch();
+            k_node_gather3<8, TY><<<gn, 256, 0, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, scr, y), note_launch();
+        } else {
+            k_kmv<4, TK, TU, TY, true><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, scr, alpha), note_launch();
+            k_node_gather3<4, TY><<<gn, 256, 0, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, scr, y), note_launch();
+        }
+        TCK(cudaGetLastError());
+        return 0;
+    }
     if (c.nen == 8)
-        k_kmv<8, TK, TU, TY><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, y, alpha), note_launch();
+        k_kmv<8, TK, TU, TY, false><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, y, alpha), note_launch();
     else
-        k_kmv<4, TK, TU, TY><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, y, alpha), note_launch();
+        k_kmv<4, TK, TU, TY, false><<<grid, block, 0, c.s>>>(c.ne, c.conn.p, c.emask.p, ke, Ee, u, y, alpha), note_launch();
     TCK(cudaGetLastError());
     return 0;
 }
@@ -543,7 +605,7 @@ int fem_sensitivities(Ctx& c, const double* xphys, double* dfdx, double* dgdx) {
     if (!c.uku.p) TRET(c.uku.alloc(c.ne));
     // the block solve leaves all cases in one case-interleaved vector: one
     // tensor-core pass gives the uKu sum over the cases
-    const bool blk = c.ncases > 1 && c.p.fem_block && c.blk.u_fresh;
+    const bool blk = block_cases(c) && c.blk.u_fresh;
     if (blk) TRET(blk_uku(c, c.blk.U.p, c.uku.p));
     for (int cs = 0; cs < c.ncases && !blk; cs++) {
         const double* Uc = c.U.p + (size_t)cs * c.ndof;
@@ -574,8 +636,25 @@ __global__ void k_tf(int ne, const int* __restrict__ conn, const double* __restr
         atomicAdd(&tx[nd], tf[((size_t)tile * NEN + l) * 32 + lane] * xe);
     }
 }
-// y = KF r, matrix free over the packed NEN x NEN Helmholtz matrices
+// deterministic form of k_tf: node n sums T_e[l] x_e over its elements in
+// the fixed order of the node-to-element map
 template <int NEN>
+__global__ void k_tf_gather(int nn, const int* __restrict__ n2e_ptr, const int* __restrict__ n2e,
+                            const double* __restrict__ tf, const double* __restrict__ x, double* __restrict__ tx) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nn) return;
+    double s = 0.0;
+    const int p1 = n2e_ptr[n + 1];
+    for (int p = n2e_ptr[n]; p < p1; p++) {
+        const int q = n2e[p], e = q / NEN, l = q - e * NEN;
+        s += tf[((size_t)(e >> 5) * NEN + l) * 32 + (e & 31)] * x[e];
+    }
+    tx[n] = s;
+}
+// y = KF r, matrix free over the packed NEN x NEN Helmholtz matrices
+// (STORE: the element outputs go to the scratch y as [tile][NEN][32] for
+// k_node_gather1, the deterministic form)
+template <int NEN, bool STORE>
 __global__ void __launch_bounds__(128) k_kf(int ne, const int* __restrict__ conn, const double* __restrict__ kf,
                                             const double* __restrict__ r, double* __restrict__ y) {
     constexpr int NPK = NEN * (NEN + 1) / 2;
@@ -600,8 +679,13 @@ __global__ void __launch_bounds__(128) k_kf(int ne, const int* __restrict__ conn
             ye[i] += a * re[j];
             if (j != i) ye[j] += a * re[i];
         }
+    if constexpr (STORE) {
 #pragma unroll
-    for (int l = 0; l < NEN; l++) atomicAdd(&y[nd[l]], ye[l]);
+        for (int l = 0; l < NEN; l++) y[((size_t)tile * NEN + l) * 32 + lane] = ye[l];
+    } else {
+#pragma unroll
+        for (int l = 0; l < NEN; l++) atomicAdd(&y[nd[l]], ye[l]);
+    }
 }
 // xf_e = sum_l (1/NEN) rx[node_l]  (MatMultTranspose(TFX), PDEFilter.cpp:107,149), optional clamp
 template <int NEN>
@@ -622,6 +706,13 @@ __global__ void k_tfxT(int ne, const int* __restrict__ conn, const double* __res
 }
 
 int filter_tf(Ctx& c, const double* x, double* tx) {
+    if (c.p.deterministic) {
+        const int gn = (c.nn + 255) / 256;
+        if (c.nen == 8) k_tf_gather<8><<<gn, 256, 0, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.tf.p, x, tx), note_launch();
+        else k_tf_gather<4><<<gn, 256, 0, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, c.tf.p, x, tx), note_launch();
+        TCK(cudaGetLastError());
+        return 0;
+    }
     TCK(cudaMemsetAsync(tx, 0, sizeof(double) * c.nn, c.s));
     int g = (c.ne + 127) / 128;
     if (c.nen == 8) k_tf<8><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.tf.p, x, tx), note_launch();
@@ -634,8 +725,23 @@ int filter_kf(Ctx& c, const double* r, double* y) {
     int g = (c.ne + 127) / 128;
     cudaEvent_t e0;
     prof_begin(c, PS_FILTER, &e0);
-    if (c.nen == 8) k_kf<8><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.kf.p, r, y), note_launch();
-    else k_kf<4><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.kf.p, r, y), note_launch();
+    if (c.p.deterministic) {
+        // per-element outputs into scratch, then a fixed-order node gather
+        double* scr = c.det_scr.p;
+        if (!scr) { set_error("deterministic form: no scratch (the option is fixed at creation)"); return TOPO_ERR_ARG; }
+        const int gn = (c.nn + 255) / 256;
+        if (c.nen == 8) {
+            k_kf<8, true><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.kf.p, r, scr), note_launch();
+            k_node_gather1<8><<<gn, 256, 0, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, scr, y), note_launch();
+        } else {
+            k_kf<4, true><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.kf.p, r, scr), note_launch();
+            k_node_gather1<4><<<gn, 256, 0, c.s>>>(c.nn, c.n2e_ptr.p, c.n2e.p, scr, y), note_launch();
+        }
+    } else if (c.nen == 8) {
+        k_kf<8, false><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.kf.p, r, y), note_launch();
+    } else {
+        k_kf<4, false><<<g, 128, 0, c.s>>>(c.ne, c.conn.p, c.kf.p, r, y), note_launch();
+    }
     prof_end(c, PS_FILTER, e0);
     TCK(cudaGetLastError());
     return 0;

@@ -245,7 +245,7 @@ static int time_best(Ctx& c, F&& fn, double* ms) {
 }
 
 int autotune_single(Ctx& c) {
-    if (!c.p.autotune || c.tune.single_done || !c.V.p) return 0;
+    if (!tuning_on(c) || c.tune.single_done || !c.V.p) return 0;
     c.tune.single_done = true;
     const long n = c.ndof;
     const long ldv = (n + 31) & ~31L;
@@ -521,7 +521,7 @@ static int fgmres_dd(Ctx& c, const double* b, double* x) {
     const long ldv = (n + 31) & ~31L;
     const bool mixed = c.p.precision == TOPO_PREC_MIXED;
     if (!c.V.p || (long)c.V.n < (long)(m + 1) * ldv || (mixed ? !c.Z32.p : !c.Z64.p) ||
-        (c.p.autotune && !c.tune.single_done)) {
+        (tuning_on(c) && !c.tune.single_done)) {
         set_error("the device-driven step needs a direct solve of this form first");
         return TOPO_ERR_ARG;
     }
@@ -701,7 +701,7 @@ int fem_solve(Ctx& c, const double* xphys, double* u) {
 
 // moduli, AMG numeric setup, U = 0, FGMRES, then the true relative residual
 static int fem_solve_impl(Ctx& c, const double* xphys, double* u) {
-    if (c.ncases > 1 && c.p.fem_block) return fem_solve_block(c, xphys, u);
+    if (block_cases(c)) return fem_solve_block(c, xphys, u);
     if (c.sg.dd && c.ncases != 1) {
         set_error("the device-driven step supports one load case (or the block solver)");
         return TOPO_ERR_UNSUPPORTED;

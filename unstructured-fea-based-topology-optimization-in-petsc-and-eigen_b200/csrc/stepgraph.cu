@@ -259,7 +259,7 @@ static int capture_step(Ctx& c) {
 // precision) has allocated it and the autotuner has run
 static bool graph_ready(const Ctx& c) {
     const bool mixed = c.p.precision == TOPO_PREC_MIXED;
-    return c.X.p && c.U.p && c.V.p && c.uku.p && c.L.p && (!c.p.autotune || c.tune.single_done) &&
+    return c.X.p && c.U.p && c.V.p && c.uku.p && c.L.p && (!tuning_on(c) || c.tune.single_done) &&
            (mixed ? (c.Z32.p && c.v32.allocated) : (c.Z64.p && c.v64.allocated));
 }
 
