@@ -183,13 +183,95 @@ int blk_build_schedule(Ctx& c, int node_cap) {
     return 0;
 }
 
-// keb[slot][k] = Ke entry k of element sl_elem[slot] (from the AoSoA tiles)
-__global__ void k_keb_gather(int nslot, int npk, const int* __restrict__ sl_elem, const double* __restrict__ ke,
-                             double* __restrict__ keb) {
+__host__ __device__ __forceinline__ int pk_idx(int i, int j, int n) {
+    if (i > j) { int t = i; i = j; j = t; }
+    return i * n - (i * (i - 1)) / 2 + (j - i);
+}
+
+// Bank layout of the block operator's packed element matrices.  Lane l of a
+// warp reads the A-fragment entry (8 mt + l/4, 4 kt + l%4) of the packed
+// symmetric Ke; a 64-bit shared load is served per half-warp, without bank
+// conflicts when its 16 lanes' distinct entries sit at positions distinct
+// mod 16.  The packed entries are therefore stored permuted: entry k at
+// perm[k], with perm built from a colouring of the entries by position mod
+// 16 in which every half-warp fragment gets distinct colours (a greedy
+// colouring with a fixed seed; the identity if none is found).
+int blk_bank_perm(int nd, std::vector<int>& perm) {
+    const int npk = nd * (nd + 1) / 2, MT = (nd + 7) / 8, KT = (nd + 3) / 4;
+    std::vector<std::vector<int>> groups;
+    for (int mt = 0; mt < MT; mt++)
+        for (int kt = 0; kt < KT; kt++)
+            for (int h = 0; h < 2; h++) {
+                std::vector<int> g;
+                for (int l = 16 * h; l < 16 * h + 16; l++) {
+                    const int i = 8 * mt + l / 4, j = 4 * kt + l % 4;
+                    if (i < nd && j < nd) g.push_back(pk_idx(i, j, nd));
+                }
+                std::sort(g.begin(), g.end());
+                g.erase(std::unique(g.begin(), g.end()), g.end());
+                groups.push_back(g);
+            }
+    std::vector<std::vector<int>> member(npk);
+    std::vector<int> weight(npk, 0);
+    for (int gi = 0; gi < (int)groups.size(); gi++)
+        for (int k : groups[gi]) {
+            member[k].push_back(gi);
+            weight[k] += (int)groups[gi].size();
+        }
+    uint64_t rs = 0x2545F4914F6CDD1Dull;
+    auto rnd = [&]() {
+        rs ^= rs << 13;
+        rs ^= rs >> 7;
+        rs ^= rs << 17;
+        return rs;
+    };
+    perm.resize(npk);
+    for (int t = 0; t < 200; t++) {
+        std::vector<int> order(npk);
+        for (int k = 0; k < npk; k++) order[k] = k;
+        for (int k = npk - 1; k > 0; k--) std::swap(order[k], order[(int)(rnd() % (uint64_t)(k + 1))]);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return weight[a] > weight[b]; });
+        int left[16];
+        for (int r = 0; r < 16; r++) left[r] = (npk - r + 15) / 16;
+        std::vector<int> col(npk, -1);
+        std::vector<uint32_t> used(groups.size(), 0u);
+        bool ok = true;
+        for (int k : order) {
+            uint32_t bad = 0;
+            for (int g : member[k]) bad |= used[g];
+            int best = -1;
+            uint64_t bkey = 0;
+            for (int r = 0; r < 16; r++) {
+                if (((bad >> r) & 1u) || left[r] == 0) continue;
+                const uint64_t key = ((uint64_t)left[r] << 32) | (rnd() & 0xffffffffull);
+                if (best < 0 || key > bkey) { best = r; bkey = key; }
+            }
+            if (best < 0) { ok = false; break; }
+            col[k] = best;
+            left[best]--;
+            for (int g : member[k]) used[g] |= 1u << best;
+        }
+        if (!ok) continue;
+        int next[16];
+        for (int r = 0; r < 16; r++) next[r] = r;
+        for (int k = 0; k < npk; k++) {
+            perm[k] = next[col[k]];
+            next[col[k]] += 16;
+        }
+        return 1;
+    }
+    for (int k = 0; k < npk; k++) perm[k] = k;
+    return 0;
+}
+
+// keb[slot][perm[k]] = Ke entry k of element sl_elem[slot] (from the AoSoA tiles)
+__global__ void k_keb_gather(int nslot, int npk, const int* __restrict__ sl_elem, const int* __restrict__ perm,
+                             const double* __restrict__ ke, double* __restrict__ keb) {
     const int slot = blockIdx.x;
     if (slot >= nslot) return;
     const int e = sl_elem[slot], t = e >> 5, lane = e & 31;
-    for (int k = threadIdx.x; k < npk; k += blockDim.x) keb[(size_t)slot * npk + k] = ke[((size_t)t * npk + k) * 32 + lane];
+    for (int k = threadIdx.x; k < npk; k += blockDim.x)
+        keb[(size_t)slot * npk + perm[k]] = ke[((size_t)t * npk + k) * 32 + lane];
 }
 
 // Es[slot] = E[sl_elem[slot]] (refreshed when the moduli change)
@@ -246,10 +328,6 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-__host__ __device__ __forceinline__ int pk_idx(int i, int j, int n) {
-    if (i > j) { int t = i; i = j; j = t; }
-    return i * n - (i * (i - 1)) / 2 + (j - i);
-}
 
 struct BlkArgs {
     int nchunks;
@@ -261,7 +339,8 @@ struct BlkArgs {
     const int* sl_gn;        // slot -> nen global nodes
     const uint16_t* sl_lc;   // slot -> nen chunk-local nodes
     const uint32_t* sl_mask; // slot -> fixed local DOFs (bit c*nen + l)
-    const double* keb;       // slot -> packed Ke
+    const double* keb;       // slot -> packed Ke, entry k at kperm[k]
+    const int* kperm;
     const double* Es;        // slot -> element modulus
     int max_nodes;           // largest chunk node count (shared image rows)
     int* err;
@@ -274,7 +353,7 @@ struct BlkArgs {
 //         sets them).
 // MODE 1: uku[e] = sum_case u_e' Ke_e u_e (E = 1, unmasked u).
 template <int NEN, int KB, int MODE, class TU, int ST>
-__global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __restrict__ u, double* __restrict__ y,
+__global__ void __launch_bounds__(kWarps * 32, 3) k_blk_kmv(BlkArgs a, const TU* __restrict__ u, double* __restrict__ y,
                                                        double alpha, double* __restrict__ uku) {
     constexpr int ND = 3 * NEN, NPK = ND * (ND + 1) / 2;
     constexpr int MT = (ND + 7) / 8, KT = (ND + 3) / 4, NT = (KB + 7) / 8;
@@ -297,7 +376,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_blk_kmv(BlkArgs a, const TU* __
 #pragma unroll
         for (int kt = 0; kt < KT; kt++) {
             const int i = 8 * mt + (lane >> 2), j = 4 * kt + (lane & 3);
-            aoff[mt][kt] = (i < ND && j < ND) ? pk_idx(i, j, ND) : -1;
+            aoff[mt][kt] = (i < ND && j < ND) ? a.kperm[pk_idx(i, j, ND)] : -1;
         }
     if (MODE == 0)
         for (int i = threadIdx.x; i < a.max_nodes * NVL; i += blockDim.x) yl[i] = 0.0;
@@ -559,7 +638,7 @@ static int launch_blk_st(Ctx& c, const TU* u, double* y, double alpha, double* u
     const int per_sm = c.tune.blk_ctas > 0 ? std::min(std::max(1, occ), c.tune.blk_ctas) : std::max(1, occ);
     const int grid = std::max(1, std::min(B.nchunks, per_sm * nsm));
     BlkArgs a{B.nchunks, B.ch_ph.p, B.ph_sl.p, B.ch_np.p, B.ch_nodes.p, B.sl_elem.p, B.sl_gn.p, B.sl_lc.p,
-              B.sl_mask.p, B.keb.p, B.Es.p, B.max_nodes, B.err.p, c.wait.copy_cycles, c.wait.hold};
+              B.sl_mask.p, B.keb.p, B.kperm.p, B.Es.p, B.max_nodes, B.err.p, c.wait.copy_cycles, c.wait.hold};
     kern<<<grid, kWarps * 32, smem, c.s>>>(a, u, y, alpha, uku), note_launch();
     TCK(cudaGetLastError());
     return 0;
@@ -595,7 +674,10 @@ int blk_setup(Ctx& c) {
     TRET(B.keb.alloc((size_t)c.ne * c.npk));
     TRET(B.Es.alloc(c.ne));
     B.es_gen = -1;
-    k_keb_gather<<<c.ne, 128, 0, c.s>>>(c.ne, c.npk, B.sl_elem.p, c.ke64.p, B.keb.p), note_launch();
+    std::vector<int> perm;
+    blk_bank_perm(c.nde, perm);
+    TRET(B.kperm.upload(perm, c.s));
+    k_keb_gather<<<c.ne, 128, 0, c.s>>>(c.ne, c.npk, B.sl_elem.p, B.kperm.p, c.ke64.p, B.keb.p), note_launch();
     TCK(cudaGetLastError());
     TRET(B.err.alloc(1));
     TRET(B.err.zero(c.s));

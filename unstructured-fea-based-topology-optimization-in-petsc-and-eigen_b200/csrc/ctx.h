@@ -153,7 +153,8 @@ struct BlockState {
     DBuf<int> sl_elem, sl_gn;   // slot -> element, slot -> global nodes
     DBuf<uint16_t> sl_lc;       // slot -> chunk-local nodes
     DBuf<uint32_t> sl_mask;     // slot -> fixed local DOFs
-    DBuf<double> keb;           // slot -> packed Ke (E = 1)
+    DBuf<double> keb;           // slot -> packed Ke (E = 1), entry k at kperm[k] (bank layout)
+    DBuf<int> kperm;
     DBuf<double> Es;            // slot -> SIMP modulus of the current design
     int es_gen = -1;            // moduli generation Es was gathered from
     DBuf<int> err;              // set when a bounded wait expired
@@ -379,6 +380,7 @@ int filter_tfxT(Ctx& c, const double* rx, double* xf, bool clamp, double xmin);
 int von_mises(Ctx& c, const double* xphys, double* vms);
 
 int blk_width(int ncases);                                         // block.cu
+int blk_bank_perm(int nd, std::vector<int>& perm);  // 1: conflict-free layout found, 0: identity
 int blk_setup(Ctx& c);
 int blk_apply(Ctx& c, const double* u, double* y, const double* b, double alpha);
 int blk_apply_f32in(Ctx& c, const float* u, double* y, const double* b, double alpha);
