@@ -212,6 +212,34 @@ def run_device(ctx, T, torch, steps, warmup, stream, dist=None, profile=True):
     return ms, l1 - l0, prof, its
 
 
+def run_deterministic(T, torch, stream, wl, steps, warmup):
+    """The headline form (mixed, warm start, step graphs) with deterministic=1,
+    run twice in fresh contexts: design iterations/s and whether the two runs'
+    per-iteration compliance and final design agree bit for bit."""
+    v, e, f, ld, lv = T.gen_cantilever(wl["nx"], wl["ny"], wl["nz"], wl["nen"])
+    runs = []
+    for _ in range(2):
+        ctx = T.Context(v, e, f, ld, lv, precision=T.PREC_MIXED, deterministic=1, **PARAMS)
+        ctx.set_params(fem_warm_start=1)
+        ctx.opt_init()
+        for _ in range(warmup):
+            ctx.opt_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fx = [ctx.opt_step()[1] for _ in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        xp = ctx.opt_tensor(1).cpu()
+        runs.append((e0.elapsed_time(e1), fx, xp))
+        ctx.close()
+    ms = min(r[0] for r in runs)
+    return {"form": "mixed, warm start, step graphs, deterministic=1 (fixed-order node gathers, no autotuning)",
+            "steps": steps, "warmup": warmup, "value": steps / (ms / 1e3), "ms_per_step": ms / steps,
+            "two_runs_bitwise_equal": bool(runs[0][1] == runs[1][1] and torch.equal(runs[0][2], runs[1][2])),
+            "fx_last": runs[0][1][-1]}
+
+
 def run_e2e(ctx, T, torch, steps, warmup, stream, dist=None):
     import numpy as np
     ne = ctx.ne
@@ -477,6 +505,7 @@ def main():
     ap.add_argument("--multiload-forms", default="block_mixed,block_fp64,one_by_one_mixed")
     ap.add_argument("--no-tet4", action="store_true", help="skip the tet4 2.35M configuration")
     ap.add_argument("--no-instances", action="store_true", help="skip the batch of design instances")
+    ap.add_argument("--no-deterministic", action="store_true", help="skip the bitwise-reproducible form")
     ap.add_argument("--tet4-steps", type=int, default=4)
     ap.add_argument("--tet4-cpu-steps", type=int, default=1)
     ap.add_argument("--param", action="append", default=[],
@@ -649,6 +678,10 @@ def main():
     inst = None
     if not args.no_instances and rank == 0 and world == 1:
         inst = run_instances(T)
+    detm = None
+    if not args.no_deterministic and rank == 0 and world == 1:
+        detm = run_deterministic(T, torch, stream, wl, min(args.steps, 10), min(args.warmup, 3))
+        detm["over_atomic_form"] = detm["value"] / value
     tet4 = None
     if not args.no_tet4 and rank == 0 and world == 1:
         tet4 = run_tet4(T, torch, stream, args.tet4_steps, 2, 0 if args.no_cpu_baseline else args.tet4_cpu_steps)
@@ -672,7 +705,7 @@ def main():
             "e2e": {"value": e2e_val, "unit": "design iters/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "clocks": clocks, "cpu_baseline": cpu,
             "fgmres_initial_guess": "previous design iteration's U (warm start); stopping rule unchanged",
-            "multiload": multi, "tet4": tet4, "instances": inst, "serve_small_jobs": serve_small, "serve_unbatched": serve_unbatched,
+            "multiload": multi, "tet4": tet4, "instances": inst, "deterministic": detm, "serve_small_jobs": serve_small, "serve_unbatched": serve_unbatched,
             "serve": serve, "kernels": kern,
             "fgmres_its_per_step": {"mixed_warm": its, "mixed_zero_start": itsz, "fp64": its64, "fp64_warm": its64w,
                                     "mixed_fp16_fine": its16},
