@@ -139,11 +139,15 @@ __global__ void k_diag_inv(int nnode, const int* __restrict__ rp, const int* __r
 
 // ----------------------------------------------------------------- BSR SpMV
 // G lanes per block row.  mode 0: y = A x; 1: y = b - A x; 2: y += A x;
-// 3 (power iteration): y = sigma * Dinv A x with sigma = *scal.
+// 3 (power iteration): y = sigma * Dinv A x with sigma = *scal;
+// 5 (restriction into a level that is smoothed next): y = A x, and the
+// level's first Chebyshev step from a zero guess on the same rows (the
+// operations of k_cheb_first): r5 = y, d5 = x5 = Dinv y / (0.6 *scal).
 template <class T, int BR, int BC, int G>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_bsr_spmv(int nrows, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ A,
                            const T* __restrict__ x, T* __restrict__ y, const T* __restrict__ b, int mode,
-                           const T* __restrict__ dinv, const double* __restrict__ scal) {
+                           const T* __restrict__ dinv, const double* __restrict__ scal, T* __restrict__ r5,
+                           T* __restrict__ d5, T* __restrict__ x5) {
     pdl_trigger();
     const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     const int gl = threadIdx.x % G;
@@ -191,7 +195,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_bsr_spmv(int nr
         else if (mode == 1) y[o] = pre - v;
         else if (mode == 2) y[o] = pre + v;
         else if (mode == 4) y[o] += pre * v;  // row-scaled prolongation into hat variables
-        else y[o] = T(*scal) * pre * v;
+        else if (mode == 5) {
+            y[o] = v;
+            r5[o] = v;
+            const T it = T(1.0 / (0.6 * (*scal)));
+            const T di = pre * v * it;
+            d5[o] = di;
+            x5[o] = di;
+        } else y[o] = T(*scal) * pre * v;
     }
 }
 
@@ -879,6 +890,23 @@ __global__ void k_dense_apply(int n, const double* __restrict__ inv, const T* __
     if (lane == 0) x[i] = T(s);
 }
 
+// the mixed form's FP64 right-hand side to FP32 and, on the same entries,
+// the level-0 first Chebyshev step from the zero guess (the operations of
+// k_cheb_first): r = b, d = x = Dinv b / (0.6 rho)
+__global__ void k_convert_first(long n, const double* __restrict__ b64, float* __restrict__ b, float* __restrict__ r,
+                                float* __restrict__ d, float* __restrict__ x, const float* __restrict__ dinv,
+                                const double* __restrict__ rho) {
+    const double theta = 0.6 * (*rho);
+    const float it = float(1.0 / theta);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const float bi = float(b64[i]);
+        b[i] = bi;
+        r[i] = bi;
+        const float di = dinv[i] * bi * it;
+        d[i] = di;
+        x[i] = di;
+    }
+}
 template <class TI, class TO>
 __global__ void k_convert(long n, const TI* __restrict__ a, TO* __restrict__ b) {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = TO(a[i]);
@@ -1136,20 +1164,20 @@ static int spgemm_plan(Ctx& c, const DevPattern& Ap, const T* A, const T* B, con
 
 template <class T, int BR, int BC>
 static int spmv(Ctx& c, const DevPattern& Ap, const T* A, const T* x, T* y, const T* b, int mode, const T* dinv = nullptr,
-                const double* scal = nullptr, int gsel = 0) {
+                const double* scal = nullptr, int gsel = 0, T* r5 = nullptr, T* d5 = nullptr, T* x5 = nullptr) {
     const long nrows = Ap.nrows;
     const double avg = nrows ? (double)Ap.nnzb / nrows : 1.0;
     int G = gsel;
     if (G != 8 && G != 16 && G != 32) G = avg <= 6.0 ? 8 : (avg <= 20.0 ? 16 : 32);
     if (G == 8) {
         TCK(launch_k(c.vc_pdl, k_bsr_spmv<T, BR, BC, 8>, dim3((unsigned)((nrows * 8 + 255) / 256)), dim3(256), 0, c.s,
-                     (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal));
+                     (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal, r5, d5, x5));
     } else if (G == 16) {
         TCK(launch_k(c.vc_pdl, k_bsr_spmv<T, BR, BC, 16>, dim3((unsigned)((nrows * 16 + 255) / 256)), dim3(256), 0, c.s,
-                     (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal));
+                     (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal, r5, d5, x5));
     } else {
         TCK(launch_k(c.vc_pdl, k_bsr_spmv<T, BR, BC, 32>, dim3((unsigned)((nrows * 32 + 255) / 256)), dim3(256), 0, c.s,
-                     (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal));
+                     (int)nrows, Ap.rp.p, Ap.ci.p, A, x, y, b, mode, dinv, scal, r5, d5, x5));
     }
     TCK(cudaGetLastError());
     return 0;
@@ -1424,7 +1452,9 @@ void cheb_coeffs(int deg, double* cr, double* cq) {
 }
 
 template <class T>
-static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
+// first_done: the first Chebyshev step from the zero guess (r = b,
+// d = x = Dinv b / theta) was already taken by the kernel that produced b
+static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init, bool first_done = false) {
     AmgVals<T>& v = vals<T>(c);
     AmgDevLevel& D = c.dl[l];
     const long n = D.ndof;
@@ -1464,8 +1494,9 @@ static int smooth(Ctx& c, int l, const T* b, T* x, bool zero_init) {
             TRET(level_spmv<T>(c, l, x, v.r[l].p, b, 1));
         }
     }
-    TCK(launch_k(c.vc_pdl, k_cheb_first<T>, dim3(grid_for(n, 256)), dim3(256), 0, c.s, n, b, v.r[l].p, v.d[l].p, x,
-                 v.dinv[l].p, rho, zero_init ? 1 : 0));
+    if (!(zero_init && first_done))
+        TCK(launch_k(c.vc_pdl, k_cheb_first<T>, dim3(grid_for(n, 256)), dim3(256), 0, c.s, n, b, v.r[l].p, v.d[l].p, x,
+                     v.dinv[l].p, rho, zero_init ? 1 : 0));
     T* dcur = v.d[l].p;
     T* dnxt = v.d2[l].p;
     for (int k = 1; k < deg && k < 16; k++) {
@@ -1511,7 +1542,9 @@ struct PdlScope {
 };
 
 template <class T>
-static int vcycle(Ctx& c, const T* b0, T* x0) {
+// first0_done: the level-0 first Chebyshev step was taken with the
+// right-hand side's conversion (k_convert_first)
+static int vcycle(Ctx& c, const T* b0, T* x0, bool first0_done = false) {
     PdlScope pdl_scope(c, c.p.pdl != 0);
     AmgVals<T>& v = vals<T>(c);
     const int L = c.nlev - 1;
@@ -1524,9 +1557,10 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
     // levels l0..L run in one CTA (k_coarse_cycle); above them, per-level kernels
     const int l0 = coarse_cta_level(c);
     const int ldown = l0 > 0 ? l0 : L;
+    bool first_done = first0_done && !half_level<T>(c, 0);
     for (int l = 0; l < ldown; l++) {
         AmgDevLevel& D = c.dl[l];
-        TRET(smooth<T>(c, l, bl[l], xl[l], true));
+        TRET(smooth<T>(c, l, bl[l], xl[l], true, first_done));
         if (half_level<T>(c, l)) {
             // unscaled residual t = D^1/2 (b^ - A^ x^) for the restriction
             cudaEvent_t e0;
@@ -1540,8 +1574,20 @@ static int vcycle(Ctx& c, const T* b0, T* x0) {
         } else {
             TRET(level_spmv<T>(c, l, xl[l], v.t[l].p, bl[l], 1));
         }
-        if (D.bs == 3) TRET((spmv<T, 6, 3>(c, D.R, v.R[l].p, v.t[l].p, v.b[l + 1].p, nullptr, 0)));
-        else TRET((spmv<T, 6, 6>(c, D.R, v.R[l].p, v.t[l].p, v.b[l + 1].p, nullptr, 0)));
+        // when level l+1 is smoothed next, its first step from the zero guess
+        // is taken by the restriction that produces its right-hand side
+        const bool fuse = l + 1 < ldown;
+        const int rmode = fuse ? 5 : 0;
+        const T* di5 = fuse ? v.dinv[l + 1].p : nullptr;
+        const double* rho5 = fuse ? c.rho.p + 2 * kMaxLevels + l + 1 : nullptr;
+        T* r5 = fuse ? v.r[l + 1].p : nullptr;
+        T* d5 = fuse ? v.d[l + 1].p : nullptr;
+        T* x5 = fuse ? xl[l + 1] : nullptr;
+        if (D.bs == 3)
+            TRET((spmv<T, 6, 3>(c, D.R, v.R[l].p, v.t[l].p, v.b[l + 1].p, nullptr, rmode, di5, rho5, 0, r5, d5, x5)));
+        else
+            TRET((spmv<T, 6, 6>(c, D.R, v.R[l].p, v.t[l].p, v.b[l + 1].p, nullptr, rmode, di5, rho5, 0, r5, d5, x5)));
+        first_done = fuse;
         if (l == 0) prof_begin(c, PS_VC_COARSE, &ecoarse);
     }
     if (l0 > 0) {
@@ -1730,13 +1776,15 @@ int amg_vcycle64(Ctx& c, const double* b, double* x) { return vcycle<double>(c, 
 int amg_vcycle32(Ctx& c, const double* b64, float* x) {
     AmgVals<float>& v = c.v32;
     const long n = c.dl[0].ndof;
-    if (half_level<float>(c, 0))
+    const bool half = half_level<float>(c, 0);
+    if (half)
         k_to_hat<<<grid_for(n, 256), 256, 0, c.s>>>(n, b64, c.h0.sinv.p, v.b[0].p), note_launch();
     else
-        k_convert<double, float><<<grid_for(n, 256), 256, 0, c.s>>>(n, b64, v.b[0].p), note_launch();
+        k_convert_first<<<grid_for(n, 256), 256, 0, c.s>>>(n, b64, v.b[0].p, v.r[0].p, v.d[0].p, x, v.dinv[0].p,
+                                                          c.rho.p + 2 * kMaxLevels), note_launch();
     TCK(cudaGetLastError());
     // level-0 rhs lives in v.b[0]; the smoother keeps b intact
-    return vcycle<float>(c, v.b[0].p, x);
+    return vcycle<float>(c, v.b[0].p, x, !half);
 }
 
 }  // namespace topo
