@@ -12,14 +12,14 @@
 // a time: its packed Ke (300 doubles) is brought into shared memory by the
 // TMA engine (cp.async.bulk, completion on a per-warp mbarrier, a ring of
 // ST copies in flight per warp, 2 or 3 picked by the autotuner: 2 leaves room
-// for a third CTA per SM), the U_e fragments are gathered from
+// for more CTAs per SM), the U_e fragments are gathered from
 // global memory one phase ahead, and the outputs accumulate in a
 // shared-memory image of the chunk's nodes.  Elements are grouped (host
-// side, once per mesh) into chunks of <= 64 spatially close elements (Morton
+// side, once per mesh) into chunks of <= 32 spatially close elements (Morton
 // order of the centroids) and each chunk into phases of <= kWarps elements
 // that share no node, so a phase's warps update the shared image without
 // atomics; a chunk's image is added to global memory once, which cuts the
-// global atomics about 4x against per-element scatter.
+// global atomics about 3x against per-element scatter.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,8 +31,8 @@
 
 namespace topo {
 
-constexpr int kWarps = 8;      // warps (= elements per phase) per CTA
-constexpr int kChunkElems = 64;
+constexpr int kWarps = 4;      // warps (= elements per phase) per CTA
+constexpr int kChunkElems = 32;
 
 // ----------------------------------------------------------------- host: chunks and phases
 // spread the low 21 bits of v to every third bit (3D Morton code)
@@ -52,9 +52,11 @@ int blk_build_schedule(Ctx& c, int node_cap) {
     if (c.nn >= (1 << 29)) { set_error("block operator: at most 2^29 nodes"); return TOPO_ERR_UNSUPPORTED; }
     // Morton order of the element centroids on a grid of the mean element
     // size h = (node bounding box volume / elements)^(1/3); on a lattice the
-    // rounded centroid is the element's lattice index, so 64 consecutive
-    // codes are an aligned 4x4x4 brick, which the phase colouring below
-    // splits into 8 node-disjoint phases of 8
+    // rounded centroid is the element's lattice index, so 32 consecutive
+    // codes are an aligned 4x4x2 brick, which the phase colouring below
+    // splits into 8 node-disjoint phases of 4 (one element per warp of a
+    // 4-warp CTA; small CTAs keep 5 per SM resident, so 40 element-matrix
+    // copies per SM are in flight with 2 per warp)
     double lo[3] = {1e300, 1e300, 1e300}, nlo[3] = {1e300, 1e300, 1e300}, nhi[3] = {-1e300, -1e300, -1e300};
     for (int i = 0; i < c.nn; i++)
         for (int d = 0; d < 3; d++) {
@@ -353,7 +355,7 @@ struct BlkArgs {
 //         sets them).
 // MODE 1: uku[e] = sum_case u_e' Ke_e u_e (E = 1, unmasked u).
 template <int NEN, int KB, int MODE, class TU, int ST>
-__global__ void __launch_bounds__(kWarps * 32, 3) k_blk_kmv(BlkArgs a, const TU* __restrict__ u, double* __restrict__ y,
+__global__ void __launch_bounds__(kWarps * 32, 5) k_blk_kmv(BlkArgs a, const TU* __restrict__ u, double* __restrict__ y,
                                                        double alpha, double* __restrict__ uku) {
     constexpr int ND = 3 * NEN, NPK = ND * (ND + 1) / 2;
     constexpr int MT = (ND + 7) / 8, KT = (ND + 3) / 4, NT = (KB + 7) / 8;
@@ -669,7 +671,7 @@ int blk_setup(Ctx& c) {
     BlockState& B = c.blk;
     if (B.ready) return 0;
     B.kb = blk_width(c.ncases);
-    const int node_cap = B.kb <= 8 ? 192 : 128;
+    const int node_cap = B.kb <= 8 ? 96 : 64;
     TRET(blk_build_schedule(c, node_cap));
     TRET(B.keb.alloc((size_t)c.ne * c.npk));
     TRET(B.Es.alloc(c.ne));
