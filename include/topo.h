@@ -373,6 +373,14 @@ int topo_server_stats_get(topo_server* s, topo_server_stats* st);
  *                  TOPO_ERR_TIMEOUT and the context stays usable; 0 restores
  *                  normal operation. */
 int topo_test_wait_limits(topo_ctx* ctx, unsigned barrier_spins, unsigned long long copy_cycles, int hold);
+/* Test hook (no counterpart in the reference; host only): the order in which
+ * the k-load block operator stores the packed upper triangle of an nd x nd
+ * element matrix (nd = 24 hex8, 12 tet4) in its shared-memory ring: entry k
+ * at perm[k] (nd (nd + 1) / 2 entries).  Returns 1 when the order is free of
+ * shared-memory bank conflicts for every half-warp A fragment of the
+ * m8n8k4 products, 0 when it fell back to the identity, < 0 on bad
+ * arguments. */
+int topo_test_block_bank_layout(int nd, int32_t* perm);
 
 /* ---------------------------------------------------------------- instrumentation */
 /* Kernel launches issued by this library in this process (all contexts). */

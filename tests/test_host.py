@@ -242,3 +242,31 @@ def test_batch_and_server_arguments_checked_on_the_host(T):
     assert L.topo_opt_step_batch(arr, 2, None, None) == T.TOPO_ERR_ARG and "null context" in T.last_error()
     assert L.topo_opt_step_batch(arr, 0, None, None) == 0  # nothing to do
     assert L.topo_server_set_batching(None, 10) == T.TOPO_ERR_ARG
+
+
+@pytest.mark.parametrize("nd", [24, 12])
+def test_block_bank_layout_is_conflict_free(T, nd):
+    """The block operator stores the packed element matrix permuted so that the
+    distinct entries each half-warp reads for one m8n8k4 A fragment (lane l:
+    row 8 mt + l/4, column 4 kt + l%4) sit at positions distinct mod 16, i.e.
+    in distinct shared-memory banks for 64-bit loads.  Checked here against
+    an independent restatement of the fragment layout (host only)."""
+    import ctypes as C
+    npk = nd * (nd + 1) // 2
+    perm = (C.c_int32 * npk)()
+    assert T.lib().topo_test_block_bank_layout(nd, perm) == 1
+    p = np.array(perm[:])
+    assert sorted(p.tolist()) == list(range(npk))
+
+    def pk(i, j):
+        i, j = min(i, j), max(i, j)
+        return i * nd - i * (i - 1) // 2 + (j - i)
+
+    for mt in range((nd + 7) // 8):
+        for kt in range((nd + 3) // 4):
+            for half in range(2):
+                ks = {pk(8 * mt + l // 4, 4 * kt + l % 4) for l in range(16 * half, 16 * half + 16)
+                      if 8 * mt + l // 4 < nd}
+                res = [p[k] % 16 for k in ks]
+                assert len(set(res)) == len(res), (mt, kt, half)
+    assert T.lib().topo_test_block_bank_layout(10, perm) == -1

@@ -133,6 +133,7 @@ _SIGS = {
     "topo_server_cancel": ([C.c_void_p, C.c_int], C.c_int),
     "topo_server_set_batching": ([C.c_void_p, C.c_int], C.c_int),
     "topo_test_wait_limits": ([C.c_void_p, C.c_uint, C.c_ulonglong, C.c_int], C.c_int),
+    "topo_test_block_bank_layout": ([C.c_int, C.POINTER(C.c_int32)], C.c_int),
     "topo_server_job": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)] + [C.c_void_p] * 3 +
                         [_dp, _dp], C.c_int),
     "topo_server_stats_get": ([C.c_void_p, C.c_void_p], C.c_int),

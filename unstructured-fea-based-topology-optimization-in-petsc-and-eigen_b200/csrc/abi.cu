@@ -733,6 +733,16 @@ int topo_mma_kkt_residual(topo_ctx* ctx, const double* x_d, const double* dfdx_d
     return mma_kkt(c, x_d, dfdx_d, c.dsc.p + DS_TMP + 1, dgdx_d, xmin_d, xmax_d, norm2, norm_inf);
 }
 
+int topo_test_block_bank_layout(int nd, int32_t* perm) {
+    if (nd != 24 && nd != 12) { set_error("nd must be 24 (hex8) or 12 (tet4)"); return TOPO_ERR_ARG; }
+    if (!perm) { set_error("null output pointer"); return TOPO_ERR_ARG; }
+    GUARD_BEGIN
+    std::vector<int> p;
+    const int rc = blk_bank_perm(nd, p);
+    for (size_t k = 0; k < p.size(); k++) perm[k] = p[k];
+    return rc;
+    GUARD_END
+}
 int topo_test_wait_limits(topo_ctx* ctx, unsigned barrier_spins, unsigned long long copy_cycles, int hold) {
     if (!ctx || (hold != 0 && hold != 1)) { set_error("bad argument"); return TOPO_ERR_ARG; }
     Ctx::WaitLimits d;
