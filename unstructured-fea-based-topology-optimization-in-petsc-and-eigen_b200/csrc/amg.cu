@@ -654,11 +654,22 @@ __global__ void k_cheb_upd(long n, const T* __restrict__ t, T* __restrict__ r, T
 }
 
 // ----------------------------------------------------------------- fixed-pattern SpGEMM
+// entries of a BB-entry block stored block by block, rounded up to whole
+// 16-byte vectors
+template <class T, int BB>
+__host__ __device__ constexpr int padded_block() {
+    return (BB + 16 / (int)sizeof(T) - 1) / (16 / (int)sizeof(T)) * (16 / (int)sizeof(T));
+}
+
 // C = A * B with blocks A: BR x BK, B: BK x BC, C: BR x BC, from the
 // product's plan (output-stationary): G lanes per C row, a lane owns one C block at a time and sums its contributing (A block,
-// B block) pairs in registers: no shared memory, no atomics, no searches,
-// and the C block's entries are written as coalesced runs.
-template <class T, int BR, int BK, int BC, int GS, int PS>
+// B block) pairs in registers: no shared memory, no atomics, no searches.
+// BL 0: B slot-interleaved (the plan gives the block's first value), read
+//       entry by entry; 1: B block by block, padded to 16-byte vectors (the
+//       plan gives the block index), each block read as whole vectors.
+// CL 0: C slot-interleaved, a row's entries written as coalesced runs;
+//       1: C block by block, padded (the B operand of a later product).
+template <class T, int BR, int BK, int BC, int GS, int PS, int BL, int CL>
 __global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __restrict__ Arp, const T* __restrict__ A,
                                                      const T* __restrict__ B, const int* __restrict__ Crp,
                                                      T* __restrict__ C, const int* __restrict__ pptr,
@@ -667,6 +678,8 @@ __global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __res
     // lists: shorter dependent-load chains), combined by xor shuffles; the
     // next pair's plan entry is fetched while the current pair is summed
     constexpr int BRK = BR * BK, BKC = BK * BC, BRC = BR * BC, G = GS * PS;
+    constexpr int VPL = 16 / (int)sizeof(T);
+    constexpr int BKCP = padded_block<T, BKC>(), BRCP = padded_block<T, BRC>();
     const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
     const int i = (int)(tid / G), gl = (int)(tid % G), gs = gl / PS, ps = gl % PS;
     if (i >= nrows) return;
@@ -684,12 +697,21 @@ __global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __res
         uint2 w = p < p1 ? __ldg(pr + p) : make_uint2(0u, 0u);
         for (; p < p1; p += PS) {
             const int a = (int)(w.x >> 16), nB = (int)(w.x & 0xffffu);
-            const T* Bb = B + w.y;
-            T ab[BRK], bb[BKC];
+            T ab[BRK], bb[BL ? BKCP : BKC];
 #pragma unroll
             for (int e = 0; e < BRK; e++) ab[e] = __ldg(Ar + (size_t)e * nA + a);
+            if constexpr (BL == 1) {
+                const uint4* Bv = reinterpret_cast<const uint4*>(B + (size_t)w.y * BKCP);
 #pragma unroll
-            for (int e = 0; e < BKC; e++) bb[e] = __ldg(Bb + (size_t)e * nB);
+                for (int q = 0; q < BKCP / VPL; q++) {
+                    const uint4 t = __ldg(Bv + q);
+                    memcpy(bb + q * VPL, &t, 16);
+                }
+            } else {
+                const T* Bb = B + w.y;
+#pragma unroll
+                for (int e = 0; e < BKC; e++) bb[e] = __ldg(Bb + (size_t)e * nB);
+            }
             if (p + PS < p1) w = __ldg(pr + p + PS);
 #pragma unroll
             for (int r = 0; r < BR; r++)
@@ -707,9 +729,37 @@ __global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __res
 #pragma unroll
                 for (int o = PS / 2; o > 0; o >>= 1) acc[e] += __shfl_xor_sync(gmask, acc[e], o);
         }
-        if (ps == 0)
+        if (ps == 0) {
+            if constexpr (CL == 1) {
+                T out[BRCP];
 #pragma unroll
-            for (int e = 0; e < BRC; e++) C[(size_t)c0 * BRC + (size_t)e * nC + sl] = acc[e];
+                for (int e = 0; e < BRCP; e++) out[e] = e < BRC ? acc[e < BRC ? e : 0] : T(0);
+                uint4* Cv = reinterpret_cast<uint4*>(C + (size_t)(c0 + sl) * BRCP);
+#pragma unroll
+                for (int q = 0; q < BRCP / VPL; q++) {
+                    uint4 t;
+                    memcpy(&t, out + q * VPL, 16);
+                    Cv[q] = t;
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < BRC; e++) C[(size_t)c0 * BRC + (size_t)e * nC + sl] = acc[e];
+            }
+        }
+    }
+}
+
+// P block by block (padded to 16-byte vectors) from its slot-interleaved
+// copy: warp per row, lanes over the row's values in storage order
+template <class T, int BB>
+__global__ void k_block_pad(int nrows, const int* __restrict__ rp, const T* __restrict__ P, T* __restrict__ Pb) {
+    constexpr int BBP = padded_block<T, BB>();
+    const int i = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (i >= nrows) return;
+    const int r0 = rp[i], nb = rp[i + 1] - r0;
+    for (int t = lane; t < nb * BB; t += 32) {
+        const int e = t / nb, sl = t - e * nb;
+        Pb[(size_t)(r0 + sl) * BBP + e] = P[(size_t)r0 * BB + t];
     }
 }
 
@@ -1109,7 +1159,12 @@ static int alloc_vals(Ctx& c) {
         if (l + 1 < c.nlev) {
             TRET(v.P[l].alloc((size_t)D.P.nnzb * bs * 6));
             TRET(v.T_[l].alloc((size_t)D.P.nnzb * bs * 6));
-            TRET(v.AP[l].alloc((size_t)D.AP.nnzb * bs * 6));
+            // A P and the copy of P that is its B operand: block by block, padded
+            const int bbp = bs == 3 ? padded_block<T, 18>() : padded_block<T, 36>();
+            TRET(v.AP[l].alloc((size_t)D.AP.nnzb * bbp));
+            TRET(v.AP[l].zero(c.s));
+            TRET(v.Pb[l].alloc((size_t)D.P.nnzb * bbp));
+            TRET(v.Pb[l].zero(c.s));
             TRET(v.R[l].alloc((size_t)D.R.nnzb * bs * 6));
             if (D.pnw) TRET(v.Pk[l].alloc((size_t)D.P.nnzb * bs * 6));
         }
@@ -1134,28 +1189,28 @@ static const T* pt_vals(Ctx& c, int l) {
     return (const T*)c.dl[l].Pt32c.p;
 }
 
-template <int BR, int BK, int BC, class T, int GS, int PS>
+template <int BR, int BK, int BC, class T, int GS, int PS, int BL, int CL>
 static void spgemm_plan_g(Ctx& c, const DevPattern& Ap, const T* A, const T* B, const DevPattern& Cp, T* C,
                           const ProductPlan& pl) {
     const long nt = (long)Cp.nrows * GS * PS;
-    k_spgemm_plan<T, BR, BK, BC, GS, PS><<<(int)((nt + 255) / 256), 256, 0, c.s>>>(
+    k_spgemm_plan<T, BR, BK, BC, GS, PS, BL, CL><<<(int)((nt + 255) / 256), 256, 0, c.s>>>(
         Cp.nrows, Ap.rp.p, A, B, Cp.rp.p, C, pl.ptr.p, pl.pr.p);
 }
 // C = A B from the product's plan: lanes per C block by the mean pair count,
 // C blocks per row group by the mean row length (at most 32 lanes per row)
-template <int BR, int BK, int BC, class T>
+template <int BR, int BK, int BC, class T, int BL = 0, int CL = 0>
 static int spgemm_plan(Ctx& c, const DevPattern& Ap, const T* A, const T* B, const DevPattern& Cp, T* C,
                        const ProductPlan& pl) {
     if (pl.avg_pairs >= 48) {
-        if (pl.avg_row > 2) spgemm_plan_g<BR, BK, BC, T, 4, 8>(c, Ap, A, B, Cp, C, pl);
-        else spgemm_plan_g<BR, BK, BC, T, 2, 8>(c, Ap, A, B, Cp, C, pl);
+        if (pl.avg_row > 2) spgemm_plan_g<BR, BK, BC, T, 4, 8, BL, CL>(c, Ap, A, B, Cp, C, pl);
+        else spgemm_plan_g<BR, BK, BC, T, 2, 8, BL, CL>(c, Ap, A, B, Cp, C, pl);
     } else if (pl.avg_pairs >= 16) {
-        if (pl.avg_row > 4) spgemm_plan_g<BR, BK, BC, T, 8, 4>(c, Ap, A, B, Cp, C, pl);
-        else spgemm_plan_g<BR, BK, BC, T, 4, 4>(c, Ap, A, B, Cp, C, pl);
+        if (pl.avg_row > 4) spgemm_plan_g<BR, BK, BC, T, 8, 4, BL, CL>(c, Ap, A, B, Cp, C, pl);
+        else spgemm_plan_g<BR, BK, BC, T, 4, 4, BL, CL>(c, Ap, A, B, Cp, C, pl);
     } else {
-        if (pl.avg_row > 12) spgemm_plan_g<BR, BK, BC, T, 16, 1>(c, Ap, A, B, Cp, C, pl);
-        else if (pl.avg_row > 6) spgemm_plan_g<BR, BK, BC, T, 8, 1>(c, Ap, A, B, Cp, C, pl);
-        else spgemm_plan_g<BR, BK, BC, T, 4, 1>(c, Ap, A, B, Cp, C, pl);
+        if (pl.avg_row > 12) spgemm_plan_g<BR, BK, BC, T, 16, 1, BL, CL>(c, Ap, A, B, Cp, C, pl);
+        else if (pl.avg_row > 6) spgemm_plan_g<BR, BK, BC, T, 8, 1, BL, CL>(c, Ap, A, B, Cp, C, pl);
+        else spgemm_plan_g<BR, BK, BC, T, 4, 1, BL, CL>(c, Ap, A, B, Cp, C, pl);
     }
     note_launch();
     TCK(cudaGetLastError());
@@ -1391,10 +1446,12 @@ static int numeric(Ctx& c) {
             } else {
                 TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 18, cudaMemcpyDeviceToDevice, c.s));
             }
-            TRET((spgemm_plan<3, 3, 6, T>(c, D.A, v.A[l].p, v.P[l].p, D.AP, v.AP[l].p, D.plan_AP)));
+            k_block_pad<T, 18><<<(D.P.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.P.nrows, D.P.rp.p, v.P[l].p,
+                                                                              v.Pb[l].p), note_launch();
+            TRET((spgemm_plan<3, 3, 6, T, 1, 1>(c, D.A, v.A[l].p, v.Pb[l].p, D.AP, v.AP[l].p, D.plan_AP)));
             k_transpose<T, 3><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
                                                                              D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();
-            TRET((spgemm_plan<6, 3, 6, T>(c, D.R, v.R[l].p, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
+            TRET((spgemm_plan<6, 3, 6, T, 1, 0>(c, D.R, v.R[l].p, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
         } else {
             if (c.p.amg_smooth_p) {
                 TRET((spgemm_plan<6, 6, 6, T>(c, D.A, v.A[l].p, ptv, D.P, v.T_[l].p, D.plan_T)));
@@ -1403,10 +1460,12 @@ static int numeric(Ctx& c) {
             } else {
                 TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 36, cudaMemcpyDeviceToDevice, c.s));
             }
-            TRET((spgemm_plan<6, 6, 6, T>(c, D.A, v.A[l].p, v.P[l].p, D.AP, v.AP[l].p, D.plan_AP)));
+            k_block_pad<T, 36><<<(D.P.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.P.nrows, D.P.rp.p, v.P[l].p,
+                                                                              v.Pb[l].p), note_launch();
+            TRET((spgemm_plan<6, 6, 6, T, 1, 1>(c, D.A, v.A[l].p, v.Pb[l].p, D.AP, v.AP[l].p, D.plan_AP)));
             k_transpose<T, 6><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
                                                                              D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();
-            TRET((spgemm_plan<6, 6, 6, T>(c, D.R, v.R[l].p, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
+            TRET((spgemm_plan<6, 6, 6, T, 1, 0>(c, D.R, v.R[l].p, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
         }
         TRET(pack_p<T>(c, l));
         TCK(cudaGetLastError());

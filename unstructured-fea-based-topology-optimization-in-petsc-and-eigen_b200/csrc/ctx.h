@@ -69,7 +69,8 @@ struct ProductPlan {
     int avg_row = 0;            // mean blocks per C row (picks lanes per row)
     int avg_pairs = 0;          // mean pairs per C block (picks lanes per block)
 };
-int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, int bkc, ProductPlan& out, cudaStream_t s);
+int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, int bkc, ProductPlan& out, cudaStream_t s,
+               bool block_index);
 
 struct AmgDevLevel {
     int bs = 3, nnode = 0, ndof = 0, nagg = 0;
@@ -95,12 +96,14 @@ struct AmgDevLevel {
 // numeric values of the hierarchy in precision T
 template <class T>
 struct AmgVals {
-    DBuf<T> A[kMaxLevels], P[kMaxLevels], T_[kMaxLevels], AP[kMaxLevels], R[kMaxLevels];
+    DBuf<T> A[kMaxLevels], P[kMaxLevels], T_[kMaxLevels], R[kMaxLevels];
+    DBuf<T> AP[kMaxLevels];     // A P block by block, padded (the B operand of R (A P))
     DBuf<T> dinv[kMaxLevels];
     DBuf<T> x[kMaxLevels], b[kMaxLevels], r[kMaxLevels], d[kMaxLevels], d2[kMaxLevels], t[kMaxLevels];
     DBuf<T> pv[kMaxLevels], pw[kMaxLevels];   // power-iteration vectors (warm start)
     DBuf<T> A0s;                // level-0 operator in the sliced-ELLPACK layout
     DBuf<T> Pk[kMaxLevels];     // P in the packed block-major layout (pk_off)
+    DBuf<T> Pb[kMaxLevels];     // P block by block, each block padded to 16 bytes (the B operand of A P)
     DBuf<T> kst;                // node-row copy of the element matrices (k_ke_node_rows), built once
     bool allocated = false;
 };

@@ -61,7 +61,11 @@ static void run_threads(int nth, F&& body) {
 // the offset of the B block's first value in the slot-interleaved B array
 // (bkc values per block), so the device reads both blocks without looking
 // up A's column or B's row pointer.
-int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, int bkc, ProductPlan& out, cudaStream_t s) {
+// block_index: each pair's B entry is the B block's index (B stored block by
+// block, padded, see k_spgemm_plan's BL); otherwise the offset of the block's
+// first value in the slot-interleaved layout
+int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, int bkc, ProductPlan& out, cudaStream_t s,
+               bool block_index) {
     const int n = A.nrows;
     std::vector<int> ptr((size_t)C.nnzb() + 1, 0);
     const int nth = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
@@ -103,7 +107,8 @@ int build_plan(const Pattern& A, const Pattern& B, const Pattern& C, int bkc, Pr
             for (int sb = 0; sb < nb; sb++) {
                 const int q = slot[B.ci[B.rp[k] + sb]];
                 pr[fill[q]++] = make_uint2(((uint32_t)a << 16) | (uint32_t)nb,
-                                           (uint32_t)((size_t)B.rp[k] * bkc + (size_t)sb));
+                                           block_index ? (uint32_t)(B.rp[k] + sb)
+                                                       : (uint32_t)((size_t)B.rp[k] * bkc + (size_t)sb));
             }
         }
         for (int q = C.rp[i]; q < C.rp[i + 1]; q++) slot[C.ci[q]] = -1;
@@ -586,9 +591,9 @@ int build_amg_host(Ctx& c) {
             TRET(D.Pt64c.upload(pv, s));
             TRET(D.Pt32c.upload(pv32, s));
             // B blocks are bs x 6 in all three products (Pt, P, A P)
-            TRET(build_plan(H.A, Ptp, H.P, H.bs * 6, D.plan_T, s));
-            TRET(build_plan(H.A, H.P, H.AP, H.bs * 6, D.plan_AP, s));
-            TRET(build_plan(H.R, H.AP, c.hl[l + 1].A, H.bs * 6, D.plan_RAP, s));
+            TRET(build_plan(H.A, Ptp, H.P, H.bs * 6, D.plan_T, s, false));
+            TRET(build_plan(H.A, H.P, H.AP, H.bs * 6, D.plan_AP, s, true));     // B: P block by block
+            TRET(build_plan(H.R, H.AP, c.hl[l + 1].A, H.bs * 6, D.plan_RAP, s, true));  // B: A P block by block
         }
     }
     return 0;
