@@ -767,8 +767,10 @@ __global__ void k_block_pad(int nrows, const int* __restrict__ rp, const T* __re
 template <class T, int BS>
 __global__ void k_smooth_p(int nnode, const int* __restrict__ rp, const int* __restrict__ ptpos,
                            const int* __restrict__ ptrp, const T* __restrict__ Ptv, const T* __restrict__ Tv,
-                           const T* __restrict__ dinv, const double* __restrict__ rho, T* __restrict__ P) {
-    constexpr int BB = BS * 6;
+                           const T* __restrict__ dinv, const double* __restrict__ rho, T* __restrict__ P,
+                           T* __restrict__ Pb) {
+    // P slot-interleaved, and block by block (padded) in Pb for the product A P
+    constexpr int BB = BS * 6, BBP = padded_block<T, BB>();
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (i >= nnode) return;
     const T w = T(4.0 / (3.0 * (*rho)));
@@ -779,6 +781,7 @@ __global__ void k_smooth_p(int nnode, const int* __restrict__ rp, const int* __r
         T v = -w * dinv[(long)BS * i + r] * Tv[(size_t)r0 * BB + q];
         if (haspt && s == pp) v += Ptv[(size_t)ptrp[i] * BB + e];
         P[(size_t)r0 * BB + q] = v;
+        Pb[(size_t)(r0 + s) * BBP + e] = v;
     }
 }
 
@@ -1188,6 +1191,11 @@ static const T* pt_vals(Ctx& c, int l) {
     if (std::is_same<T, double>::value) return (const T*)c.dl[l].Pt64c.p;
     return (const T*)c.dl[l].Pt32c.p;
 }
+template <class T>
+static const T* pt_vals_padded(Ctx& c, int l) {
+    if (std::is_same<T, double>::value) return (const T*)c.dl[l].Pt64p.p;
+    return (const T*)c.dl[l].Pt32p.p;
+}
 
 template <int BR, int BK, int BC, class T, int GS, int PS, int BL, int CL>
 static void spgemm_plan_g(Ctx& c, const DevPattern& Ap, const T* A, const T* B, const DevPattern& Cp, T* C,
@@ -1440,28 +1448,30 @@ static int numeric(Ctx& c) {
         const T* ptv = pt_vals<T>(c, l);
         if (D.bs == 3) {
             if (c.p.amg_smooth_p) {
-                TRET((spgemm_plan<3, 3, 6, T>(c, D.A, v.A[l].p, ptv, D.P, v.T_[l].p, D.plan_T)));
+                TRET((spgemm_plan<3, 3, 6, T, 1, 0>(c, D.A, v.A[l].p, pt_vals_padded<T>(c, l), D.P, v.T_[l].p, D.plan_T)));
                 k_smooth_p<T, 3><<<(D.nnode * 32 + 255) / 256, 256, 0, c.s>>>(
-                    D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p), note_launch();
+                    D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p,
+                    v.Pb[l].p), note_launch();
             } else {
                 TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 18, cudaMemcpyDeviceToDevice, c.s));
+                k_block_pad<T, 18><<<(D.P.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.P.nrows, D.P.rp.p, v.P[l].p,
+                                                                                  v.Pb[l].p), note_launch();
             }
-            k_block_pad<T, 18><<<(D.P.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.P.nrows, D.P.rp.p, v.P[l].p,
-                                                                              v.Pb[l].p), note_launch();
             TRET((spgemm_plan<3, 3, 6, T, 1, 1>(c, D.A, v.A[l].p, v.Pb[l].p, D.AP, v.AP[l].p, D.plan_AP)));
             k_transpose<T, 3><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
                                                                              D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();
             TRET((spgemm_plan<6, 3, 6, T, 1, 0>(c, D.R, v.R[l].p, v.AP[l].p, N.A, v.A[l + 1].p, D.plan_RAP)));
         } else {
             if (c.p.amg_smooth_p) {
-                TRET((spgemm_plan<6, 6, 6, T>(c, D.A, v.A[l].p, ptv, D.P, v.T_[l].p, D.plan_T)));
+                TRET((spgemm_plan<6, 6, 6, T, 1, 0>(c, D.A, v.A[l].p, pt_vals_padded<T>(c, l), D.P, v.T_[l].p, D.plan_T)));
                 k_smooth_p<T, 6><<<(D.nnode * 32 + 255) / 256, 256, 0, c.s>>>(
-                    D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p), note_launch();
+                    D.nnode, D.P.rp.p, D.ptpos.p, D.Ptp.rp.p, ptv, v.T_[l].p, v.dinv[l].p, c.rho.p + l, v.P[l].p,
+                    v.Pb[l].p), note_launch();
             } else {
                 TCK(cudaMemcpyAsync(v.P[l].p, ptv, sizeof(T) * D.P.nnzb * 36, cudaMemcpyDeviceToDevice, c.s));
+                k_block_pad<T, 36><<<(D.P.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.P.nrows, D.P.rp.p, v.P[l].p,
+                                                                                  v.Pb[l].p), note_launch();
             }
-            k_block_pad<T, 36><<<(D.P.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.P.nrows, D.P.rp.p, v.P[l].p,
-                                                                              v.Pb[l].p), note_launch();
             TRET((spgemm_plan<6, 6, 6, T, 1, 1>(c, D.A, v.A[l].p, v.Pb[l].p, D.AP, v.AP[l].p, D.plan_AP)));
             k_transpose<T, 6><<<(D.R.nrows * 32 + 255) / 256, 256, 0, c.s>>>(D.R.nrows, D.R.rp.p, D.R.ci.p, D.rperm.p,
                                                                              D.P.rp.p, v.P[l].p, v.R[l].p), note_launch();

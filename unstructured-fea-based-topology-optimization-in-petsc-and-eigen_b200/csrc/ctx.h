@@ -91,6 +91,8 @@ struct AmgDevLevel {
     DevPattern Ptp;             // tentative prolongator: one block per aggregated node
     DBuf<double> Pt64c;         // its bs x 6 blocks (compact, FP64)
     DBuf<float> Pt32c;          // (FP32 copy for the mixed form)
+    DBuf<double> Pt64p;         // the same blocks padded to 16-byte vectors (B operand of A Pt)
+    DBuf<float> Pt32p;
 };
 
 // numeric values of the hierarchy in precision T

@@ -590,8 +590,22 @@ int build_amg_host(Ctx& c) {
             TRET(D.Ptp.upload(Ptp, s));
             TRET(D.Pt64c.upload(pv, s));
             TRET(D.Pt32c.upload(pv32, s));
+            {
+                // the same blocks padded to whole 16-byte vectors (the B operand of A Pt)
+                const int bb = H.bs * 6, b64 = (bb + 1) / 2 * 2, b32 = (bb + 3) / 4 * 4;
+                const size_t nbk = pv.size() / bb;
+                std::vector<double> q64(nbk * b64, 0.0);
+                std::vector<float> q32(nbk * b32, 0.0f);
+                for (size_t g = 0; g < nbk; g++)
+                    for (int e = 0; e < bb; e++) {
+                        q64[g * b64 + e] = pv[g * bb + e];
+                        q32[g * b32 + e] = pv32[g * bb + e];
+                    }
+                TRET(D.Pt64p.upload(q64, s));
+                TRET(D.Pt32p.upload(q32, s));
+            }
             // B blocks are bs x 6 in all three products (Pt, P, A P)
-            TRET(build_plan(H.A, Ptp, H.P, H.bs * 6, D.plan_T, s, false));
+            TRET(build_plan(H.A, Ptp, H.P, H.bs * 6, D.plan_T, s, true));  // B: Pt block by block
             TRET(build_plan(H.A, H.P, H.AP, H.bs * 6, D.plan_AP, s, true));     // B: P block by block
             TRET(build_plan(H.R, H.AP, c.hl[l + 1].A, H.bs * 6, D.plan_RAP, s, true));  // B: A P block by block
         }
