@@ -733,7 +733,9 @@ __global__ void __launch_bounds__(256) k_spgemm_plan(int nrows, const int* __res
             if constexpr (CL == 1) {
                 T out[BRCP];
 #pragma unroll
-                for (int e = 0; e < BRCP; e++) out[e] = e < BRC ? acc[e < BRC ? e : 0] : T(0);
+                for (int e = 0; e < BRC; e++) out[e] = acc[e];
+#pragma unroll
+                for (int e = BRC; e < BRCP; e++) out[e] = T(0);
                 uint4* Cv = reinterpret_cast<uint4*>(C + (size_t)(c0 + sl) * BRCP);
 #pragma unroll
                 for (int q = 0; q < BRCP / VPL; q++) {

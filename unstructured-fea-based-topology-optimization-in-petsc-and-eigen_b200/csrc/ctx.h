@@ -61,11 +61,12 @@ struct AmgHostLevel {
 
 // Output-stationary plan of a fixed-pattern block product C = A B: for every
 // block of C (CSR order) the (A block, B block) pairs that contribute, each
-// as {slot in A's row << 16 | length of B's row, offset of the B block's
-// first value}.  Built on the host once per mesh.
+// as {slot in A's row << 16 | length of B's row, B block}, the B block given
+// as the offset of its first value (B slot-interleaved) or as its index (B
+// stored block by block, padded).  Built on the host once per mesh.
 struct ProductPlan {
     DBuf<int> ptr;              // nnzb(C) + 1
-    DBuf<uint2> pr;             // pairs: {A slot << 16 | B row length, B block's first value offset}
+    DBuf<uint2> pr;             // pairs: {A slot << 16 | B row length, B block (offset or index)}
     int avg_row = 0;            // mean blocks per C row (picks lanes per row)
     int avg_pairs = 0;          // mean pairs per C block (picks lanes per block)
 };
