@@ -171,8 +171,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_bsr_spmv(int nr
     for (int r = 0; r < BR; r++) acc[r] = T(0);
     if (active) {
         const T* Ar = A + (size_t)r0 * BR * BC;
+        // the next block's column id is fetched while this block is summed:
+        // one memory round trip per block instead of two
+        int j = gl < nb ? ci[r0 + gl] : 0;
         for (int s = gl; s < nb; s += G) {
-            const int j = ci[r0 + s];
+            const int jn = s + G < nb ? ci[r0 + s + G] : 0;
             T xv[BC];
 #pragma unroll
             for (int d = 0; d < BC; d++) xv[d] = x[(long)BC * j + d];
@@ -180,6 +183,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_bsr_spmv(int nr
             for (int r = 0; r < BR; r++)
 #pragma unroll
                 for (int d = 0; d < BC; d++) acc[r] += Ar[(r * BC + d) * nb + s] * xv[d];
+            j = jn;
         }
     }
 #pragma unroll
@@ -350,8 +354,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (BS <= 3 ? 5 : 4) : 2) k
     for (int q = 0; q < BS; q++) acc[q] = T(0);
     if (active) {
         const T* Ar = A + (size_t)r0 * BS * BS;
+        int j = gl < nb ? ci[r0 + gl] : 0;  // next column id prefetched as in k_bsr_spmv
         for (int s = gl; s < nb; s += G) {
-            const int j = ci[r0 + s];
+            const int jn = s + G < nb ? ci[r0 + s + G] : 0;
             T xv[BS];
 #pragma unroll
             for (int d = 0; d < BS; d++) xv[d] = dold[(long)BS * j + d];
@@ -359,6 +364,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (BS <= 3 ? 5 : 4) : 2) k
             for (int q = 0; q < BS; q++)
 #pragma unroll
                 for (int d = 0; d < BS; d++) acc[q] += Ar[(q * BS + d) * nb + s] * xv[d];
+            j = jn;
         }
     }
 #pragma unroll

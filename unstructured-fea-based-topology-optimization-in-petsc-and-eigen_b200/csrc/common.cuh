@@ -147,6 +147,30 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
+// Warp reduce-scatter of NV per-lane sums (NV a power of two, at most 32):
+// each halving step sends one half of the remaining sums to the partner lane
+// and keeps the other half, NV - 1 shuffles in all instead of 5 per sum; the
+// lanes that still share a sum then add it with a butterfly.  On return lane
+// l holds the warp's total of sum l % NV.  The order of additions is fixed.
+template <int NV>
+__device__ __forceinline__ double warp_reduce_scatter(double (&a)[NV]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int h = NV / 2; h >= 1; h >>= 1) {
+        const bool up = lane & h;
+#pragma unroll
+        for (int k = 0; k < h; k++) {
+            const double send = up ? a[k] : a[k + h];
+            const double keep = up ? a[k + h] : a[k];
+            a[k] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+        }
+    }
+    double r = a[0];
+#pragma unroll
+    for (int o = NV; o < 32; o <<= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    return r;
+}
+
 // Deterministic block reduction of NV sums; result valid in thread 0.
 // smem must hold NV * 32 doubles.
 template <int NV>

@@ -53,19 +53,62 @@ int dev_dot(Ctx& c, const double* a, const double* b, long n, double* out_dev) {
 }
 
 // ----------------------------------------------------------------- FGMRES kernels
+// The last block of a sweep to finish sums the sweep's per-block partials
+// part[k * gridDim.x + b] (k < nv) in a fixed order (a warp per sum, lanes
+// striding over the blocks) and writes out[k], so no separate launch is
+// needed for the grid-level sum; it then re-arms the counter for the next
+// sweep.  Optional sqrt of entry `sqrt_idx`.
+__device__ __forceinline__ void last_block_sum(int nv, const double* part, double* out, int sqrt_idx,
+                                               unsigned* count, bool* last) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) *last = atomicAdd(count, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!*last) return;
+    __threadfence();
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5, nb = gridDim.x;
+    for (int k = threadIdx.x >> 5; k < nv; k += nw) {
+        double v = 0.0;
+        for (int i = lane; i < nb; i += 32) v += __ldcg(part + (long)k * nb + i);
+        v = warp_sum(v);
+        if (lane == 0) out[k] = (k == sqrt_idx) ? sqrt(v) : v;
+    }
+    if (threadIdx.x == 0) *count = 0u;
+}
+
 // h_j = V_j . w for j < nv (classical Gram-Schmidt: one pass over w).
 // Two entries per thread and load (16-byte vectors: the basis rows are
-// 16-byte aligned, ld even), the odd last entry by one thread.
-template <int NV>
+// 16-byte aligned, ld even), U grid strides per loop trip so that small nv
+// still keeps several loads in flight, the odd last entry by one thread.
+// Warp sums by reduce-scatter, block sums by one thread per j.
+template <int NV, int U>
 __global__ void __launch_bounds__(256) k_mdot(long n, int nv, const double* __restrict__ V, long ld,
-                                              const double* __restrict__ w, double* __restrict__ part) {
-    __shared__ double sm[NV * 32];
+                                              const double* __restrict__ w, double* __restrict__ part,
+                                              double* __restrict__ out, unsigned* __restrict__ count) {
+    __shared__ double sm[8 * NV];
+    __shared__ bool last;
     double acc[NV];
 #pragma unroll
     for (int j = 0; j < NV; j++) acc[j] = 0.0;
     const long n2 = n >> 1;
     const double2* w2 = reinterpret_cast<const double2*>(w);
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n2; i += (long)gridDim.x * blockDim.x) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    for (; i + (U - 1) * stride < n2; i += U * stride) {
+        double2 wi[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) wi[u] = w2[i + u * stride];
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < nv) {
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const double2 v = reinterpret_cast<const double2*>(V + j * ld)[i + u * stride];
+                    acc[j] += v.x * wi[u].x + v.y * wi[u].y;
+                }
+            }
+    }
+    for (; i < n2; i += stride) {
         const double2 wi = w2[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
@@ -78,25 +121,54 @@ __global__ void __launch_bounds__(256) k_mdot(long n, int nv, const double* __re
 #pragma unroll
         for (int j = 0; j < NV; j++)
             if (j < nv) acc[j] += V[j * ld + n - 1] * w[n - 1];
-    block_sum<NV>(acc, sm);
-    if (threadIdx.x == 0)
-#pragma unroll
-        for (int j = 0; j < NV; j++)  // unrolled with a guard: a runtime bound would put acc in local memory
-            if (j < nv) part[(long)blockIdx.x * nv + j] = acc[j];
+    const double r = warp_reduce_scatter<NV>(acc);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane < NV) sm[wid * NV + lane] = r;
+    __syncthreads();
+    if (threadIdx.x < nv) {
+        double s = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += sm[q * NV + threadIdx.x];
+        part[(long)threadIdx.x * gridDim.x + blockIdx.x] = s;
+    }
+    last_block_sum(nv, part, out, -1, count, &last);
 }
-// w -= sum_j h_j V_j ; partial ||w||^2
-template <int NV>
+// w -= sum_j h_j V_j ; ||w|| (the last block's sum)
+template <int NV, int U>
 __global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __restrict__ V, long ld,
                                               const double* __restrict__ h, double* __restrict__ w,
-                                              double* __restrict__ part) {
-    __shared__ double sm[32];
+                                              double* __restrict__ part, double* __restrict__ norm_out,
+                                              unsigned* __restrict__ count) {
+    __shared__ double sm[8];
     __shared__ double hs[NV];
+    __shared__ bool last;
     if (threadIdx.x < nv) hs[threadIdx.x] = h[threadIdx.x];
     __syncthreads();
-    double v[1] = {0.0};
+    double s = 0.0;
     const long n2 = n >> 1;
     double2* w2 = reinterpret_cast<double2*>(w);
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n2; i += (long)gridDim.x * blockDim.x) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    for (; i + (U - 1) * stride < n2; i += U * stride) {
+        double2 wi[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) wi[u] = w2[i + u * stride];
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+            if (j < nv) {
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const double2 vv = reinterpret_cast<const double2*>(V + j * ld)[i + u * stride];
+                    wi[u].x -= hs[j] * vv.x;
+                    wi[u].y -= hs[j] * vv.y;
+                }
+            }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            w2[i + u * stride] = wi[u];
+            s += wi[u].x * wi[u].x + wi[u].y * wi[u].y;
+        }
+    }
+    for (; i < n2; i += stride) {
         double2 wi = w2[i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
@@ -106,7 +178,7 @@ __global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __re
                 wi.y -= hs[j] * vv.y;
             }
         w2[i] = wi;
-        v[0] += wi.x * wi.x + wi.y * wi.y;
+        s += wi.x * wi.x + wi.y * wi.y;
     }
     if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
         double wi = w[n - 1];
@@ -114,10 +186,18 @@ __global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __re
         for (int j = 0; j < NV; j++)
             if (j < nv) wi -= hs[j] * V[j * ld + n - 1];
         w[n - 1] = wi;
-        v[0] += wi * wi;
+        s += wi * wi;
     }
-    block_sum<1>(v, sm);
-    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    s = warp_sum(s);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sm[wid] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += sm[q];
+        part[blockIdx.x] = t;
+    }
+    last_block_sum(1, part, norm_out, 0, count, &last);
 }
 __global__ void k_scale_to(long n, const double* __restrict__ w, const double* __restrict__ s, double* __restrict__ v,
                            int invert) {
@@ -151,59 +231,54 @@ static int wave_of(const void* kern) {
     cudaGetLastError();
     return occ * nsm;
 }
-template <int NV>
+template <int NV, int U>
 static int mdot_grid(int cap) {
-    static const int wave = wave_of(reinterpret_cast<const void*>(k_mdot<NV>));
+    static const int wave = wave_of(reinterpret_cast<const void*>(k_mdot<NV, U>));
     return std::max(1, std::min(cap, wave));
 }
-template <int NV>
+template <int NV, int U>
 static int orth_grid(int cap) {
-    static const int wave = wave_of(reinterpret_cast<const void*>(k_orth<NV>));
+    static const int wave = wave_of(reinterpret_cast<const void*>(k_orth<NV, U>));
     return std::max(1, std::min(cap, wave));
 }
 
+// out[j] = V_j . w (j < nv), one sweep per 32 basis vectors, each finished by
+// its own last block
 static int mdot(Ctx& c, int nv, const double* V, long ld, const double* w, double* out) {
-    long n = c.ndof;
+    const long n = c.ndof;
     for (int j0 = 0; j0 < nv; j0 += 32) {
         const int k = std::min(32, nv - j0);
         const double* Vj = V + (size_t)j0 * ld;
-        int g = c.tune.red_blocks;
-        if (k <= 8) {
-            g = mdot_grid<8>(g);
-            k_mdot<8><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
-        } else if (k <= 16) {
-            g = mdot_grid<16>(g);
-            k_mdot<16><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
-        } else {
-            g = mdot_grid<32>(g);
-            k_mdot<32><<<g, 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p), note_launch();
-        }
+        const int g0 = c.tune.red_blocks;
+        if (k <= 8)
+            k_mdot<8, 2><<<mdot_grid<8, 2>(g0), 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p, out + j0, c.red_count.p);
+        else if (k <= 16)
+            k_mdot<16, 2><<<mdot_grid<16, 2>(g0), 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p, out + j0, c.red_count.p);
+        else
+            k_mdot<32, 1><<<mdot_grid<32, 1>(g0), 256, 0, c.s>>>(n, k, Vj, ld, w, c.red.p, out + j0, c.red_count.p);
+        note_launch();
         TCK(cudaGetLastError());
-        TRET(finalize_sum(c, c.red.p, g, k, out + j0));
     }
     return 0;
 }
+// w -= V h; *hn_out = ||w|| of the fully orthogonalised w (the last sweep's)
 static int orth(Ctx& c, int nv, const double* V, long ld, const double* h, double* w, double* hn_out) {
-    long n = c.ndof;
-    int g = c.tune.red_blocks;
+    const long n = c.ndof;
     for (int j0 = 0; j0 < nv; j0 += 32) {
         const int k = std::min(32, nv - j0);
         const double* Vj = V + (size_t)j0 * ld;
-        g = c.tune.red_blocks;
-        if (k <= 8) {
-            g = orth_grid<8>(g);
-            k_orth<8><<<g, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
-        } else if (k <= 16) {
-            g = orth_grid<16>(g);
-            k_orth<16><<<g, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
-        } else {
-            g = orth_grid<32>(g);
-            k_orth<32><<<g, 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p), note_launch();
-        }
+        const int g0 = c.tune.red_blocks;
+        if (k <= 8)
+            k_orth<8, 2><<<orth_grid<8, 2>(g0), 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p, hn_out, c.red_count.p);
+        else if (k <= 16)
+            k_orth<16, 2><<<orth_grid<16, 2>(g0), 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p, hn_out,
+                                                               c.red_count.p);
+        else
+            k_orth<32, 1><<<orth_grid<32, 1>(g0), 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p, hn_out,
+                                                               c.red_count.p);
+        note_launch();
+        TCK(cudaGetLastError());
     }
-    // the last sweep's partials hold ||w||^2 of the fully orthogonalised w
-    k_final<<<1, 32, 0, c.s>>>(g, 1, c.red.p, hn_out, 0), note_launch();
-    TCK(cudaGetLastError());
     return 0;
 }
 
@@ -597,6 +672,10 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
     if (c.p.precision == TOPO_PREC_MIXED && !c.Z32.p) TRET(c.Z32.alloc((size_t)m * n));
     if (c.p.precision != TOPO_PREC_MIXED && !c.Z64.p) TRET(c.Z64.alloc((size_t)m * n));
     if ((long)c.red.n < kRedMax * 40L) TRET(c.red.alloc(std::max<long>(kRedMax * 40L, 4096)));
+    if (!c.red_count.p) {
+        TRET(c.red_count.alloc(1));
+        TCK(cudaMemsetAsync(c.red_count.p, 0, sizeof(unsigned), c.s));
+    }
     while ((int)c.gm_ev.size() < m + 1) {
         cudaEvent_t e;
         TCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
