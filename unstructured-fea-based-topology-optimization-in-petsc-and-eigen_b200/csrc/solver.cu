@@ -132,7 +132,10 @@ __global__ void __launch_bounds__(256) k_mdot(long n, int nv, const double* __re
     }
     last_block_sum(nv, part, out, -1, count, &last);
 }
-// w -= sum_j h_j V_j ; ||w|| (the last block's sum)
+// w -= sum_j h_j V_j ; ||w|| (the last block's sum).  The sweep runs from the
+// top of the vectors down: k_mdot's last grid strides read the top entries of
+// w and of every V_j just before, so the first strides here find them in L2
+// (all of them while (nv + 1) vectors fit in L2).
 template <int NV, int U>
 __global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __restrict__ V, long ld,
                                               const double* __restrict__ h, double* __restrict__ w,
@@ -147,37 +150,37 @@ __global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __re
     const long n2 = n >> 1;
     double2* w2 = reinterpret_cast<double2*>(w);
     const long stride = (long)gridDim.x * blockDim.x;
-    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;  // entry pair n2 - 1 - i
     for (; i + (U - 1) * stride < n2; i += U * stride) {
         double2 wi[U];
 #pragma unroll
-        for (int u = 0; u < U; u++) wi[u] = w2[i + u * stride];
+        for (int u = 0; u < U; u++) wi[u] = w2[n2 - 1 - (i + u * stride)];
 #pragma unroll
         for (int j = 0; j < NV; j++)
             if (j < nv) {
 #pragma unroll
                 for (int u = 0; u < U; u++) {
-                    const double2 vv = reinterpret_cast<const double2*>(V + j * ld)[i + u * stride];
+                    const double2 vv = reinterpret_cast<const double2*>(V + j * ld)[n2 - 1 - (i + u * stride)];
                     wi[u].x -= hs[j] * vv.x;
                     wi[u].y -= hs[j] * vv.y;
                 }
             }
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            w2[i + u * stride] = wi[u];
+            w2[n2 - 1 - (i + u * stride)] = wi[u];
             s += wi[u].x * wi[u].x + wi[u].y * wi[u].y;
         }
     }
     for (; i < n2; i += stride) {
-        double2 wi = w2[i];
+        double2 wi = w2[n2 - 1 - i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
             if (j < nv) {
-                const double2 vv = reinterpret_cast<const double2*>(V + j * ld)[i];
+                const double2 vv = reinterpret_cast<const double2*>(V + j * ld)[n2 - 1 - i];
                 wi.x -= hs[j] * vv.x;
                 wi.y -= hs[j] * vv.y;
             }
-        w2[i] = wi;
+        w2[n2 - 1 - i] = wi;
         s += wi.x * wi.x + wi.y * wi.y;
     }
     if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
