@@ -132,11 +132,13 @@ __global__ void __launch_bounds__(256) k_mdot(long n, int nv, const double* __re
     }
     last_block_sum(nv, part, out, -1, count, &last);
 }
-// w -= sum_j h_j V_j ; ||w|| (the last block's sum).  The sweep runs from the
-// top of the vectors down: k_mdot's last grid strides read the top entries of
-// w and of every V_j just before, so the first strides here find them in L2
-// (all of them while (nv + 1) vectors fit in L2).
-template <int NV, int U>
+// w -= sum_j h_j V_j ; ||w|| (the last block's sum).  With TD the sweep
+// runs from the top of the vectors down: k_mdot's last grid strides read the
+// top entries of w and of every V_j just before, so when the nv + 1 vectors
+// do not all fit in L2 the first strides here still find the ones k_mdot left
+// there.  When they do fit, the ascending order is faster (descending
+// addresses stream more slowly from DRAM).
+template <int NV, int U, bool TD>
 __global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __restrict__ V, long ld,
                                               const double* __restrict__ h, double* __restrict__ w,
                                               double* __restrict__ part, double* __restrict__ norm_out,
@@ -150,37 +152,39 @@ __global__ void __launch_bounds__(256) k_orth(long n, int nv, const double* __re
     const long n2 = n >> 1;
     double2* w2 = reinterpret_cast<double2*>(w);
     const long stride = (long)gridDim.x * blockDim.x;
-    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;  // entry pair n2 - 1 - i
+    // entry pair q(i): i from the bottom up, or mirrored from the top down
+    const long qb = TD ? n2 - 1 : 0, qs = TD ? -1 : 1;
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
     for (; i + (U - 1) * stride < n2; i += U * stride) {
         double2 wi[U];
 #pragma unroll
-        for (int u = 0; u < U; u++) wi[u] = w2[n2 - 1 - (i + u * stride)];
+        for (int u = 0; u < U; u++) wi[u] = w2[qb + qs * (i + u * stride)];
 #pragma unroll
         for (int j = 0; j < NV; j++)
             if (j < nv) {
 #pragma unroll
                 for (int u = 0; u < U; u++) {
-                    const double2 vv = reinterpret_cast<const double2*>(V + j * ld)[n2 - 1 - (i + u * stride)];
+                    const double2 vv = reinterpret_cast<const double2*>(V + j * ld)[qb + qs * (i + u * stride)];
                     wi[u].x -= hs[j] * vv.x;
                     wi[u].y -= hs[j] * vv.y;
                 }
             }
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            w2[n2 - 1 - (i + u * stride)] = wi[u];
+            w2[qb + qs * (i + u * stride)] = wi[u];
             s += wi[u].x * wi[u].x + wi[u].y * wi[u].y;
         }
     }
     for (; i < n2; i += stride) {
-        double2 wi = w2[n2 - 1 - i];
+        double2 wi = w2[qb + qs * i];
 #pragma unroll
         for (int j = 0; j < NV; j++)
             if (j < nv) {
-                const double2 vv = reinterpret_cast<const double2*>(V + j * ld)[n2 - 1 - i];
+                const double2 vv = reinterpret_cast<const double2*>(V + j * ld)[qb + qs * i];
                 wi.x -= hs[j] * vv.x;
                 wi.y -= hs[j] * vv.y;
             }
-        w2[n2 - 1 - i] = wi;
+        w2[qb + qs * i] = wi;
         s += wi.x * wi.x + wi.y * wi.y;
     }
     if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -239,10 +243,15 @@ static int mdot_grid(int cap) {
     static const int wave = wave_of(reinterpret_cast<const void*>(k_mdot<NV, U>));
     return std::max(1, std::min(cap, wave));
 }
-template <int NV, int U>
+template <int NV, int U, bool TD>
 static int orth_grid(int cap) {
-    static const int wave = wave_of(reinterpret_cast<const void*>(k_orth<NV, U>));
+    static const int wave = wave_of(reinterpret_cast<const void*>(k_orth<NV, U, TD>));
     return std::max(1, std::min(cap, wave));
+}
+template <int NV, int U, bool TD>
+static void launch_orth(Ctx& c, int g0, long n, int k, const double* Vj, long ld, const double* h, double* w,
+                        double* hn_out) {
+    k_orth<NV, U, TD><<<orth_grid<NV, U, TD>(g0), 256, 0, c.s>>>(n, k, Vj, ld, h, w, c.red.p, hn_out, c.red_count.p);
 }
 
 // out[j] = V_j . w (j < nv), one sweep per 32 basis vectors, each finished by
@@ -264,6 +273,15 @@ static int mdot(Ctx& c, int nv, const double* V, long ld, const double* w, doubl
     }
     return 0;
 }
+static long l2_bytes() {
+    static const long b = [] {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrL2CacheSize, dev) != cudaSuccess) { cudaGetLastError(); v = 0; }
+        return (long)v;
+    }();
+    return b;
+}
 // w -= V h; *hn_out = ||w|| of the fully orthogonalised w (the last sweep's)
 static int orth(Ctx& c, int nv, const double* V, long ld, const double* h, double* w, double* hn_out) {
     const long n = c.ndof;
@@ -271,14 +289,17 @@ static int orth(Ctx& c, int nv, const double* V, long ld, const double* h, doubl
         const int k = std::min(32, nv - j0);
         const double* Vj = V + (size_t)j0 * ld;
         const int g0 = c.tune.red_blocks;
-        if (k <= 8)
-            k_orth<8, 2><<<orth_grid<8, 2>(g0), 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p, hn_out, c.red_count.p);
-        else if (k <= 16)
-            k_orth<16, 2><<<orth_grid<16, 2>(g0), 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p, hn_out,
-                                                               c.red_count.p);
-        else
-            k_orth<32, 1><<<orth_grid<32, 1>(g0), 256, 0, c.s>>>(n, k, Vj, ld, h + j0, w, c.red.p, hn_out,
-                                                               c.red_count.p);
+        const bool td = (long)(k + 1) * n * (long)sizeof(double) > l2_bytes();
+        if (k <= 8) {
+            if (td) launch_orth<8, 2, true>(c, g0, n, k, Vj, ld, h + j0, w, hn_out);
+            else launch_orth<8, 2, false>(c, g0, n, k, Vj, ld, h + j0, w, hn_out);
+        } else if (k <= 16) {
+            if (td) launch_orth<16, 2, true>(c, g0, n, k, Vj, ld, h + j0, w, hn_out);
+            else launch_orth<16, 2, false>(c, g0, n, k, Vj, ld, h + j0, w, hn_out);
+        } else {
+            if (td) launch_orth<32, 1, true>(c, g0, n, k, Vj, ld, h + j0, w, hn_out);
+            else launch_orth<32, 1, false>(c, g0, n, k, Vj, ld, h + j0, w, hn_out);
+        }
         note_launch();
         TCK(cudaGetLastError());
     }
