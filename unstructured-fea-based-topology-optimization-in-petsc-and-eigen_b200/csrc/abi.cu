@@ -248,6 +248,10 @@ int create(Ctx& c, int nen, int n_nodes, const double* vertex, int n_elems, cons
     TRET(build_amg_host(c));
     TRET(amg_alloc(c));
     if (c.p.deterministic) TRET(c.det_scr.alloc((size_t)c.ntiles * 32 * c.nde));  // per-element contributions
+    // completion counter of the reductions that finish in their last block
+    // (allocated here, never inside a graph capture)
+    TRET(c.red_count.alloc(1));
+    TCK(cudaMemsetAsync(c.red_count.p, 0, sizeof(unsigned), c.s));
     TRET(mma_alloc(c));
     TCK(cudaStreamSynchronize(c.s));
     return 0;

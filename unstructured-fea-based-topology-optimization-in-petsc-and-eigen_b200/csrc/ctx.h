@@ -235,7 +235,7 @@ struct Ctx {
     std::vector<cudaEvent_t> gm_ev;  // one per Arnoldi step (pipelined residual checks)
     StepGraphs graphs;          // captured Arnoldi steps of the single-load FGMRES
     DBuf<double> red;           // reduction partials
-    DBuf<unsigned> red_count;   // blocks done of the Gram-Schmidt sweep in flight (0 between sweeps)
+    DBuf<unsigned> red_count;   // blocks done of the last-block reduction in flight (0 between launches)
     DBuf<double> dsc;           // device scalars
     DBuf<int> di;               // device integers (DiSlot)
     PinnedScalars hsc;          // pinned host mirror for readbacks

@@ -696,10 +696,6 @@ static int fgmres(Ctx& c, const double* b, double* x, int* its_out, int* status)
     if (c.p.precision == TOPO_PREC_MIXED && !c.Z32.p) TRET(c.Z32.alloc((size_t)m * n));
     if (c.p.precision != TOPO_PREC_MIXED && !c.Z64.p) TRET(c.Z64.alloc((size_t)m * n));
     if ((long)c.red.n < kRedMax * 40L) TRET(c.red.alloc(std::max<long>(kRedMax * 40L, 4096)));
-    if (!c.red_count.p) {
-        TRET(c.red_count.alloc(1));
-        TCK(cudaMemsetAsync(c.red_count.p, 0, sizeof(unsigned), c.s));
-    }
     while ((int)c.gm_ev.size() < m + 1) {
         cudaEvent_t e;
         TCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -877,11 +873,27 @@ __global__ void k_cg_p(long n, const double* __restrict__ z, double* __restrict_
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         p[i] = first ? z[i] : z[i] + bb * p[i];
 }
-// a = beta/dpi; x += a p; r -= a w; z = Dinv r; partial (z.z, z.r)
+// sc[4] = dpi = p.w, the grid sum finished by the last block
+__global__ void k_cg_dot(long n, const double* __restrict__ p, const double* __restrict__ w, double* __restrict__ sc,
+                         double* __restrict__ part, unsigned* __restrict__ count) {
+    __shared__ double sm[32];
+    __shared__ bool last;
+    double v[1] = {0.0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) v[0] += p[i] * w[i];
+    block_sum<1>(v, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    last_block_sum(1, part, sc + 4, -1, count, &last);
+}
+// a = beta/dpi; x += a p; r -= a w; z = Dinv r; then, in the last block to
+// finish (every block has read sc by then): sc[1] = dp = sqrt(z.z),
+// sc[3] = betaold = sc[2], sc[2] = beta = z.r
 __global__ void k_cg_step(long n, const double* __restrict__ p, const double* __restrict__ w,
                           const double* __restrict__ dinv, double* __restrict__ x, double* __restrict__ r,
-                          double* __restrict__ z, const double* __restrict__ sc, double* __restrict__ part) {
+                          double* __restrict__ z, double* __restrict__ sc, double* __restrict__ part,
+                          unsigned* __restrict__ count) {
     __shared__ double sm[2 * 32];
+    __shared__ double tot[2];
+    __shared__ bool last;
     const double a = sc[2] / sc[4];
     double v[2] = {0.0, 0.0};
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -894,7 +906,28 @@ __global__ void k_cg_step(long n, const double* __restrict__ p, const double* __
         v[1] += zi * ri;
     }
     block_sum<2>(v, sm);
-    if (threadIdx.x == 0) { part[2L * blockIdx.x] = v[0]; part[2L * blockIdx.x + 1] = v[1]; }
+    const long nb = gridDim.x;
+    if (threadIdx.x == 0) { part[blockIdx.x] = v[0]; part[nb + blockIdx.x] = v[1]; }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(count, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (wid < 2) {
+        double t = 0.0;
+        for (long i = lane; i < nb; i += 32) t += __ldcg(part + wid * nb + i);
+        t = warp_sum(t);
+        if (lane == 0) tot[wid] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        sc[1] = sqrt(tot[0]);
+        sc[3] = sc[2];
+        sc[2] = tot[1];
+        *count = 0u;
+    }
 }
 // sc[1] = dp = sqrt(z.z); sc[3] = betaold = sc[2]; sc[2] = beta = z.r (+ sc[0] = snorm on start)
 __global__ void k_cg_final(int nb, int nv, const double* __restrict__ part, double* __restrict__ sc, int start) {
@@ -959,11 +992,10 @@ static int filter_cg_dd(Ctx& c, const double* b, double* x, int slot) {
     TRET(cond_begin(c, h, cudaGraphCondTypeWhile));
     k_cg_p<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.fz.p, c.fp.p, sc, 0, di + DI_CG_CUR), note_launch();
     TRET(filter_kf(c, c.fp.p, c.fw.p));
-    k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.red.p), note_launch();
-    k_final<<<1, 32, 0, c.s>>>(kRedBlocks, 1, c.red.p, sc + 4, -1), note_launch();
-    k_cg_step<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.fdiag_inv.p, x, c.fr.p, c.fz.p, sc, c.red.p),
+    k_cg_dot<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, sc, c.red.p, c.red_count.p), note_launch();
+    k_cg_step<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.fdiag_inv.p, x, c.fr.p, c.fz.p, sc, c.red.p,
+                                           c.red_count.p),
         note_launch();
-    k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 2, c.red.p, sc, 0), note_launch();
     k_cgdd_after<<<1, 32, 0, c.s>>>(sc, ttol, c.p.filter_dtol, c.p.filter_maxit, di, slot, h), note_launch();
     TRET(cond_end(c));
     TCK(cudaGetLastError());
@@ -1000,10 +1032,10 @@ int filter_cg(Ctx& c, const double* b, double* x, int* its_out, int slot) {
         if (hs[2] == 0.0) return 0;  // beta == 0
         k_cg_p<<<grid_for(n, 256), 256, 0, c.s>>>(n, c.fz.p, c.fp.p, sc, i == 0, nullptr), note_launch();
         TRET(filter_kf(c, c.fp.p, c.fw.p));
-        k_dot<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.red.p), note_launch();
-        k_final<<<1, 32, 0, c.s>>>(kRedBlocks, 1, c.red.p, sc + 4, -1), note_launch();
-        k_cg_step<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.fdiag_inv.p, x, c.fr.p, c.fz.p, sc, c.red.p), note_launch();
-        k_cg_final<<<1, 512, 0, c.s>>>(kRedBlocks, 2, c.red.p, sc, 0), note_launch();
+        k_cg_dot<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, sc, c.red.p, c.red_count.p), note_launch();
+        k_cg_step<<<kRedBlocks, 256, 0, c.s>>>(n, c.fp.p, c.fw.p, c.fdiag_inv.p, x, c.fr.p, c.fz.p, sc, c.red.p,
+                                               c.red_count.p),
+            note_launch();
         TCK(cudaMemcpyAsync(hs, sc, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
         TCK(cudaStreamSynchronize(c.s));
         dp = hs[1];
